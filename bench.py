@@ -1,0 +1,331 @@
+"""Benchmark of the direct Coulomb summation path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: the full 3D map, 256 x 256 x 256 grid at 0.5 A spacing, 65,536 atoms uniform in the
+128 A cube with charges U[-1, 1] (seeded synthetic data).  One step = one map.  Metric: pair
+evaluations per second (Gpair-evals/s, one pair = one (grid point, atom) term), whole job.
+
+Our arm (``--impl ours``, default) prints one JSON line with
+  value        device-timed throughput of the chosen form (CUDA events on the launching stream,
+               inputs resident in HBM, L2 flushed between steps), max over ranks;
+  plain        the same for the plain FP32 kernel (all-MUFU, FP32 accumulation);
+  e2e          the chosen form through the host-buffer C-ABI call (coul_forward_3d_host): atoms
+               copied from pinned host memory and the map copied back, inside the timed region;
+  roofline     achieved pair rate of the forward kernel against the MUFU+FMA pair roofline built
+               from pipe rates measured in the same run;
+  cpu_baseline the FP64 oracle (restatement of KTT's reference computation) on the host cores, on
+               a bounded sample of grid points; the same sample gives the error of the GPU maps.
+Under torchrun each rank computes its own map (weak scaling, no collective on the data path);
+timings are reduced with MAX over ranks.
+
+The reference arm (``--impl reference``) times KTT's reference computation restated in C (the
+oracle, all host threads) on a bounded sample of the same workload on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "Coulomb Gpair-evals/s vs plain kernel & rsqrt roofline at ≤1e-5 FP64 rel err"
+UNIT = "Gpair-evals/s"
+WORKLOAD = "CoulombSum3d full map 256^3 grid, h=0.5 A, 65536 atoms U[0,128)^3, q U[-1,1]"
+SOFT_ISSUE_SLOTS = 8  # FMA-pipe rsqrt: 2 integer + 6 FP32 instructions
+
+
+def _chosen_tune():
+    import ktt_b200
+    path = os.path.join(REPO, "ktt_b200", "tuned", "b200_map3d.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return ktt_b200.Tune(**json.load(f)["tune"]), os.path.relpath(path, REPO)
+    return ktt_b200.Tune(), "built-in default"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu_index = gpu_index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"coul_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu_index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self) -> dict | None:
+        if self.proc is None or not os.path.exists(self.path):
+            return None
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def _dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_reference(args) -> None:
+    """KTT's reference computation (FP64 C restatement, all host threads) on a bounded sample."""
+    world, rank, _ = _dist()
+    if rank != 0:
+        return
+    import oracle
+    from ktt_b200 import workloads
+    w = workloads.uniform_map()
+    total = int(np.prod(w.dims))
+    threads = oracle.max_threads()
+    # size the per-step sample for about 2 s of CPU work: calibrate on 1024 points
+    cal = workloads.subset_indices(total, 1024 / total, seed=101)
+    t0 = time.perf_counter()
+    oracle.points3d(w.atoms, w.spacing, w.dims, cal)
+    rate = len(cal) * w.atoms.shape[0] / max(time.perf_counter() - t0, 1e-6)
+    npts = int(min(max(256, 2.0 * rate / w.atoms.shape[0]), total))
+    idx = workloads.subset_indices(total, npts / total, seed=102)
+    for _ in range(args.warmup):
+        oracle.points3d(w.atoms, w.spacing, w.dims, idx[: max(1, len(idx) // 8)])
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        oracle.points3d(w.atoms, w.spacing, w.dims, idx)
+        times.append(time.perf_counter() - t0)
+    pairs = len(idx) * w.atoms.shape[0]
+    value = pairs * len(times) / sum(times) / 1e9
+    sample = f"{len(idx)} seeded grid points x {w.atoms.shape[0]} atoms per step (FP64)"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": WORKLOAD, "sample_points_per_step": len(idx), "l2": "n/a (host CPU)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def _load_traffic() -> dict | None:
+    path = os.path.join(REPO, "profiles", "forward_map3d_traffic.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f)
+    return None
+
+
+def run_ours(args) -> None:
+    import torch
+    import ktt_b200
+    from ktt_b200 import errors, workloads
+
+    world, rank, local = _dist()
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.device("cuda", torch.cuda.current_device())
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    ctx = ktt_b200.CoulombContext(dev.index)
+    w = workloads.uniform_map(seed=2 + rank)  # each rank: its own map (weak scaling)
+    nx, ny, nz = w.dims
+    pairs = w.pairs
+    atoms = torch.from_numpy(w.atoms).to(dev)
+    out = torch.empty((nz, ny, nx), dtype=torch.float32, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # 256 MiB > 126 MB L2
+    stream = torch.cuda.current_stream(dev)
+
+    chosen, chosen_src = _chosen_tune()
+    plain = ktt_b200.Tune(block_x=chosen.block_x, block_y=chosen.block_y, z_iterations=chosen.z_iterations,
+                          x_points=chosen.x_points, unroll=chosen.unroll)
+    if not ktt_b200.tune_supported(plain):
+        plain = ktt_b200.Tune()
+
+    def timed_steps(tune, steps, warmup):
+        for _ in range(warmup):
+            ctx.forward_3d(atoms, w.dims, w.spacing, tune=tune, out=out)
+        torch.cuda.synchronize(dev)
+        barrier()
+        torch.cuda.synchronize(dev)
+        evs = []
+        for _ in range(steps):
+            flush.zero_()  # L2 flush outside the timed interval
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            ctx.forward_3d(atoms, w.dims, w.spacing, tune=tune, out=out)
+            b.record(stream)
+            evs.append((a, b))
+        torch.cuda.synchronize(dev)
+        barrier()
+        torch.cuda.synchronize(dev)
+        ms = [a.elapsed_time(b) for a, b in evs]
+        return max_over_ranks(sum(ms)), ms
+
+    rsqrt_rate, ffma_rate = ctx.pipe_rates()
+
+    with ClockSampler(dev.index) as clocks:
+        total_ms, step_ms = timed_steps(chosen, args.steps, args.warmup)
+    clk = clocks.summary()
+    value = world * pairs * args.steps / (total_ms * 1e-3) / 1e9
+    chosen_map = out.clone()
+
+    plain_ms, _ = timed_steps(plain, max(2, args.steps // 2), 1)
+    plain_value = world * pairs * max(2, args.steps // 2) / (plain_ms * 1e-3) / 1e9
+    plain_map = out.clone()
+
+    # end to end through the host-buffer C ABI call, pinned host memory
+    h_atoms = torch.from_numpy(w.atoms).pin_memory()
+    h_out = torch.empty((nz, ny, nx), dtype=torch.float32).pin_memory()
+    e2e_steps = max(2, args.steps // 2)
+    for _ in range(1):
+        ctx.forward_3d_host(h_atoms.numpy(), w.dims, w.spacing, tune=chosen, out_np=h_out.numpy())
+    torch.cuda.synchronize(dev)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        ctx.forward_3d_host(h_atoms.numpy(), w.dims, w.spacing, tune=chosen, out_np=h_out.numpy())
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e_value = world * pairs * e2e_steps / e2e_s / 1e9
+
+    # roofline of the forward kernel (one launch per step)
+    avg_launch_s = 1e-3 * sum(step_ms) / len(step_ms)
+    achieved = pairs / avg_launch_s / 1e9
+    fm = ffma_rate / rsqrt_rate
+    s = SOFT_ISSUE_SLOTS
+    r_mufu = rsqrt_rate / 1e9
+    r_comb = rsqrt_rate * (fm - 1 + s) / (2 + s) / 1e9
+    traffic = _load_traffic()
+    roofline = {
+        "bound": "mufu+fma", "achieved": achieved, "peak": r_comb, "unit": UNIT, "frac": achieved / r_comb,
+        "traffic": traffic.get("bytes_per_launch") if traffic else None,
+        "peak_source": "measured in this run: MUFU rsqrt and FP32 FMA throughput microkernels",
+        "peak_mufu_only": r_mufu, "frac_mufu_only": achieved / r_mufu,
+        "rsqrt_per_s": rsqrt_rate, "ffma_per_s": ffma_rate, "soft_rsqrt_issue_slots": s,
+        "plain_achieved": plain_value / world, "plain_frac": plain_value / world / r_comb,
+    }
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if chosen.precision == ktt_b200.PREC_FP32 else "f32 pairs, f64 merge",
+        "data": "synthetic (seeded)",
+        "config": {"workload": WORKLOAD, "pairs_per_step_per_gpu": pairs, "tune": chosen.as_dict(),
+                   "tune_source": chosen_src, "l2": "flushed between timed steps (256 MiB write)",
+                   "parallelism": f"replicas x{world} (each rank its own map)"},
+        "plain": {"value": plain_value, "unit": UNIT, "tune": plain.as_dict()},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(w.atoms.nbytes),
+                "d2h_bytes_per_step": int(nx * ny * nz * 4), "api": "coul_forward_3d_host (pinned host buffers)"},
+        "gpu_launches": args.steps,
+        "roofline": roofline,
+        "clocks": clk,
+    }
+
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle
+        total = nx * ny * nz
+        threads = oracle.max_threads()
+        cal = workloads.subset_indices(total, 1024 / total, seed=101)
+        t0 = time.perf_counter()
+        oracle.points3d(w.atoms, w.spacing, w.dims, cal)
+        rate = len(cal) * w.atoms.shape[0] / max(time.perf_counter() - t0, 1e-6)
+        npts = int(min(max(1024, args.cpu_seconds * rate / w.atoms.shape[0]), total))
+        idx = workloads.subset_indices(total, npts / total, seed=102)
+        t0 = time.perf_counter()
+        ref, sabs = oracle.points3d(w.atoms, w.spacing, w.dims, idx, want_sumabs=True)
+        cpu_s = time.perf_counter() - t0
+        cpu_value = len(idx) * w.atoms.shape[0] / cpu_s / 1e9
+        line["cpu_baseline"] = {"value": cpu_value, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": f"{len(idx)} seeded grid points x {w.atoms.shape[0]} atoms, FP64, "
+                                          f"{cpu_s:.1f} s"}
+        line["accuracy"] = {
+            "chosen": errors.report(chosen_map.cpu().numpy().reshape(-1)[idx], ref, sumabs=sabs),
+            "plain": errors.report(plain_map.cpu().numpy().reshape(-1)[idx], ref, sumabs=sabs),
+            "points": len(idx), "tolerance_rel_norm": 1e-5,
+        }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="size of the CPU-baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,203 @@
+/*
+ * coulktt.h -- C ABI of the B200-native direct Coulomb summation library
+ * (libcoulktt.so).
+ *
+ * This is the thin layer that KTT-style host code reaches through the C++
+ * ktt::Tuner surface (include/Ktt.h), and that other languages bind directly
+ * (Python ctypes in ktt_b200/__init__.py).  Plain pointers and sizes only; no
+ * C++ or torch types cross it; no exception crosses it.  Every function
+ * returns a coul_status; on failure a description is available from
+ * coul_last_error() (thread-local).
+ *
+ * What each entry point replaces in KTT 2.1.0 (paths relative to the KTT tree):
+ *   coul_ctx_create/destroy   Tuner::Tuner / ~Tuner on one CUDA device
+ *                             (Source/Tuner.h:70, Source/ComputeEngine/Cuda/CudaEngine.cpp:29-60)
+ *   coul_forward_3d           launch of directCoulombSum, 3D
+ *                             (Examples/CoulombSum3d/CoulombSum3d.cu:1-47 through
+ *                             Source/ComputeEngine/Cuda/CudaKernel.cpp:43-70)
+ *   coul_forward_3d_soa       same with USE_SOA == 1 argument layout
+ *                             (Examples/CoulombSum3d/CoulombSum3d.cu:23-28)
+ *   coul_forward_3d_reference launch of directCoulombSumReference
+ *                             (Examples/CoulombSum3d/CoulombSum3dReference.cu:1-28)
+ *   coul_forward_2d           launch of directCoulombSum, 2D slice with the
+ *                             precomputed dz^2 in the atom's .z
+ *                             (Examples/CoulombSum2d/CoulombSum2dSimple.cl:29-79,
+ *                             reference Examples/CoulombSum2d/CoulombSum2dReference.cl:1-21)
+ *   coul_slice_atoms          the host-side dz^2 precompute of the iterative
+ *                             launcher (Examples/CoulombSum3dIterative/CoulombSum3dIterative.cpp:160-179),
+ *                             done on the device
+ *   coul_forward_3d_host      Tuner::Run with host output buffers
+ *                             (Source/Tuner.h:536, BufferOutputDescriptor download)
+ *   coul_elapsed_ms           kernel duration from the event pair bracketing the launch
+ *                             (Source/ComputeEngine/Cuda/CudaKernel.cpp:62-67, CudaEvent.cpp:30-36)
+ *   coul_synchronize          ComputeInterface::SynchronizeQueue / WaitForComputeAction
+ *                             (Source/Api/ComputeInterface.h)
+ *   coul_tune_supported       the CompilationFailed / DeviceLimitsExceeded checks made before a
+ *                             launch (Source/ComputeEngine/Cuda/CudaEngine.cpp:117-138); here a
+ *                             configuration maps onto an ahead-of-time compiled sm_100a variant
+ *
+ * Units and layout: atoms are float4 (x, y, z, q) in Angstrom / elementary
+ * charge, 16-byte aligned; grid point (i, j, k) sits at
+ * (fmaf(i, h, ox), fmaf(j, h, oy), fmaf(k, h, oz)) -- for a zero origin this
+ * is KTT's gridSpacing * index; the map is stored x fastest:
+ * out[(k * ny + j) * nx + i].  Pointers named d_* are device pointers, h_*
+ * host pointers.  All launches are asynchronous on the context's stream
+ * unless stated otherwise.
+ */
+#ifndef COULKTT_H
+#define COULKTT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define COUL_API __attribute__((visibility("default")))
+#else
+#define COUL_API
+#endif
+
+typedef enum coul_status {
+    COUL_OK = 0,
+    COUL_ERR_INVALID_ARGUMENT = 1,  /* bad pointer, size, alignment or grid */
+    COUL_ERR_CUDA = 2,              /* a CUDA runtime call failed */
+    COUL_ERR_UNSUPPORTED = 3,       /* no compiled variant for this configuration (KTT: CompilationFailed) */
+    COUL_ERR_DEVICE_LIMITS = 4,     /* block size / shared memory beyond the device (KTT: DeviceLimitsExceeded) */
+    COUL_ERR_TIMEOUT = 5,           /* a bounded device-side wait gave up; results are invalid */
+    COUL_ERR_NO_DEVICE = 6,         /* no CUDA device, or not an sm_100 device */
+    COUL_ERR_OUT_OF_MEMORY = 7
+} coul_status;
+
+/* Where the atom stream is read from inside the kernel (KTT USE_CONSTANT_MEMORY). */
+enum {
+    COUL_ATOMS_SHARED_TMA = 0, /* tiles staged into shared memory by TMA bulk copies */
+    COUL_ATOMS_CONSTANT = 1    /* chunks of 4096 atoms copied into __constant__ memory */
+};
+
+/* Accumulation form.  All forms evaluate each pair in FP32. */
+enum {
+    COUL_PREC_FP32 = 0,        /* one FP32 accumulator per point (KTT's kernel) */
+    COUL_PREC_COMPENSATED = 1, /* FP32 partial per atom sub-tile, merged by two-sum into (sum, error) */
+    COUL_PREC_FP64_MERGE = 2   /* FP32 partial per atom sub-tile, merged into an FP64 accumulator */
+};
+
+/*
+ * Tuning parameters of the forward kernel.  The names in brackets are the KTT
+ * tuning parameters of Examples/CoulombSum3d/CoulombSum3d.cpp:137-216 that
+ * map onto each field.
+ */
+typedef struct coul_tune {
+    int block_x;      /* threads per block along x             [WORK_GROUP_SIZE_X] */
+    int block_y;      /* threads per block along y             [WORK_GROUP_SIZE_Y] */
+    int z_iterations; /* grid points per thread along z         [Z_ITERATIONS] (3D); along y for 2D */
+    int x_points;     /* grid points per thread along x, stored as one float/float2/float4 vector
+                                                               [VECTOR_SIZE; OUTER_UNROLL_FACTOR in 2D] */
+    int unroll;       /* unroll of the atom loop; 0 and 1 mean none [INNER_UNROLL_FACTOR] */
+    int atom_source;  /* COUL_ATOMS_*                          [USE_CONSTANT_MEMORY] */
+    int precision;    /* COUL_PREC_* */
+    int rsqrt_soft;   /* of every 8 reciprocal square roots, how many run as FMA-pipe
+                         Newton iterations instead of on the MUFU unit (0 = all MUFU) */
+} coul_tune;
+
+typedef struct coul_grid {
+    int nx, ny, nz;    /* points along each axis (nz = 1 for a single slice) */
+    float spacing;     /* h, Angstrom */
+    float origin[3];   /* coordinate of point (0, 0, 0) */
+} coul_grid;
+
+typedef struct coul_ctx coul_ctx;
+
+/* ---- context ------------------------------------------------------------ */
+COUL_API int coul_ctx_create(int device, coul_ctx** ctx);
+COUL_API int coul_ctx_destroy(coul_ctx* ctx);
+/* Use an existing cudaStream_t (passed as void*); NULL selects the context's own stream. */
+COUL_API int coul_ctx_set_stream(coul_ctx* ctx, void* stream);
+COUL_API void* coul_ctx_get_stream(coul_ctx* ctx);
+/* Number of SMs and compute capability of the context's device. */
+COUL_API int coul_ctx_device_info(coul_ctx* ctx, int* sm_count, int* cc_major, int* cc_minor);
+/* Wait for the context's stream; returns COUL_ERR_TIMEOUT if a kernel reported a bounded-wait expiry. */
+COUL_API int coul_synchronize(coul_ctx* ctx);
+/* Duration in ms between the events bracketing the most recent forward/adjoint/batched call
+   (waits for it).  With several launches in one call the span covers all of them. */
+COUL_API int coul_elapsed_ms(coul_ctx* ctx, double* ms);
+/* Thread-local message for the last failing call on this thread ("" if none). */
+COUL_API const char* coul_last_error(void);
+COUL_API const char* coul_status_string(int status);
+
+/* ---- tuning parameters ---------------------------------------------------- */
+COUL_API void coul_tune_default(coul_tune* tune);
+/* COUL_OK if the configuration maps to a compiled kernel variant that fits the device. */
+COUL_API int coul_tune_supported(const coul_tune* tune);
+/* Number of compiled forward variants, and the i-th one (for the tuner's space checks): its
+   tuning fields (block shape left at the default), whether it is a 2D-slice variant, and whether
+   it reads the four-array atom layout. */
+COUL_API int coul_variant_count(void);
+COUL_API int coul_variant_get(int i, coul_tune* tune, int* is_2d, int* is_soa);
+
+/* ---- forward: potential map -------------------------------------------------- */
+/*
+ * 3D map on a regular grid.  accumulate = 0 writes out = V; accumulate = 1
+ * adds (out += V, KTT's kernel semantics: the grid is zeroed by the caller).
+ */
+COUL_API int coul_forward_3d(coul_ctx* ctx, const float* d_atoms, int64_t n_atoms, const coul_grid* grid,
+                             const coul_tune* tune, int accumulate, float* d_out);
+/* Same with the atom coordinates and charges in four separate arrays. */
+COUL_API int coul_forward_3d_soa(coul_ctx* ctx, const float* d_x, const float* d_y, const float* d_z,
+                                 const float* d_q, int64_t n_atoms, const coul_grid* grid, const coul_tune* tune,
+                                 int accumulate, float* d_out);
+/*
+ * One grid point per thread, atoms read straight from global memory, FP32
+ * accumulation: the semantics of KTT's reference kernel (out += V).  Kept as
+ * a cross-check and as the "plain launch" baseline of the tuner.
+ */
+COUL_API int coul_forward_3d_reference(coul_ctx* ctx, const float* d_atoms, int64_t n_atoms,
+                                       const coul_grid* grid, int accumulate, float* d_out);
+/*
+ * 2D slice in KTT's 2D argument convention: d_atoms holds (x, y, dz2, q) with
+ * dz2 the squared z distance of the atom to the slice.  out[j*nx + i] over an
+ * nx * ny slice with spacing h and zero origin.  tune->z_iterations is the
+ * register block along y, tune->x_points along x.
+ */
+COUL_API int coul_forward_2d(coul_ctx* ctx, const float* d_atoms_xy_dz2_q, int64_t n_atoms, float spacing, int nx,
+                             int ny, const coul_tune* tune, int accumulate, float* d_out);
+/* Convert (x, y, z, q) atoms into the 2D convention (x, y, (z_slice - z)^2, q) on the device. */
+COUL_API int coul_slice_atoms(coul_ctx* ctx, const float* d_xyzq, int64_t n_atoms, float z_slice,
+                              float* d_xy_dz2_q);
+/*
+ * Host-buffer convenience call: uploads h_atoms, computes the 3D map (out = V)
+ * and downloads it into h_out, then waits.  Device buffers are cached in the
+ * context and grown on demand.
+ */
+COUL_API int coul_forward_3d_host(coul_ctx* ctx, const float* h_atoms, int64_t n_atoms, const coul_grid* grid,
+                                  const coul_tune* tune, float* h_out);
+
+/* ---- roofline ------------------------------------------------------------------ */
+/*
+ * Measures, on the context's device at its current clocks, the whole-GPU rate of MUFU reciprocal
+ * square roots and of FP32 FMAs (operations per second) with two throughput microkernels.  The
+ * pair-evaluation rooflines follow from them: all-MUFU R_mufu = rsqrt_per_s; with a share of the
+ * rsqrts moved to the FMA pipe at s issue slots each, R_comb = rsqrt_per_s * (F/M - 1 + s) / (2 + s)
+ * with F/M = ffma_per_s / rsqrt_per_s.  (KTT reads pipe utilisation from CUPTI instead:
+ * Source/ComputeEngine/Cuda/Cupti/CuptiMetricInterface.cpp:621-660.)
+ */
+COUL_API int coul_measure_pipe_rates(coul_ctx* ctx, double* rsqrt_per_s, double* ffma_per_s);
+
+/* ---- failure detection ------------------------------------------------------ */
+/*
+ * Runs one CTA that waits on an mbarrier with the given budget (at most 2 s).  With arrive != 0
+ * the barrier completes and the call returns COUL_OK; with arrive == 0 nothing arrives, the
+ * bounded wait expires, the kernel records the expiry in the context's status word and exits, and
+ * the call returns COUL_ERR_TIMEOUT with the context still usable.  This exercises the same
+ * bounded-wait and status path every kernel of the library uses (KTT has no counterpart: its
+ * failures surface as ResultStatus::ComputationFailed, Source/Api/Output/ResultStatus.h:12-33).
+ */
+COUL_API int coul_probe_bounded_wait(coul_ctx* ctx, int arrive, uint64_t budget_ns);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* COULKTT_H */

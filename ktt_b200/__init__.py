@@ -1,0 +1,307 @@
+"""ktt_b200 -- B200-native direct Coulomb summation behind a KTT-compatible surface.
+
+Python binding of the C ABI in ``include/coulktt.h`` (``libcoulktt.so``,
+built by ``python -m ktt_b200.build``).  Tensors are PyTorch CUDA tensors;
+PyTorch provides device memory and streams only -- every computation runs in
+the library's own sm_100a kernels.  There is no CPU fallback: if the library
+or a B200 is missing, the calls raise.
+
+The C++ ``ktt::Tuner`` surface (``include/Ktt.h``, ``libktt_b200.so``) is
+the drop-in for KTT host programs; this module is the drop-in for KTT's
+Python examples (``Examples/CoulombSum2d/CoulombSum2d.py``) at the level of
+the kernel call, and hosts the ``torch.autograd.Function`` of the adjoint.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field, fields
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libcoulktt.so")
+
+COUL_OK = 0
+COUL_ERR_INVALID_ARGUMENT = 1
+COUL_ERR_CUDA = 2
+COUL_ERR_UNSUPPORTED = 3
+COUL_ERR_DEVICE_LIMITS = 4
+COUL_ERR_TIMEOUT = 5
+COUL_ERR_NO_DEVICE = 6
+COUL_ERR_OUT_OF_MEMORY = 7
+
+ATOMS_SHARED_TMA = 0
+ATOMS_CONSTANT = 1
+PREC_FP32 = 0
+PREC_COMPENSATED = 1
+PREC_FP64_MERGE = 2
+
+
+class CoulombError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"[{status}] {message}")
+        self.status = status
+
+
+class _Tune(ctypes.Structure):
+    _fields_ = [("block_x", ctypes.c_int), ("block_y", ctypes.c_int), ("z_iterations", ctypes.c_int),
+                ("x_points", ctypes.c_int), ("unroll", ctypes.c_int), ("atom_source", ctypes.c_int),
+                ("precision", ctypes.c_int), ("rsqrt_soft", ctypes.c_int)]
+
+
+class _Grid(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int), ("spacing", ctypes.c_float),
+                ("origin", ctypes.c_float * 3)]
+
+
+@dataclass
+class Tune:
+    """Forward-kernel configuration; field names follow coul_tune (KTT parameter in brackets).
+
+    block_x [WORK_GROUP_SIZE_X], block_y [WORK_GROUP_SIZE_Y], z_iterations [Z_ITERATIONS],
+    x_points [VECTOR_SIZE / OUTER_UNROLL_FACTOR], unroll [INNER_UNROLL_FACTOR],
+    atom_source [USE_CONSTANT_MEMORY], precision, rsqrt_soft.
+    """
+    block_x: int = 32
+    block_y: int = 4
+    z_iterations: int = 16
+    x_points: int = 4
+    unroll: int = 1
+    atom_source: int = ATOMS_SHARED_TMA
+    precision: int = PREC_FP32
+    rsqrt_soft: int = 0
+
+    def c(self) -> _Tune:
+        return _Tune(*(int(getattr(self, f.name)) for f in fields(self)))
+
+    def as_dict(self) -> dict:
+        return {f.name: int(getattr(self, f.name)) for f in fields(self)}
+
+
+_lib = None
+
+
+def library_path() -> str:
+    return LIB_PATH
+
+
+def load_library():
+    """Load libcoulktt.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise CoulombError(COUL_ERR_NO_DEVICE, f"{LIB_PATH} is missing; run `python -m ktt_b200.build`")
+    lib = ctypes.CDLL(LIB_PATH)
+    vp, i64, ci, cf = ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_float
+    T, G = ctypes.POINTER(_Tune), ctypes.POINTER(_Grid)
+    sig = {
+        "coul_ctx_create": [ci, ctypes.POINTER(vp)],
+        "coul_ctx_destroy": [vp],
+        "coul_ctx_set_stream": [vp, vp],
+        "coul_ctx_device_info": [vp, ctypes.POINTER(ci), ctypes.POINTER(ci), ctypes.POINTER(ci)],
+        "coul_synchronize": [vp],
+        "coul_elapsed_ms": [vp, ctypes.POINTER(ctypes.c_double)],
+        "coul_tune_supported": [T],
+        "coul_variant_count": [],
+        "coul_variant_get": [ci, T, ctypes.POINTER(ci), ctypes.POINTER(ci)],
+        "coul_forward_3d": [vp, vp, i64, G, T, ci, vp],
+        "coul_forward_3d_soa": [vp, vp, vp, vp, vp, i64, G, T, ci, vp],
+        "coul_forward_3d_reference": [vp, vp, i64, G, ci, vp],
+        "coul_forward_2d": [vp, vp, i64, cf, ci, ci, T, ci, vp],
+        "coul_slice_atoms": [vp, vp, i64, cf, vp],
+        "coul_forward_3d_host": [vp, vp, i64, G, T, vp],
+        "coul_probe_bounded_wait": [vp, ci, ctypes.c_uint64],
+        "coul_measure_pipe_rates": [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)],
+    }
+    for name, args in sig.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = ci
+    lib.coul_ctx_get_stream.argtypes = [vp]
+    lib.coul_ctx_get_stream.restype = vp
+    lib.coul_last_error.restype = ctypes.c_char_p
+    lib.coul_status_string.argtypes = [ci]
+    lib.coul_status_string.restype = ctypes.c_char_p
+    lib.coul_tune_default.argtypes = [T]
+    lib.coul_tune_default.restype = None
+    _register_optional(lib)
+    _lib = lib
+    return lib
+
+
+def _register_optional(lib) -> None:
+    """Signatures of entry points added by later units (batched, adjoint, ...)."""
+    try:
+        from . import _signatures  # noqa: F401
+        _signatures.register(lib)
+    except ImportError:
+        pass
+
+
+def _check(rc: int) -> None:
+    if rc != COUL_OK:
+        msg = _lib.coul_last_error().decode(errors="replace") if _lib is not None else ""
+        raise CoulombError(rc, msg or "error")
+
+
+def variants() -> list[tuple[Tune, bool, bool]]:
+    """All compiled forward variants as (tune, is_2d, is_soa)."""
+    lib = load_library()
+    out = []
+    for i in range(lib.coul_variant_count()):
+        t = _Tune()
+        d2, soa = ctypes.c_int(), ctypes.c_int()
+        _check(lib.coul_variant_get(i, ctypes.byref(t), ctypes.byref(d2), ctypes.byref(soa)))
+        out.append((Tune(*(getattr(t, n) for n, _ in _Tune._fields_)), bool(d2.value), bool(soa.value)))
+    return out
+
+
+def tune_supported(tune: Tune) -> bool:
+    lib = load_library()
+    return lib.coul_tune_supported(ctypes.byref(tune.c())) == COUL_OK
+
+
+def _grid(dims, spacing, origin) -> _Grid:
+    nx, ny, nz = (int(d) for d in dims)
+    o = (0.0, 0.0, 0.0) if origin is None else tuple(float(v) for v in origin)
+    return _Grid(nx, ny, nz, float(spacing), (ctypes.c_float * 3)(*o))
+
+
+def _ptr(t) -> int:
+    return int(t.data_ptr())
+
+
+class CoulombContext:
+    """One CUDA device; calls are enqueued on PyTorch's current stream of that device."""
+
+    def __init__(self, device: int = 0):
+        self._lib = load_library()
+        self._ctx = ctypes.c_void_p()
+        _check(self._lib.coul_ctx_create(int(device), ctypes.byref(self._ctx)))
+        self.device = int(device)
+        sm, ma, mi = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(self._lib.coul_ctx_device_info(self._ctx, ctypes.byref(sm), ctypes.byref(ma), ctypes.byref(mi)))
+        self.sm_count, self.cc = sm.value, (ma.value, mi.value)
+
+    # -- plumbing ---------------------------------------------------------------------------
+    def close(self) -> None:
+        if self._ctx:
+            self._lib.coul_ctx_destroy(self._ctx)
+            self._ctx = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._ctx
+
+    def _bind_stream(self) -> None:
+        import torch
+        s = torch.cuda.current_stream(self.device)
+        _check(self._lib.coul_ctx_set_stream(self._ctx, ctypes.c_void_p(s.cuda_stream)))
+
+    def probe_bounded_wait(self, arrive: bool, budget_ns: int) -> int:
+        """Status of the bounded-wait self-test kernel (COUL_OK, or COUL_ERR_TIMEOUT when nothing arrives)."""
+        return int(self._lib.coul_probe_bounded_wait(self._ctx, 1 if arrive else 0, int(budget_ns)))
+
+    def pipe_rates(self) -> tuple[float, float]:
+        """(MUFU rsqrt/s, FP32 FMA/s) of the whole GPU, measured now by throughput microkernels."""
+        m, f = ctypes.c_double(), ctypes.c_double()
+        _check(self._lib.coul_measure_pipe_rates(self._ctx, ctypes.byref(m), ctypes.byref(f)))
+        return m.value, f.value
+
+    def synchronize(self) -> None:
+        _check(self._lib.coul_synchronize(self._ctx))
+
+    def elapsed_ms(self) -> float:
+        ms = ctypes.c_double()
+        _check(self._lib.coul_elapsed_ms(self._ctx, ctypes.byref(ms)))
+        return ms.value
+
+    @staticmethod
+    def _check_atoms(atoms, cols: int = 4):
+        import torch
+        if not (isinstance(atoms, torch.Tensor) and atoms.is_cuda and atoms.dtype == torch.float32):
+            raise CoulombError(COUL_ERR_INVALID_ARGUMENT, "atoms must be a float32 CUDA tensor")
+        if atoms.dim() != 2 or atoms.shape[1] != cols or not atoms.is_contiguous():
+            raise CoulombError(COUL_ERR_INVALID_ARGUMENT, f"atoms must be a contiguous (n, {cols}) tensor")
+
+    @staticmethod
+    def _out(out, shape, device):
+        import torch
+        if out is None:
+            return torch.empty(shape, dtype=torch.float32, device=device)
+        if tuple(out.shape) != tuple(shape) or out.dtype != torch.float32 or not out.is_contiguous():
+            raise CoulombError(COUL_ERR_INVALID_ARGUMENT, f"out must be a contiguous float32 tensor of shape {shape}")
+        return out
+
+    # -- forward ------------------------------------------------------------------------------
+    def forward_3d(self, atoms, dims, spacing, origin=None, tune: Tune | None = None, out=None,
+                   accumulate: bool = False):
+        """Map of shape (nz, ny, nx) for dims = (nx, ny, nz)."""
+        self._check_atoms(atoms)
+        nx, ny, nz = (int(d) for d in dims)
+        out = self._out(out, (nz, ny, nx), atoms.device)
+        self._bind_stream()
+        g = _grid(dims, spacing, origin)
+        t = (tune or Tune()).c()
+        _check(self._lib.coul_forward_3d(self._ctx, _ptr(atoms), atoms.shape[0], ctypes.byref(g), ctypes.byref(t),
+                                         1 if accumulate else 0, _ptr(out)))
+        return out
+
+    def forward_3d_soa(self, x, y, z, q, dims, spacing, origin=None, tune: Tune | None = None, out=None,
+                       accumulate: bool = False):
+        nx, ny, nz = (int(d) for d in dims)
+        out = self._out(out, (nz, ny, nx), x.device)
+        self._bind_stream()
+        g = _grid(dims, spacing, origin)
+        t = (tune or Tune()).c()
+        _check(self._lib.coul_forward_3d_soa(self._ctx, _ptr(x), _ptr(y), _ptr(z), _ptr(q), x.shape[0],
+                                             ctypes.byref(g), ctypes.byref(t), 1 if accumulate else 0, _ptr(out)))
+        return out
+
+    def forward_3d_reference(self, atoms, dims, spacing, origin=None, out=None, accumulate: bool = False):
+        self._check_atoms(atoms)
+        nx, ny, nz = (int(d) for d in dims)
+        out = self._out(out, (nz, ny, nx), atoms.device)
+        self._bind_stream()
+        g = _grid(dims, spacing, origin)
+        _check(self._lib.coul_forward_3d_reference(self._ctx, _ptr(atoms), atoms.shape[0], ctypes.byref(g),
+                                                   1 if accumulate else 0, _ptr(out)))
+        return out
+
+    def forward_2d(self, atoms_xy_dz2_q, spacing, nx, ny, tune: Tune | None = None, out=None,
+                   accumulate: bool = False):
+        """Slice of shape (ny, nx) in KTT's 2D convention (atom column 2 holds dz^2)."""
+        self._check_atoms(atoms_xy_dz2_q)
+        out = self._out(out, (int(ny), int(nx)), atoms_xy_dz2_q.device)
+        self._bind_stream()
+        t = (tune or Tune(block_x=32, block_y=4, z_iterations=4, x_points=4)).c()
+        _check(self._lib.coul_forward_2d(self._ctx, _ptr(atoms_xy_dz2_q), atoms_xy_dz2_q.shape[0], float(spacing),
+                                         int(nx), int(ny), ctypes.byref(t), 1 if accumulate else 0, _ptr(out)))
+        return out
+
+    def slice_atoms(self, atoms, z_slice: float, out=None):
+        import torch
+        self._check_atoms(atoms)
+        out = torch.empty_like(atoms) if out is None else out
+        self._bind_stream()
+        _check(self._lib.coul_slice_atoms(self._ctx, _ptr(atoms), atoms.shape[0], float(z_slice), _ptr(out)))
+        return out
+
+    def forward_3d_host(self, atoms_np, dims, spacing, origin=None, tune: Tune | None = None, out_np=None):
+        """Host (numpy) buffers in and out; copies are part of the call (KTT Tuner::Run semantics)."""
+        import numpy as np
+        a = np.ascontiguousarray(np.asarray(atoms_np, dtype=np.float32).reshape(-1, 4))
+        nx, ny, nz = (int(d) for d in dims)
+        out = np.empty((nz, ny, nx), dtype=np.float32) if out_np is None else out_np
+        assert out.flags.c_contiguous and out.dtype == np.float32 and out.size == nx * ny * nz
+        g = _grid(dims, spacing, origin)
+        t = (tune or Tune()).c()
+        _check(self._lib.coul_forward_3d_host(self._ctx, a.ctypes.data, a.shape[0], ctypes.byref(g), ctypes.byref(t),
+                                              out.ctypes.data))
+        return out

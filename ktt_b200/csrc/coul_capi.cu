@@ -1,0 +1,620 @@
+// coul_capi.cu -- the C ABI of libcoulktt.so (declared in include/coulktt.h).
+//
+// Replaces, for the Coulomb path, what KTT's CUDA compute engine does per run: context and stream
+// set-up (Source/ComputeEngine/Cuda/CudaEngine.cpp:29-60), pre-launch limit checks
+// (CudaEngine.cpp:117-138), the event-bracketed launch (Source/ComputeEngine/Cuda/CudaKernel.cpp:43-70)
+// and the event timing (Source/ComputeEngine/Cuda/CudaEvent.cpp:30-36).  Instead of JIT-compiling
+// the kernel source with #define prefixes through NVRTC, a configuration selects one of the
+// ahead-of-time compiled sm_100a variants registered by the coul_fwd_*.cu translation units.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "coul_forward.cuh"
+#include "coulktt.h"
+#include "coul_internal.h"
+
+using namespace coul;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+std::vector<VariantEntry>& registry()
+{
+    static std::vector<VariantEntry> v;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        register_fwd_3d_aos(v);
+        register_fwd_3d_aos_z32(v);
+        register_fwd_3d_soa(v);
+        register_fwd_3d_const(v);
+        register_fwd_3d_precise(v);
+        register_fwd_3d_soft(v);
+        register_fwd_2d(v);
+    });
+    return v;
+}
+
+const VariantEntry* find_variant(const VariantKey& k)
+{
+    for (const auto& e : registry())
+        if (e.key == k)
+            return &e;
+    return nullptr;
+}
+
+// ---- reference kernel: KTT's directCoulombSumReference semantics (one point per thread, atoms
+// from global memory, FP32 accumulation, out += V), Examples/CoulombSum3d/CoulombSum3dReference.cu:1-28.
+__global__ void reference_kernel(const float4* __restrict__ atoms, int64_t n, int nx, int ny, int nz, float h,
+                                 float ox, float oy, float oz, int accumulate, float* __restrict__ out)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x >= nx || y >= ny || z >= nz)
+        return;
+    const float gx = fmaf(static_cast<float>(x), h, ox);
+    const float gy = fmaf(static_cast<float>(y), h, oy);
+    const float gz = fmaf(static_cast<float>(z), h, oz);
+    float e = 0.0f;
+    for (int64_t j = 0; j < n; ++j) {
+        const float4 a = atoms[j];
+        const float dx = gx - a.x, dy = gy - a.y, dz = gz - a.z;
+        e = fmaf(a.w, rsqrt_mufu(fmaf(dz, dz, fmaf(dy, dy, dx * dx))), e);
+    }
+    const int64_t o = (static_cast<int64_t>(z) * ny + y) * nx + x;
+    out[o] = accumulate ? out[o] + e : e;
+}
+
+// (x, y, z, q) -> (x, y, (z_slice - z)^2, q): KTT's 2D convention, computed on the device
+// (the iterative example does it on the host per slice: CoulombSum3dIterative.cpp:160-179).
+__global__ void slice_atoms_kernel(const float4* __restrict__ in, int64_t n, float zs, float4* __restrict__ out)
+{
+    const int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (j >= n)
+        return;
+    const float4 a = in[j];
+    const float dz = zs - a.z;
+    out[j] = make_float4(a.x, a.y, dz * dz, a.w);
+}
+
+// Self-test of the bounded-wait machinery: one CTA arms an mbarrier for one arrival and waits on
+// it with a short budget.  With arrive != 0 the arrival happens and the wait succeeds; with
+// arrive == 0 nothing ever arrives, the wait expires, and the kernel records kStatusTimeout in the
+// context's status word and returns -- the host then sees COUL_ERR_TIMEOUT.
+__global__ void probe_wait_kernel(int arrive, uint64_t budget_ns, int* status)
+{
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (arrive && threadIdx.x == 0)
+        mbar_arrive_expect_tx(&bar, 0);
+    const bool ok = mbar_wait_bounded(&bar, 0, budget_ns);
+    if (__syncthreads_or(ok ? 0 : 1) && threadIdx.x == 0)
+        report_status(status, kStatusTimeout);
+}
+
+}  // namespace
+
+// struct coul_ctx is defined in coul_internal.h (shared with the batched and adjoint units).
+
+
+namespace coul {
+
+int set_error(int status, const std::string& msg)
+{
+    g_last_error = msg;
+    return status;
+}
+
+int cuda_error(cudaError_t e, const char* what)
+{
+    return set_error(COUL_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+int ctx_activate(coul_ctx* ctx)
+{
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess)
+        return cuda_error(e, "cudaSetDevice");
+    return COUL_OK;
+}
+
+
+int ctx_begin_timing(coul_ctx* ctx)
+{
+    cudaError_t e = cudaEventRecord(ctx->ev_start, ctx->stream);
+    if (e != cudaSuccess)
+        return cuda_error(e, "cudaEventRecord");
+    return COUL_OK;
+}
+
+int ctx_end_timing(coul_ctx* ctx)
+{
+    cudaError_t e = cudaEventRecord(ctx->ev_stop, ctx->stream);
+    if (e != cudaSuccess)
+        return cuda_error(e, "cudaEventRecord");
+    ctx->have_timing = true;
+    return COUL_OK;
+}
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+int validate_tune(const coul_tune* t, int mode, int soa, const VariantEntry** out)
+{
+    if (t == nullptr)
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "tune is NULL");
+    const int threads = t->block_x * t->block_y;
+    if (t->block_x < 1 || t->block_y < 1 || threads > kMaxThreads)
+        return set_error(COUL_ERR_DEVICE_LIMITS, "block " + std::to_string(t->block_x) + "x" +
+                                                     std::to_string(t->block_y) + " is outside 1.." +
+                                                     std::to_string(kMaxThreads) + " threads");
+    if (t->atom_source != COUL_ATOMS_SHARED_TMA && t->atom_source != COUL_ATOMS_CONSTANT)
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "unknown atom_source");
+    if (t->precision < COUL_PREC_FP32 || t->precision > COUL_PREC_FP64_MERGE)
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "unknown precision");
+    if (t->rsqrt_soft < 0 || t->rsqrt_soft > 8)
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "rsqrt_soft must be in 0..8");
+    const int unroll = t->unroll <= 1 ? 1 : t->unroll;
+    const VariantKey key{t->z_iterations, t->x_points, unroll, t->atom_source, soa, t->precision, t->rsqrt_soft, mode};
+    const VariantEntry* e = find_variant(key);
+    if (e == nullptr) {
+        char buf[256];
+        std::snprintf(buf, sizeof buf,
+                      "no compiled variant for z_iterations=%d x_points=%d unroll=%d atom_source=%d soa=%d "
+                      "precision=%d rsqrt_soft=%d mode=%s",
+                      t->z_iterations, t->x_points, unroll, t->atom_source, soa, t->precision, t->rsqrt_soft,
+                      mode == kModeGrid3d ? "3d" : "2d");
+        return set_error(COUL_ERR_UNSUPPORTED, buf);
+    }
+    if (out)
+        *out = e;
+    return COUL_OK;
+}
+
+int validate_grid(const coul_grid* g)
+{
+    if (g == nullptr)
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "grid is NULL");
+    if (g->nx < 1 || g->ny < 1 || g->nz < 1)
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "grid dimensions must be positive");
+    if (!std::isfinite(g->spacing) || !std::isfinite(g->origin[0]) || !std::isfinite(g->origin[1]) ||
+        !std::isfinite(g->origin[2]))
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "grid spacing and origin must be finite");
+    return COUL_OK;
+}
+
+// Launch one forward variant over a grid; shared by the 3D AoS/SoA and 2D entry points and by
+// the batched path's plain-launch baseline.
+int launch_forward(coul_ctx* ctx, const VariantEntry* v, const FwdParams& prm, int mode, const coul_tune* t)
+{
+    FwdLaunch L{};
+    L.p = prm;
+    L.p.status = ctx->d_status;
+    L.block = dim3(static_cast<unsigned>(t->block_x), static_cast<unsigned>(t->block_y), 1);
+    const int64_t bx = static_cast<int64_t>(t->block_x) * t->x_points;
+    const int64_t gx = (prm.nx + bx - 1) / bx;
+    int64_t gy, gz;
+    if (mode == kModeGrid3d) {
+        gy = (prm.ny + t->block_y - 1) / t->block_y;
+        gz = (prm.nz + t->z_iterations - 1) / t->z_iterations;
+    } else {
+        const int64_t by = static_cast<int64_t>(t->block_y) * t->z_iterations;
+        gy = (prm.ny + by - 1) / by;
+        gz = 1;
+    }
+    if (gx > 2147483647LL || gy > 65535 || gz > 65535)
+        return set_error(COUL_ERR_DEVICE_LIMITS, "grid too large for one launch");
+    L.grid = dim3(static_cast<unsigned>(gx), static_cast<unsigned>(gy), static_cast<unsigned>(gz));
+    L.smem = (t->atom_source == COUL_ATOMS_SHARED_TMA) ? (kStages * kTileAtoms * 16 + kStages * 8) : 0;
+    const int xp = t->x_points;
+    L.vec_store = (xp > 1 && prm.nx % xp == 0 &&
+                   (reinterpret_cast<uintptr_t>(prm.out) % (sizeof(float) * (xp >= 4 ? 4 : xp))) == 0)
+                      ? 1
+                      : 0;
+    cudaError_t e = v->launch(L, ctx->stream);
+    if (e != cudaSuccess)
+        return cuda_error(e, "forward launch");
+    return COUL_OK;
+}
+
+}  // namespace coul
+
+extern "C" {
+
+COUL_API const char* coul_last_error(void) { return g_last_error.c_str(); }
+
+COUL_API const char* coul_status_string(int status)
+{
+    switch (status) {
+    case COUL_OK: return "ok";
+    case COUL_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case COUL_ERR_CUDA: return "CUDA error";
+    case COUL_ERR_UNSUPPORTED: return "unsupported configuration";
+    case COUL_ERR_DEVICE_LIMITS: return "device limits exceeded";
+    case COUL_ERR_TIMEOUT: return "device-side wait timed out";
+    case COUL_ERR_NO_DEVICE: return "no suitable device";
+    case COUL_ERR_OUT_OF_MEMORY: return "out of memory";
+    default: return "unknown status";
+    }
+}
+
+COUL_API int coul_ctx_create(int device, coul_ctx** out)
+{
+    if (out == nullptr)
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "ctx output pointer is NULL");
+    *out = nullptr;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0)
+        return set_error(COUL_ERR_NO_DEVICE, std::string("no CUDA device: ") +
+                                                 (e != cudaSuccess ? cudaGetErrorString(e) : "count is 0"));
+    if (device < 0 || device >= count)
+        return set_error(COUL_ERR_NO_DEVICE, "device index out of range");
+    cudaDeviceProp prop{};
+    e = cudaGetDeviceProperties(&prop, device);
+    if (e != cudaSuccess)
+        return cuda_error(e, "cudaGetDeviceProperties");
+    if (prop.major != 10 || prop.minor != 0)
+        return set_error(COUL_ERR_NO_DEVICE, std::string("libcoulktt is built for sm_100a only; device is ") +
+                                                 prop.name + " (sm_" + std::to_string(prop.major) +
+                                                 std::to_string(prop.minor) + ")");
+    e = cudaSetDevice(device);
+    if (e != cudaSuccess)
+        return cuda_error(e, "cudaSetDevice");
+    auto* ctx = new coul_ctx();
+    ctx->device = device;
+    ctx->sm_count = prop.multiProcessorCount;
+    ctx->cc_major = prop.major;
+    ctx->cc_minor = prop.minor;
+    if ((e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreate(&ctx->ev_start)) != cudaSuccess || (e = cudaEventCreate(&ctx->ev_stop)) != cudaSuccess ||
+        (e = cudaMalloc(&ctx->d_status, sizeof(int))) != cudaSuccess ||
+        (e = cudaMemset(ctx->d_status, 0, sizeof(int))) != cudaSuccess) {
+        const int rc = cuda_error(e, "context set-up");
+        coul_ctx_destroy(ctx);
+        return rc;
+    }
+    ctx->stream = ctx->own_stream;
+    (void)registry();
+    *out = ctx;
+    return COUL_OK;
+}
+
+COUL_API int coul_ctx_destroy(coul_ctx* ctx)
+{
+    if (ctx == nullptr)
+        return COUL_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream)
+        cudaStreamSynchronize(ctx->stream);
+    if (ctx->d_atoms_cache)
+        cudaFree(ctx->d_atoms_cache);
+    if (ctx->d_out_cache)
+        cudaFree(ctx->d_out_cache);
+    if (ctx->d_status)
+        cudaFree(ctx->d_status);
+    if (ctx->ev_start)
+        cudaEventDestroy(ctx->ev_start);
+    if (ctx->ev_stop)
+        cudaEventDestroy(ctx->ev_stop);
+    if (ctx->own_stream)
+        cudaStreamDestroy(ctx->own_stream);
+    for (auto& f : ctx->cleanups)
+        f();
+    delete ctx;
+    return COUL_OK;
+}
+
+COUL_API int coul_ctx_set_stream(coul_ctx* ctx, void* stream)
+{
+    if (ctx == nullptr)
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
+    return COUL_OK;
+}
+
+COUL_API void* coul_ctx_get_stream(coul_ctx* ctx) { return ctx ? static_cast<void*>(ctx->stream) : nullptr; }
+
+COUL_API int coul_ctx_device_info(coul_ctx* ctx, int* sm_count, int* cc_major, int* cc_minor)
+{
+    if (ctx == nullptr)
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    if (sm_count)
+        *sm_count = ctx->sm_count;
+    if (cc_major)
+        *cc_major = ctx->cc_major;
+    if (cc_minor)
+        *cc_minor = ctx->cc_minor;
+    return COUL_OK;
+}
+
+COUL_API int coul_synchronize(coul_ctx* ctx)
+{
+    if (ctx == nullptr)
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    int rc = ctx_activate(ctx);
+    if (rc)
+        return rc;
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess)
+        return cuda_error(e, "cudaStreamSynchronize");
+    int status = 0;
+    e = cudaMemcpy(&status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess)
+        return cuda_error(e, "status read-back");
+    if (status != kStatusOk) {
+        cudaMemset(ctx->d_status, 0, sizeof(int));
+        return set_error(COUL_ERR_TIMEOUT, "a kernel gave up on a bounded wait (status " + std::to_string(status) +
+                                               "); its output is invalid");
+    }
+    return COUL_OK;
+}
+
+COUL_API int coul_elapsed_ms(coul_ctx* ctx, double* ms)
+{
+    if (ctx == nullptr || ms == nullptr)
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "ctx or ms is NULL");
+    if (!ctx->have_timing)
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "no timed call yet");
+    cudaError_t e = cudaEventSynchronize(ctx->ev_stop);
+    if (e != cudaSuccess)
+        return cuda_error(e, "cudaEventSynchronize");
+    float f = 0.0f;
+    e = cudaEventElapsedTime(&f, ctx->ev_start, ctx->ev_stop);
+    if (e != cudaSuccess)
+        return cuda_error(e, "cudaEventElapsedTime");
+    *ms = static_cast<double>(f);
+    return COUL_OK;
+}
+
+COUL_API void coul_tune_default(coul_tune* t)
+{
+    if (t == nullptr)
+        return;
+    t->block_x = 32;
+    t->block_y = 4;
+    t->z_iterations = 16;
+    t->x_points = 4;
+    t->unroll = 1;
+    t->atom_source = COUL_ATOMS_SHARED_TMA;
+    t->precision = COUL_PREC_FP32;
+    t->rsqrt_soft = 0;
+}
+
+COUL_API int coul_tune_supported(const coul_tune* t) { return validate_tune(t, kModeGrid3d, 0, nullptr); }
+
+COUL_API int coul_variant_count(void) { return static_cast<int>(registry().size()); }
+
+COUL_API int coul_variant_get(int i, coul_tune* t, int* is_2d, int* is_soa)
+{
+    if (t == nullptr || i < 0 || i >= static_cast<int>(registry().size()))
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "variant index out of range");
+    const VariantKey& k = registry()[static_cast<size_t>(i)].key;
+    coul_tune_default(t);
+    t->z_iterations = k.zi;
+    t->x_points = k.xp;
+    t->unroll = k.unroll;
+    t->atom_source = k.src;
+    t->precision = k.prec;
+    t->rsqrt_soft = k.soft;
+    if (is_2d)
+        *is_2d = k.mode == kModeSlice2d ? 1 : 0;
+    if (is_soa)
+        *is_soa = k.soa;
+    return COUL_OK;
+}
+
+static int forward_3d_common(coul_ctx* ctx, const float* d_atoms, const float* d_x, const float* d_y,
+                             const float* d_z, const float* d_q, int soa, int64_t n_atoms, const coul_grid* grid,
+                             const coul_tune* tune, int accumulate, float* d_out)
+{
+    if (ctx == nullptr)
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    int rc = validate_grid(grid);
+    if (rc)
+        return rc;
+    const VariantEntry* v = nullptr;
+    if ((rc = validate_tune(tune, kModeGrid3d, soa, &v)))
+        return rc;
+    if (n_atoms < 0)
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "negative atom count");
+    if (d_out == nullptr)
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "output pointer is NULL");
+    if (n_atoms > 0) {
+        if (!soa && (d_atoms == nullptr || !aligned16(d_atoms)))
+            return set_error(COUL_ERR_INVALID_ARGUMENT, "atoms must be a non-NULL, 16-byte aligned float4 array");
+        if (soa && (!d_x || !d_y || !d_z || !d_q || !aligned16(d_x) || !aligned16(d_y) || !aligned16(d_z) ||
+                    !aligned16(d_q)))
+            return set_error(COUL_ERR_INVALID_ARGUMENT, "SoA atom arrays must be non-NULL and 16-byte aligned");
+    }
+    if ((rc = ctx_activate(ctx)))
+        return rc;
+    FwdParams p{};
+    p.atoms = reinterpret_cast<const float4*>(d_atoms);
+    p.sx = d_x;
+    p.sy = d_y;
+    p.sz = d_z;
+    p.sq = d_q;
+    p.n_atoms = n_atoms;
+    p.nx = grid->nx;
+    p.ny = grid->ny;
+    p.nz = grid->nz;
+    p.h = grid->spacing;
+    p.ox = grid->origin[0];
+    p.oy = grid->origin[1];
+    p.oz = grid->origin[2];
+    p.out = d_out;
+    p.accumulate = accumulate ? 1 : 0;
+    if ((rc = ctx_begin_timing(ctx)))
+        return rc;
+    if ((rc = launch_forward(ctx, v, p, kModeGrid3d, tune)))
+        return rc;
+    return ctx_end_timing(ctx);
+}
+
+COUL_API int coul_forward_3d(coul_ctx* ctx, const float* d_atoms, int64_t n_atoms, const coul_grid* grid,
+                             const coul_tune* tune, int accumulate, float* d_out)
+{
+    return forward_3d_common(ctx, d_atoms, nullptr, nullptr, nullptr, nullptr, 0, n_atoms, grid, tune, accumulate,
+                             d_out);
+}
+
+COUL_API int coul_forward_3d_soa(coul_ctx* ctx, const float* d_x, const float* d_y, const float* d_z,
+                                 const float* d_q, int64_t n_atoms, const coul_grid* grid, const coul_tune* tune,
+                                 int accumulate, float* d_out)
+{
+    if (tune && tune->atom_source != COUL_ATOMS_SHARED_TMA)
+        return set_error(COUL_ERR_UNSUPPORTED, "the four-array atom layout is staged through shared memory only");
+    return forward_3d_common(ctx, nullptr, d_x, d_y, d_z, d_q, 1, n_atoms, grid, tune, accumulate, d_out);
+}
+
+COUL_API int coul_forward_3d_reference(coul_ctx* ctx, const float* d_atoms, int64_t n_atoms, const coul_grid* grid,
+                                       int accumulate, float* d_out)
+{
+    if (ctx == nullptr)
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    int rc = validate_grid(grid);
+    if (rc)
+        return rc;
+    if (n_atoms < 0 || d_out == nullptr || (n_atoms > 0 && (d_atoms == nullptr || !aligned16(d_atoms))))
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "bad atoms or output");
+    if (grid->nz > 65535)
+        return set_error(COUL_ERR_DEVICE_LIMITS, "nz above 65535");
+    if ((rc = ctx_activate(ctx)))
+        return rc;
+    const dim3 block(16, 16, 1);
+    const dim3 g((grid->nx + 15) / 16, (grid->ny + 15) / 16, grid->nz);
+    if ((rc = ctx_begin_timing(ctx)))
+        return rc;
+    reference_kernel<<<g, block, 0, ctx->stream>>>(reinterpret_cast<const float4*>(d_atoms), n_atoms, grid->nx,
+                                                   grid->ny, grid->nz, grid->spacing, grid->origin[0],
+                                                   grid->origin[1], grid->origin[2], accumulate ? 1 : 0, d_out);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess)
+        return cuda_error(e, "reference launch");
+    return ctx_end_timing(ctx);
+}
+
+COUL_API int coul_forward_2d(coul_ctx* ctx, const float* d_atoms, int64_t n_atoms, float spacing, int nx, int ny,
+                             const coul_tune* tune, int accumulate, float* d_out)
+{
+    if (ctx == nullptr)
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    coul_grid g{nx, ny, 1, spacing, {0.0f, 0.0f, 0.0f}};
+    int rc = validate_grid(&g);
+    if (rc)
+        return rc;
+    const VariantEntry* v = nullptr;
+    if ((rc = validate_tune(tune, kModeSlice2d, 0, &v)))
+        return rc;
+    if (n_atoms < 0 || d_out == nullptr || (n_atoms > 0 && (d_atoms == nullptr || !aligned16(d_atoms))))
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "bad atoms or output");
+    if ((rc = ctx_activate(ctx)))
+        return rc;
+    FwdParams p{};
+    p.atoms = reinterpret_cast<const float4*>(d_atoms);
+    p.n_atoms = n_atoms;
+    p.nx = nx;
+    p.ny = ny;
+    p.nz = 1;
+    p.h = spacing;
+    p.out = d_out;
+    p.accumulate = accumulate ? 1 : 0;
+    if ((rc = ctx_begin_timing(ctx)))
+        return rc;
+    if ((rc = launch_forward(ctx, v, p, kModeSlice2d, tune)))
+        return rc;
+    return ctx_end_timing(ctx);
+}
+
+COUL_API int coul_slice_atoms(coul_ctx* ctx, const float* d_xyzq, int64_t n_atoms, float z_slice, float* d_out)
+{
+    if (ctx == nullptr)
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    if (n_atoms < 0 || (n_atoms > 0 && (!d_xyzq || !d_out || !aligned16(d_xyzq) || !aligned16(d_out))))
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "bad atom arrays");
+    if (n_atoms == 0)
+        return COUL_OK;
+    int rc = ctx_activate(ctx);
+    if (rc)
+        return rc;
+    const int64_t blocks = (n_atoms + 255) / 256;
+    slice_atoms_kernel<<<static_cast<unsigned>(blocks), 256, 0, ctx->stream>>>(
+        reinterpret_cast<const float4*>(d_xyzq), n_atoms, z_slice, reinterpret_cast<float4*>(d_out));
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? COUL_OK : cuda_error(e, "slice launch");
+}
+
+COUL_API int coul_probe_bounded_wait(coul_ctx* ctx, int arrive, uint64_t budget_ns)
+{
+    if (ctx == nullptr)
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    if (budget_ns > 2000000000ull)
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "budget above 2 s");
+    int rc = ctx_activate(ctx);
+    if (rc)
+        return rc;
+    probe_wait_kernel<<<1, 32, 0, ctx->stream>>>(arrive ? 1 : 0, budget_ns, ctx->d_status);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess)
+        return cuda_error(e, "probe launch");
+    return coul_synchronize(ctx);
+}
+
+COUL_API int coul_forward_3d_host(coul_ctx* ctx, const float* h_atoms, int64_t n_atoms, const coul_grid* grid,
+                                  const coul_tune* tune, float* h_out)
+{
+    if (ctx == nullptr)
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    int rc = validate_grid(grid);
+    if (rc)
+        return rc;
+    if ((rc = validate_tune(tune, kModeGrid3d, 0, nullptr)))
+        return rc;
+    if (n_atoms < 0 || h_out == nullptr || (n_atoms > 0 && h_atoms == nullptr))
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "bad host buffers");
+    if ((rc = ctx_activate(ctx)))
+        return rc;
+    const size_t abytes = static_cast<size_t>(n_atoms) * 16;
+    const size_t obytes = static_cast<size_t>(grid->nx) * grid->ny * grid->nz * sizeof(float);
+    cudaError_t e;
+    if (abytes > ctx->atoms_cap) {
+        if (ctx->d_atoms_cache)
+            cudaFree(ctx->d_atoms_cache);
+        ctx->d_atoms_cache = nullptr;
+        ctx->atoms_cap = 0;
+        if ((e = cudaMalloc(&ctx->d_atoms_cache, abytes)) != cudaSuccess)
+            return set_error(COUL_ERR_OUT_OF_MEMORY, std::string("atom buffer: ") + cudaGetErrorString(e));
+        ctx->atoms_cap = abytes;
+    }
+    if (obytes > ctx->out_cap) {
+        if (ctx->d_out_cache)
+            cudaFree(ctx->d_out_cache);
+        ctx->d_out_cache = nullptr;
+        ctx->out_cap = 0;
+        if ((e = cudaMalloc(&ctx->d_out_cache, obytes)) != cudaSuccess)
+            return set_error(COUL_ERR_OUT_OF_MEMORY, std::string("map buffer: ") + cudaGetErrorString(e));
+        ctx->out_cap = obytes;
+    }
+    if (abytes > 0 &&
+        (e = cudaMemcpyAsync(ctx->d_atoms_cache, h_atoms, abytes, cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess)
+        return cuda_error(e, "atom upload");
+    if ((rc = coul_forward_3d(ctx, ctx->d_atoms_cache, n_atoms, grid, tune, 0, ctx->d_out_cache)))
+        return rc;
+    if ((e = cudaMemcpyAsync(h_out, ctx->d_out_cache, obytes, cudaMemcpyDeviceToHost, ctx->stream)) != cudaSuccess)
+        return cuda_error(e, "map download");
+    return coul_synchronize(ctx);
+}
+
+}  // extern "C"

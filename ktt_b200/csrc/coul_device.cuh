@@ -1,0 +1,292 @@
+// coul_device.cuh -- device-side building blocks of the direct Coulomb summation kernels (sm_100a).
+//
+// The path computes V(r_i) = sum_j q_j / |r_i - r_j| on a regular grid, the sum that KTT's
+// directCoulombSum kernels evaluate (Examples/CoulombSum3d/CoulombSum3d.cu:1-47,
+// Examples/CoulombSum2d/CoulombSum2dSimple.cl:29-79).  The B200 design:
+//   * atoms stream through shared memory in tiles of kTileAtoms float4 (x, y, z, q), fetched by
+//     one elected thread with TMA bulk copies (cp.async.bulk, local GPU memory, no multicast)
+//     into a kStages-deep ring guarded by mbarriers; every thread reads each atom as a
+//     shared-memory broadcast;
+//   * each thread owns XP grid points along x (stored as one float/float2/float4 vector) and ZI
+//     points along z (KTT's Z_ITERATIONS), so one atom read feeds XP*ZI pair evaluations and the
+//     per-atom differences dx, dy, dz are amortised over the block;
+//   * per pair: r2 = fma(dz, dz, dx^2 + dy^2) (one FP32 op), rsqrt on the MUFU unit or, for a
+//     static share of the pairs, Newton iterations on the FMA pipe, then acc = fma(q, 1/r, acc);
+//   * accumulation forms: plain FP32, FP32 sub-tile partials merged by two-sum, or merged into
+//     FP64 (precision modes of coulktt.h);
+//   * every wait on an mbarrier is bounded (iteration cap + globaltimer deadline); on expiry the
+//     kernel records a status word, drains, and returns instead of hanging or trapping.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace coul {
+
+constexpr int kTileAtoms = 256;       // atoms per shared-memory stage
+constexpr int kStages = 2;            // depth of the TMA ring
+constexpr int kSubTile = 32;          // atoms per FP32 partial in the compensated / FP64-merge forms
+constexpr int kMaxThreads = 256;      // launch bound of the forward kernels
+constexpr int kConstAtoms = 4096;     // atoms per __constant__ chunk (64 KiB)
+constexpr uint64_t kWaitBudgetNs = 1000000000ull;  // 1 s: a tile copy from L2 takes microseconds
+constexpr float kPadCoord = 1.0e18f;  // padding atoms sit far away with zero charge
+
+enum : int { kStatusOk = 0, kStatusTimeout = 1 };
+
+enum : int { kModeGrid3d = 0, kModeSlice2d = 1 };
+
+struct FwdParams {
+    const float4* atoms;  // AoS: (x, y, z, q), or (x, y, dz2, q) for 2D slices
+    const float* sx;      // SoA arrays (layout 1)
+    const float* sy;
+    const float* sz;
+    const float* sq;
+    int64_t n_atoms;
+    int nx, ny, nz;
+    float h, ox, oy, oz;
+    float* out;
+    int accumulate;
+    int* status;
+};
+
+// ------------------------------------------------------------------------------------------
+// PTX helpers
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// Orders this thread's generic-proxy shared-memory accesses before later async-proxy (TMA) ones.
+__device__ __forceinline__ void fence_proxy_async_smem()
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// TMA bulk copy global -> shared (this CTA), completion signalled on bar as transaction bytes.
+// Requires 16-byte aligned src/dst and a byte count that is a multiple of 16.
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
+{
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+__device__ __forceinline__ uint64_t globaltimer_ns()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait for the phase with the given parity: true when it completed, false on expiry
+// (after budget_ns of globaltimer time or 2^24 polls, whichever comes first).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity,
+                                                  uint64_t budget_ns = kWaitBudgetNs)
+{
+    if (mbar_try_wait(bar, parity))
+        return true;
+    const uint64_t t0 = globaltimer_ns();
+    for (uint32_t it = 1; it < (1u << 24); ++it) {
+        if (mbar_try_wait(bar, parity))
+            return true;
+        if ((it & 63u) == 0 && globaltimer_ns() - t0 > budget_ns)
+            return false;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void report_status(int* status, int code)
+{
+    if (status != nullptr)
+        atomicCAS(status, kStatusOk, code);
+}
+
+// MUFU reciprocal square root (approximate, flush-to-zero), the instruction KTT's kernels reach
+// through rsqrt()/half_rsqrt() under fast-math.
+__device__ __forceinline__ float rsqrt_mufu(float x)
+{
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// ------------------------------------------------------------------------------------------
+// FMA-pipe reciprocal square root.
+//
+// Initial estimate by the integer "magic constant" method (Blinn 1997; Lomont, "Fast Inverse
+// Square-Root", 2003): reinterpret x as an integer, halve it and subtract it from a constant,
+// which approximates -log2(x)/2 piecewise linearly.  The argument handed in is hx = x/2 (the
+// kernels form it directly from pre-halved differences), so the constant below carries the
+// -2^22 that undoes the halving inside the shift (bits(x/2) >> 1 == (bits(x) >> 1) - 2^22).  Two Newton-Raphson steps
+//     y <- y * (3/2 - hx * y^2)
+// follow; the error after them is one-signed (the iteration approaches from below), about
+// -1.5 e^2 for an incoming relative error e, and its mean is folded into the charge by the caller
+// (q * kSoftRsqrtScale), which costs nothing per pair.  Constants and error bounds are derived
+// and checked exhaustively over one binade pair in ktt_b200/soft_rsqrt.py.
+// ------------------------------------------------------------------------------------------
+constexpr uint32_t kSoftRsqrtMagic = 0x5f375a86u - (1u << 22);
+constexpr float kSoftRsqrtScale = 1.0000023f;  // rescales the one-signed error to be centred
+
+__device__ __forceinline__ float rsqrt_fma_half(float hx)
+{
+    float y = __uint_as_float(kSoftRsqrtMagic - (__float_as_uint(hx) >> 1));
+    float t = y * y;
+    t = fmaf(-hx, t, 1.5f);
+    y = y * t;
+    t = y * y;
+    t = fmaf(-hx, t, 1.5f);
+    return y * t;
+}
+
+// ------------------------------------------------------------------------------------------
+// Pair blocks: one atom against a thread's register block of grid points.
+// ------------------------------------------------------------------------------------------
+// Static split of the XP*ZI pairs between the MUFU unit and the FMA pipe: pair p uses the FMA
+// pipe when (p % 8) < SOFT.
+template <int SOFT>
+__device__ __forceinline__ constexpr bool pair_is_soft(int p)
+{
+    return (p & 7) < SOFT;
+}
+
+// 3D: thread owns points (gx[k], gy, gz[m]); acc[k][m] += q / |r - a|.
+template <int XP, int ZI, int SOFT>
+__device__ __forceinline__ void pair_block_3d(const float (&gx)[XP], float gy, const float (&gz)[ZI], float4 a,
+                                              float (&acc)[XP][ZI])
+{
+    const float dy = gy - a.y;
+    const float dy2 = dy * dy;
+    float dxy[XP];
+#pragma unroll
+    for (int k = 0; k < XP; ++k) {
+        const float dx = gx[k] - a.x;
+        dxy[k] = fmaf(dx, dx, dy2);
+    }
+    float dz[ZI];
+#pragma unroll
+    for (int m = 0; m < ZI; ++m)
+        dz[m] = gz[m] - a.z;
+    if constexpr (SOFT == 0) {
+#pragma unroll
+        for (int k = 0; k < XP; ++k)
+#pragma unroll
+            for (int m = 0; m < ZI; ++m) {
+                const float r2 = fmaf(dz[m], dz[m], dxy[k]);
+                acc[k][m] = fmaf(a.w, rsqrt_mufu(r2), acc[k][m]);
+            }
+    } else {
+        // Halved operands for the FMA-pipe pairs: hx = (dz^2 + dxy) / 2 formed in one fma.
+        const float qs = a.w * kSoftRsqrtScale;
+        float hdxy[XP];
+#pragma unroll
+        for (int k = 0; k < XP; ++k)
+            hdxy[k] = 0.5f * dxy[k];
+        float hdz[ZI];
+#pragma unroll
+        for (int m = 0; m < ZI; ++m)
+            hdz[m] = 0.5f * dz[m];
+#pragma unroll
+        for (int k = 0; k < XP; ++k)
+#pragma unroll
+            for (int m = 0; m < ZI; ++m) {
+                if (pair_is_soft<SOFT>(k * ZI + m)) {
+                    const float hr2 = fmaf(hdz[m], dz[m], hdxy[k]);
+                    acc[k][m] = fmaf(qs, rsqrt_fma_half(hr2), acc[k][m]);
+                } else {
+                    const float r2 = fmaf(dz[m], dz[m], dxy[k]);
+                    acc[k][m] = fmaf(a.w, rsqrt_mufu(r2), acc[k][m]);
+                }
+            }
+    }
+}
+
+// 2D slice (KTT's 2D convention): thread owns points (gx[k], gy[m]) of one slice, the atom's .z
+// holds the squared z distance c; acc[k][m] += q / sqrt(dx^2 + dy^2 + c).
+template <int XP, int YI, int SOFT>
+__device__ __forceinline__ void pair_block_2d(const float (&gx)[XP], const float (&gy)[YI], float4 a,
+                                              float (&acc)[XP][YI])
+{
+    float dyc[YI];
+#pragma unroll
+    for (int m = 0; m < YI; ++m) {
+        const float dy = gy[m] - a.y;
+        dyc[m] = fmaf(dy, dy, a.z);
+    }
+    float dx[XP];
+#pragma unroll
+    for (int k = 0; k < XP; ++k)
+        dx[k] = gx[k] - a.x;
+    if constexpr (SOFT == 0) {
+#pragma unroll
+        for (int k = 0; k < XP; ++k)
+#pragma unroll
+            for (int m = 0; m < YI; ++m) {
+                const float r2 = fmaf(dx[k], dx[k], dyc[m]);
+                acc[k][m] = fmaf(a.w, rsqrt_mufu(r2), acc[k][m]);
+            }
+    } else {
+        const float qs = a.w * kSoftRsqrtScale;
+        float hdyc[YI];
+#pragma unroll
+        for (int m = 0; m < YI; ++m)
+            hdyc[m] = 0.5f * dyc[m];
+        float hdx[XP];
+#pragma unroll
+        for (int k = 0; k < XP; ++k)
+            hdx[k] = 0.5f * dx[k];
+#pragma unroll
+        for (int k = 0; k < XP; ++k)
+#pragma unroll
+            for (int m = 0; m < YI; ++m) {
+                if (pair_is_soft<SOFT>(k * YI + m)) {
+                    const float hr2 = fmaf(hdx[k], dx[k], hdyc[m]);
+                    acc[k][m] = fmaf(qs, rsqrt_fma_half(hr2), acc[k][m]);
+                } else {
+                    const float r2 = fmaf(dx[k], dx[k], dyc[m]);
+                    acc[k][m] = fmaf(a.w, rsqrt_mufu(r2), acc[k][m]);
+                }
+            }
+    }
+}
+
+// Knuth's two-sum: s + e == a + b exactly (round-to-nearest, no contraction of additions).
+__device__ __forceinline__ void two_sum(float a, float b, float& s, float& e)
+{
+    s = a + b;
+    const float bb = s - a;
+    e = (a - (s - bb)) + (b - bb);
+}
+
+}  // namespace coul

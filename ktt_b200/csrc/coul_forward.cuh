@@ -1,0 +1,404 @@
+// coul_forward.cuh -- the forward (potential map) kernel template and its launchers.
+//
+// One template covers KTT's 3D kernel (Examples/CoulombSum3d/CoulombSum3d.cu:1-47) and its 2D
+// slice kernel (Examples/CoulombSum2d/CoulombSum2dSimple.cl:29-79).  Template parameters:
+//   ZI    grid points per thread along z (3D, KTT Z_ITERATIONS) or along y (2D)
+//   XP    grid points per thread along x, contiguous, stored as one vector (KTT VECTOR_SIZE /
+//         OUTER_UNROLL_FACTOR)
+//   UNR   unroll of the atom loop (KTT INNER_UNROLL_FACTOR)
+//   SRC   atoms from TMA-staged shared memory or from __constant__ chunks (KTT USE_CONSTANT_MEMORY)
+//   SOA   atoms as one float4 array or as four float arrays (KTT USE_SOA)
+//   PREC  accumulation form (coulktt.h COUL_PREC_*)
+//   SOFT  of every 8 rsqrts, how many run on the FMA pipe
+//   MODE  3D grid or 2D slice (KTT's 2D argument convention)
+// Block shape (KTT WORK_GROUP_SIZE_X/Y) is a launch-time choice, up to kMaxThreads threads.
+#pragma once
+
+#include <vector>
+
+#include "coul_device.cuh"
+
+namespace coul {
+
+enum : int { kSrcShared = 0, kSrcConstant = 1 };
+enum : int { kPrecFp32 = 0, kPrecCompensated = 1, kPrecFp64Merge = 2 };
+
+// Per translation unit: the constant-memory atom chunk.  Only the TU that instantiates the
+// constant-memory variants uses it; it has internal linkage so no relocatable device code is needed.
+static __constant__ float4 c_atoms[kConstAtoms];
+
+struct FwdLaunch {
+    FwdParams p;
+    dim3 grid;
+    dim3 block;
+    size_t smem;
+    int vec_store;  // 1 if x-vector stores are aligned for this launch
+};
+
+template <int MODE, int XP, int ZI, int SOFT>
+__device__ __forceinline__ void eval_atom(const float (&gx)[XP], float gy, const float (&gb)[ZI], float4 a,
+                                          float (&dst)[XP][ZI])
+{
+    if constexpr (MODE == kModeGrid3d)
+        pair_block_3d<XP, ZI, SOFT>(gx, gy, gb, a, dst);
+    else
+        pair_block_2d<XP, ZI, SOFT>(gx, gb, a, dst);
+}
+
+// Store XP contiguous values at row[x0 .. x0+XP), vectorised when aligned, guarded at the edge.
+template <int XP>
+__device__ __forceinline__ void store_points(float* __restrict__ row, int x0, int nx, const float (&v)[XP],
+                                             int accumulate, int vec_ok)
+{
+    if constexpr (XP == 1) {
+        if (x0 < nx)
+            row[x0] = accumulate ? row[x0] + v[0] : v[0];
+    } else {
+        if (vec_ok && x0 + XP <= nx) {
+            if constexpr (XP == 2) {
+                float2* q = reinterpret_cast<float2*>(row + x0);
+                float2 w = make_float2(v[0], v[1]);
+                if (accumulate) {
+                    const float2 o = *q;
+                    w.x += o.x;
+                    w.y += o.y;
+                }
+                *q = w;
+            } else {
+#pragma unroll
+                for (int c = 0; c < XP; c += 4) {
+                    float4* q = reinterpret_cast<float4*>(row + x0 + c);
+                    float4 w = make_float4(v[c], v[c + 1], v[c + 2], v[c + 3]);
+                    if (accumulate) {
+                        const float4 o = *q;
+                        w.x += o.x;
+                        w.y += o.y;
+                        w.z += o.z;
+                        w.w += o.w;
+                    }
+                    *q = w;
+                }
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < XP; ++k)
+                if (x0 + k < nx)
+                    row[x0 + k] = accumulate ? row[x0 + k] + v[k] : v[k];
+        }
+    }
+}
+
+template <int ZI, int XP, int UNR, int SRC, int SOA, int PREC, int SOFT, int MODE>
+__global__ void __launch_bounds__(kMaxThreads) fwd_kernel(const FwdParams p, const int vec_ok)
+{
+    static_assert(XP == 1 || XP == 2 || XP == 4 || XP == 8, "XP must be 1, 2, 4 or 8");
+    static_assert(kTileAtoms % kSubTile == 0, "sub-tiles must divide the stage");
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int x0 = (blockIdx.x * blockDim.x + tx) * XP;
+    int yrow, z0;
+    if constexpr (MODE == kModeGrid3d) {
+        yrow = blockIdx.y * blockDim.y + ty;
+        z0 = blockIdx.z * ZI;
+    } else {
+        yrow = (blockIdx.y * blockDim.y + ty) * ZI;
+        z0 = 0;
+    }
+
+    float gx[XP];
+#pragma unroll
+    for (int k = 0; k < XP; ++k)
+        gx[k] = fmaf(static_cast<float>(x0 + k), p.h, p.ox);
+    float gb[ZI];
+    float gy;
+    if constexpr (MODE == kModeGrid3d) {
+        gy = fmaf(static_cast<float>(yrow), p.h, p.oy);
+#pragma unroll
+        for (int m = 0; m < ZI; ++m)
+            gb[m] = fmaf(static_cast<float>(z0 + m), p.h, p.oz);
+    } else {
+        gy = 0.0f;
+#pragma unroll
+        for (int m = 0; m < ZI; ++m)
+            gb[m] = fmaf(static_cast<float>(yrow + m), p.h, p.oy);
+    }
+
+    float acc[XP][ZI];
+    float part[XP][ZI];
+    float cmp[XP][ZI];
+    double acc64[XP][ZI];
+#pragma unroll
+    for (int k = 0; k < XP; ++k)
+#pragma unroll
+        for (int m = 0; m < ZI; ++m) {
+            acc[k][m] = 0.0f;
+            if constexpr (PREC == kPrecCompensated)
+                cmp[k][m] = 0.0f;
+            if constexpr (PREC == kPrecFp64Merge)
+                acc64[k][m] = 0.0;
+        }
+
+    // Fold a sub-tile partial into the accumulator of the chosen form.
+    auto merge = [&]() {
+#pragma unroll
+        for (int k = 0; k < XP; ++k)
+#pragma unroll
+            for (int m = 0; m < ZI; ++m) {
+                if constexpr (PREC == kPrecCompensated) {
+                    float s, e;
+                    two_sum(acc[k][m], part[k][m], s, e);
+                    acc[k][m] = s;
+                    cmp[k][m] += e;
+                } else if constexpr (PREC == kPrecFp64Merge) {
+                    acc64[k][m] += static_cast<double>(part[k][m]);
+                }
+            }
+    };
+    auto clear_part = [&]() {
+#pragma unroll
+        for (int k = 0; k < XP; ++k)
+#pragma unroll
+            for (int m = 0; m < ZI; ++m)
+                part[k][m] = 0.0f;
+    };
+
+    if constexpr (SRC == kSrcConstant) {
+        static_assert(PREC == kPrecFp32 && SOA == 0, "constant-memory variants are plain FP32 AoS");
+        const int n = static_cast<int>(p.n_atoms);
+#pragma unroll UNR
+        for (int j = 0; j < n; ++j)
+            eval_atom<MODE, XP, ZI, SOFT>(gx, gy, gb, c_atoms[j], acc);
+    } else {
+        extern __shared__ __align__(128) unsigned char smem_raw[];
+        // Stage layout: AoS kTileAtoms float4; SoA four arrays of kTileAtoms floats (x, y, z, q).
+        unsigned char* tiles = smem_raw;
+        uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + kStages * kTileAtoms * 16);
+        const int nthreads = blockDim.x * blockDim.y;
+        const int tid = ty * blockDim.x + tx;
+        const int64_t n = p.n_atoms;
+        const int64_t nst = (n + kTileAtoms - 1) / kTileAtoms;
+
+        auto stage_count = [&](int64_t s) -> int {
+            const int64_t rem = n - s * kTileAtoms;
+            return static_cast<int>(rem < kTileAtoms ? rem : kTileAtoms);
+        };
+        // Producer: one thread arms the stage's barrier with the byte count and starts the copies.
+        auto issue = [&](int64_t s) {
+            const int buf = static_cast<int>(s % kStages);
+            const int64_t base = s * kTileAtoms;
+            const int cnt = stage_count(s);
+            unsigned char* dst = tiles + buf * kTileAtoms * 16;
+            if constexpr (SOA == 0) {
+                const uint32_t bytes = static_cast<uint32_t>(cnt) * 16u;
+                mbar_arrive_expect_tx(&full[buf], bytes);
+                bulk_copy_g2s(dst, p.atoms + base, bytes, &full[buf]);
+            } else {
+                const int cnt4 = cnt & ~3;  // bulk copies move multiples of 16 bytes
+                const uint32_t bytes = static_cast<uint32_t>(cnt4) * 4u;
+                mbar_arrive_expect_tx(&full[buf], 4u * bytes);
+                if (bytes > 0) {
+                    bulk_copy_g2s(dst + 0 * kTileAtoms * 4, p.sx + base, bytes, &full[buf]);
+                    bulk_copy_g2s(dst + 1 * kTileAtoms * 4, p.sy + base, bytes, &full[buf]);
+                    bulk_copy_g2s(dst + 2 * kTileAtoms * 4, p.sz + base, bytes, &full[buf]);
+                    bulk_copy_g2s(dst + 3 * kTileAtoms * 4, p.sq + base, bytes, &full[buf]);
+                }
+            }
+        };
+
+        if (tid == 0) {
+#pragma unroll
+            for (int s = 0; s < kStages; ++s)
+                mbar_init(&full[s], 1);
+            fence_mbar_init();
+        }
+        __syncthreads();
+        if (tid == 0) {
+            for (int64_t s = 0; s < nst && s < kStages; ++s)
+                issue(s);
+        }
+
+        for (int64_t s = 0; s < nst; ++s) {
+            const int buf = static_cast<int>(s % kStages);
+            const uint32_t parity = static_cast<uint32_t>((s / kStages) & 1);
+            const bool ok = mbar_wait_bounded(&full[buf], parity);
+            const int cnt = stage_count(s);
+            unsigned char* tile = tiles + buf * kTileAtoms * 16;
+            if (ok && cnt < kTileAtoms) {
+                // Ragged last stage: the SoA remainder (< 4 atoms) by plain loads, then padding atoms
+                // far away with zero charge so the unrolled loop below needs no bound.
+                if constexpr (SOA == 1) {
+                    const int cnt4 = cnt & ~3;
+                    for (int j = cnt4 + tid; j < cnt; j += nthreads) {
+                        const int64_t g = s * kTileAtoms + j;
+                        reinterpret_cast<float*>(tile)[0 * kTileAtoms + j] = p.sx[g];
+                        reinterpret_cast<float*>(tile)[1 * kTileAtoms + j] = p.sy[g];
+                        reinterpret_cast<float*>(tile)[2 * kTileAtoms + j] = p.sz[g];
+                        reinterpret_cast<float*>(tile)[3 * kTileAtoms + j] = p.sq[g];
+                    }
+                }
+                for (int j = cnt + tid; j < kTileAtoms; j += nthreads) {
+                    if constexpr (SOA == 0) {
+                        reinterpret_cast<float4*>(tile)[j] = make_float4(kPadCoord, kPadCoord, kPadCoord, 0.0f);
+                    } else {
+                        reinterpret_cast<float*>(tile)[0 * kTileAtoms + j] = kPadCoord;
+                        reinterpret_cast<float*>(tile)[1 * kTileAtoms + j] = kPadCoord;
+                        reinterpret_cast<float*>(tile)[2 * kTileAtoms + j] = kPadCoord;
+                        reinterpret_cast<float*>(tile)[3 * kTileAtoms + j] = 0.0f;
+                    }
+                }
+            }
+            if (__syncthreads_or(ok ? 0 : 1)) {
+                // A copy never completed: record it, drain what may still be in flight (bounded),
+                // and leave without storing.
+                if (tid == 0) {
+                    report_status(p.status, kStatusTimeout);
+                    for (int64_t r = s; r < nst && r < s + kStages; ++r)
+                        (void)mbar_wait_bounded(&full[r % kStages], static_cast<uint32_t>((r / kStages) & 1));
+                }
+                return;
+            }
+
+            auto atom_at = [&](int j) -> float4 {
+                if constexpr (SOA == 0) {
+                    return reinterpret_cast<const float4*>(tile)[j];
+                } else {
+                    const float* f = reinterpret_cast<const float*>(tile);
+                    return make_float4(f[j], f[kTileAtoms + j], f[2 * kTileAtoms + j], f[3 * kTileAtoms + j]);
+                }
+            };
+            if constexpr (PREC == kPrecFp32) {
+#pragma unroll UNR
+                for (int j = 0; j < kTileAtoms; ++j)
+                    eval_atom<MODE, XP, ZI, SOFT>(gx, gy, gb, atom_at(j), acc);
+            } else {
+                for (int j0 = 0; j0 < kTileAtoms; j0 += kSubTile) {
+                    clear_part();
+#pragma unroll UNR
+                    for (int j = 0; j < kSubTile; ++j)
+                        eval_atom<MODE, XP, ZI, SOFT>(gx, gy, gb, atom_at(j0 + j), part);
+                    merge();
+                }
+            }
+            // Everyone is done with this buffer; order the generic-proxy accesses before the next
+            // TMA write into it, then refill.
+            fence_proxy_async_smem();
+            __syncthreads();
+            if (tid == 0 && s + kStages < nst)
+                issue(s + kStages);
+        }
+    }
+
+    float val[XP][ZI];
+#pragma unroll
+    for (int k = 0; k < XP; ++k)
+#pragma unroll
+        for (int m = 0; m < ZI; ++m) {
+            if constexpr (PREC == kPrecFp32)
+                val[k][m] = acc[k][m];
+            else if constexpr (PREC == kPrecCompensated)
+                val[k][m] = acc[k][m] + cmp[k][m];
+            else
+                val[k][m] = static_cast<float>(acc64[k][m]);
+        }
+
+#pragma unroll
+    for (int m = 0; m < ZI; ++m) {
+        float v[XP];
+#pragma unroll
+        for (int k = 0; k < XP; ++k)
+            v[k] = val[k][m];
+        if constexpr (MODE == kModeGrid3d) {
+            const int z = z0 + m;
+            if (z < p.nz && yrow < p.ny)
+                store_points<XP>(p.out + (static_cast<int64_t>(z) * p.ny + yrow) * p.nx, x0, p.nx, v, p.accumulate,
+                                 vec_ok);
+        } else {
+            const int yy = yrow + m;
+            if (yy < p.ny)
+                store_points<XP>(p.out + static_cast<int64_t>(yy) * p.nx, x0, p.nx, v, p.accumulate, vec_ok);
+        }
+    }
+    (void)part;
+    (void)cmp;
+    (void)acc64;
+}
+
+// ------------------------------------------------------------------------------------------
+// Launchers and the variant registry
+// ------------------------------------------------------------------------------------------
+struct VariantKey {
+    int zi, xp, unroll, src, soa, prec, soft, mode;
+    bool operator==(const VariantKey& o) const
+    {
+        return zi == o.zi && xp == o.xp && unroll == o.unroll && src == o.src && soa == o.soa && prec == o.prec &&
+               soft == o.soft && mode == o.mode;
+    }
+};
+
+using FwdLaunchFn = cudaError_t (*)(const FwdLaunch&, cudaStream_t);
+
+struct VariantEntry {
+    VariantKey key;
+    FwdLaunchFn launch;
+    int regs;  // filled lazily from cudaFuncGetAttributes (0 = unknown)
+};
+
+template <int ZI, int XP, int UNR, int SRC, int SOA, int PREC, int SOFT, int MODE>
+cudaError_t launch_fwd(const FwdLaunch& L, cudaStream_t stream)
+{
+    auto kernel = fwd_kernel<ZI, XP, UNR, SRC, SOA, PREC, SOFT, MODE>;
+    if constexpr (SRC == kSrcConstant) {
+        // Chunks of kConstAtoms atoms go through this TU's __constant__ bank one launch at a time;
+        // later chunks accumulate onto the earlier ones.  Stream order serialises copy and launch.
+        FwdParams q = L.p;
+        const int64_t n = L.p.n_atoms;
+        int64_t off = 0;
+        do {
+            const int64_t cnt = (n - off) < kConstAtoms ? (n - off) : kConstAtoms;
+            if (cnt > 0) {
+                cudaError_t e = cudaMemcpyToSymbolAsync(c_atoms, L.p.atoms + off, static_cast<size_t>(cnt) * 16, 0,
+                                                        cudaMemcpyDeviceToDevice, stream);
+                if (e != cudaSuccess)
+                    return e;
+            }
+            q.n_atoms = cnt;
+            q.accumulate = (off > 0) ? 1 : L.p.accumulate;
+            kernel<<<L.grid, L.block, 0, stream>>>(q, L.vec_store);
+            cudaError_t e = cudaGetLastError();
+            if (e != cudaSuccess)
+                return e;
+            off += cnt;
+        } while (off < n);
+        return cudaSuccess;
+    } else {
+        kernel<<<L.grid, L.block, L.smem, stream>>>(L.p, L.vec_store);
+        return cudaGetLastError();
+    }
+}
+
+template <int ZI, int XP, int UNR, int SRC, int SOA, int PREC, int SOFT, int MODE>
+void add_variant(std::vector<VariantEntry>& v)
+{
+    v.push_back(VariantEntry{VariantKey{ZI, XP, UNR, SRC, SOA, PREC, SOFT, MODE},
+                             &launch_fwd<ZI, XP, UNR, SRC, SOA, PREC, SOFT, MODE>, 0});
+}
+
+// Register the four atom-loop unrolls {1, 2, 4, 8} of one variant family.
+template <int ZI, int XP, int SRC, int SOA, int PREC, int SOFT, int MODE>
+void add_unrolls(std::vector<VariantEntry>& v)
+{
+    add_variant<ZI, XP, 1, SRC, SOA, PREC, SOFT, MODE>(v);
+    add_variant<ZI, XP, 2, SRC, SOA, PREC, SOFT, MODE>(v);
+    add_variant<ZI, XP, 4, SRC, SOA, PREC, SOFT, MODE>(v);
+    add_variant<ZI, XP, 8, SRC, SOA, PREC, SOFT, MODE>(v);
+}
+
+// Registration functions, one per translation unit (see coul_fwd_*.cu).
+void register_fwd_3d_aos(std::vector<VariantEntry>& v);
+void register_fwd_3d_aos_z32(std::vector<VariantEntry>& v);
+void register_fwd_3d_soa(std::vector<VariantEntry>& v);
+void register_fwd_3d_const(std::vector<VariantEntry>& v);
+void register_fwd_3d_precise(std::vector<VariantEntry>& v);
+void register_fwd_3d_soft(std::vector<VariantEntry>& v);
+void register_fwd_2d(std::vector<VariantEntry>& v);
+
+}  // namespace coul

@@ -1,0 +1,22 @@
+// Forward variants: 3D, atoms read from __constant__ memory in chunks of 4096 (KTT
+// USE_CONSTANT_MEMORY = 1), plain FP32, all-MUFU.
+#include "coul_forward.cuh"
+
+namespace coul {
+
+void register_fwd_3d_const(std::vector<VariantEntry>& v)
+{
+#define COUL_XP(ZI)                                                        \
+    add_unrolls<ZI, 1, kSrcConstant, 0, kPrecFp32, 0, kModeGrid3d>(v);     \
+    add_unrolls<ZI, 2, kSrcConstant, 0, kPrecFp32, 0, kModeGrid3d>(v);     \
+    add_unrolls<ZI, 4, kSrcConstant, 0, kPrecFp32, 0, kModeGrid3d>(v);
+    COUL_XP(1)
+    COUL_XP(2)
+    COUL_XP(4)
+    COUL_XP(8)
+    COUL_XP(16)
+    COUL_XP(32)
+#undef COUL_XP
+}
+
+}  // namespace coul

@@ -1,0 +1,43 @@
+// coul_internal.h -- state and helpers shared by the translation units behind the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <functional>
+#include <string>
+#include <vector>
+
+#include "coul_forward.cuh"
+#include "coulktt.h"
+
+struct coul_ctx {
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;  // the stream every call of this context is enqueued on
+    cudaEvent_t ev_start = nullptr; // bracket the most recent timed call
+    cudaEvent_t ev_stop = nullptr;
+    bool have_timing = false;
+    int* d_status = nullptr;  // device status word written by kernels whose bounded waits expire
+    float* d_atoms_cache = nullptr;  // buffers of the host-pointer convenience calls
+    size_t atoms_cap = 0;
+    float* d_out_cache = nullptr;
+    size_t out_cap = 0;
+    int sm_count = 0;
+    int cc_major = 0;
+    int cc_minor = 0;
+    std::vector<std::function<void()>> cleanups;  // frees buffers owned by other units (run at destroy)
+};
+
+namespace coul {
+
+int set_error(int status, const std::string& msg);
+int cuda_error(cudaError_t e, const char* what);
+int ctx_activate(coul_ctx* ctx);
+int ctx_begin_timing(coul_ctx* ctx);
+int ctx_end_timing(coul_ctx* ctx);
+bool aligned16(const void* p);
+int validate_tune(const coul_tune* t, int mode, int soa, const VariantEntry** out);
+int validate_grid(const coul_grid* g);
+int launch_forward(coul_ctx* ctx, const VariantEntry* v, const FwdParams& prm, int mode, const coul_tune* t);
+
+}  // namespace coul

@@ -1,0 +1,72 @@
+"""C ABI checks that need no GPU: the library loads, exports every entry point the
+public headers declare, and validates configurations before any device work."""
+import ctypes
+import glob
+import os
+import re
+
+import pytest
+
+import ktt_b200
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols(header: str) -> list[str]:
+    text = open(header).read()
+    return sorted(set(re.findall(r"COUL_API\s+[\w\s\*]+?\b(coul_\w+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ktt_b200.load_library()
+    names = []
+    for h in glob.glob(os.path.join(REPO, "include", "*.h")):
+        names += declared_symbols(h)
+    assert len(names) >= 15
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_no_cpu_fallback_without_device():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(ktt_b200.CoulombError) as e:
+        ktt_b200.CoulombContext(0)
+    assert e.value.status == ktt_b200.COUL_ERR_NO_DEVICE
+
+
+def test_tune_validation_without_device():
+    T = ktt_b200.Tune
+    assert ktt_b200.tune_supported(T())
+    assert ktt_b200.tune_supported(T(z_iterations=32, x_points=1, unroll=8))
+    assert ktt_b200.tune_supported(T(atom_source=ktt_b200.ATOMS_CONSTANT, z_iterations=4, x_points=2))
+    assert not ktt_b200.tune_supported(T(z_iterations=3))              # no such variant
+    assert not ktt_b200.tune_supported(T(block_x=64, block_y=8))       # 512 threads > launch bound
+    assert not ktt_b200.tune_supported(T(precision=7))
+    lib = ktt_b200.load_library()
+    t = T(block_x=0).c()
+    assert lib.coul_tune_supported(ctypes.byref(t)) == ktt_b200.COUL_ERR_DEVICE_LIMITS
+    assert b"block" in lib.coul_last_error()
+
+
+def test_variant_inventory():
+    vs = ktt_b200.variants()
+    assert len(vs) == ktt_b200.load_library().coul_variant_count()
+    keys = {(t.z_iterations, t.x_points, t.unroll, t.atom_source, t.precision, t.rsqrt_soft, d2, soa)
+            for t, d2, soa in vs}
+    assert len(keys) == len(vs)  # no duplicates
+    # the KTT CUDA space of CoulombSum3d.cpp: Z_ITERATIONS x unroll x USE_SOA, all present for x_points 1
+    for zi in (1, 2, 4, 8, 16, 32):
+        for un in (1, 2, 4, 8):
+            for soa in (False, True):
+                assert (zi, 1, un, 0, 0, 0, False, soa) in keys
+    for prec in (1, 2):
+        assert any(t.precision == prec for t, _, _ in vs)
+    assert any(d2 for _, d2, _ in vs)
+
+
+def test_status_strings():
+    lib = ktt_b200.load_library()
+    assert lib.coul_status_string(0) == b"ok"
+    assert lib.coul_status_string(5).startswith(b"device-side wait")

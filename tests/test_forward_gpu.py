@@ -1,0 +1,224 @@
+"""Parity of the sm_100a forward kernels with the FP64 oracle (and KTT's golden output).
+
+Tolerances: FP32 pair evaluation with FP32 accumulation is required to stay within the headline
+1e-5 relative error (normwise, max|dV| / max|V*|) of the FP64 oracle; KTT's own known-answer
+threshold is 0.01 absolute (Examples/JSON/CoulombSum3d.json:172-181).
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from ktt_b200 import errors, workloads
+import ktt_b200
+
+pytestmark = pytest.mark.gpu
+
+TOL_NORM = 1e-5
+
+
+def _t(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def _np(t):
+    return t.detach().cpu().numpy()
+
+
+@pytest.fixture(scope="module")
+def kat(golden_dir):
+    with open(os.path.join(golden_dir, "coulomb3d_kat.json")) as f:
+        return json.load(f)
+
+
+def test_kat_full_map_matches_reference_output(ctx, kat):
+    cells = kat["cells"]
+    atoms = oracle.kat_atoms(64)
+    out = ctx.forward_3d(_t(atoms), (cells, cells, cells), kat["grid_spacing_f32"])
+    ctx.synchronize()
+    v = _np(out).reshape(-1)
+    idx = np.asarray(kat["index"], dtype=np.int64)
+    golden = np.asarray(kat["bits"], dtype=np.uint32).view(np.float32)
+    assert np.max(np.abs(v[idx] - golden)) <= kat["validation_threshold"]
+    ref = oracle.grid3d(atoms, kat["grid_spacing_f32"], (cells, cells, cells)).reshape(-1)
+    rep = errors.report(v, ref)
+    assert rep["rel_norm"] <= TOL_NORM, rep
+    assert rep["rel_point"] <= 1e-5, rep
+
+
+def test_slice2d_against_oracle_and_device_prep(ctx):
+    w = workloads.slice_2d()
+    ka = w.ktt_atoms()
+    ref = oracle.slice2d(ka, w.spacing, w.nx, w.ny)
+    got = _np(ctx.forward_2d(_t(ka), w.spacing, w.nx, w.ny))
+    rep = errors.report(got, ref)
+    assert rep["rel_norm"] <= TOL_NORM, rep
+    dev = ctx.slice_atoms(_t(w.atoms), w.z_slice)
+    assert np.array_equal(_np(dev).view(np.uint32), ka.view(np.uint32))
+
+
+def _small_case(n_atoms=300, seed=7):
+    rng = np.random.default_rng(seed)
+    a = np.empty((n_atoms, 4), dtype=np.float32)
+    a[:, :3] = rng.uniform(-2.0, 14.0, (n_atoms, 3))
+    a[:, 3] = rng.uniform(-1, 1, n_atoms)
+    return a, (37, 11, 19), 0.5, (-1.0, 2.0, 0.25)
+
+
+@pytest.fixture(scope="module")
+def small_ref():
+    a, dims, h, origin = _small_case()
+    return a, dims, h, origin, oracle.grid3d(a, h, dims, origin)
+
+
+def test_every_3d_variant_on_ragged_grid(ctx, small_ref):
+    import torch
+    a, dims, h, origin, ref = small_ref
+    ta = _t(a)
+    soa = [_t(np.ascontiguousarray(a[:, k])) for k in range(4)]
+    shapes = [(32, 4), (64, 2), (16, 8), (128, 1), (32, 1)]
+    failures = []
+    count = 0
+    for i, (tune, is2d, is_soa) in enumerate(ktt_b200.variants()):
+        if is2d:
+            continue
+        tune.block_x, tune.block_y = shapes[i % len(shapes)]
+        out = torch.full((dims[2], dims[1], dims[0]), float("nan"), device="cuda")
+        if is_soa:
+            ctx.forward_3d_soa(*soa, dims, h, origin, tune=tune, out=out)
+        else:
+            ctx.forward_3d(ta, dims, h, origin, tune=tune, out=out)
+        ctx.synchronize()
+        rep = errors.report(_np(out), ref)
+        tol = TOL_NORM if tune.rsqrt_soft == 0 else 1e-5
+        if not rep["rel_norm"] <= tol:
+            failures.append((tune.as_dict(), is_soa, rep))
+        count += 1
+    assert count > 250
+    assert not failures, failures[:5]
+
+
+def test_every_2d_variant(ctx):
+    import torch
+    w = workloads.slice_2d(seed=9, n_atoms=333, n=45)
+    ka = w.ktt_atoms()
+    ref = oracle.slice2d(ka, w.spacing, 45, 29)
+    ta = _t(ka)
+    failures = []
+    for i, (tune, is2d, _) in enumerate(ktt_b200.variants()):
+        if not is2d:
+            continue
+        tune.block_x, tune.block_y = [(32, 4), (16, 2), (8, 8), (64, 1)][i % 4]
+        out = torch.full((29, 45), float("nan"), device="cuda")
+        ctx.forward_2d(ta, w.spacing, 45, 29, tune=tune, out=out)
+        ctx.synchronize()
+        rep = errors.report(_np(out), ref)
+        if not rep["rel_norm"] <= TOL_NORM:
+            failures.append((tune.as_dict(), rep))
+    assert not failures, failures[:5]
+
+
+@pytest.mark.parametrize("n_atoms", [0, 1, 3, 255, 256, 257, 513, 4097, 8195])
+@pytest.mark.parametrize("form", ["tma", "soa", "const", "fp64", "comp"])
+def test_ragged_atom_counts(ctx, n_atoms, form):
+    import torch
+    a, dims, h, origin = _small_case(n_atoms=max(n_atoms, 1), seed=n_atoms + 3)
+    a = a[:n_atoms]
+    ref = oracle.grid3d(a, h, dims, origin) if n_atoms else np.zeros(dims[::-1])
+    tune = ktt_b200.Tune(block_x=32, block_y=2, z_iterations=4, x_points=2)
+    out = torch.full((dims[2], dims[1], dims[0]), float("nan"), device="cuda")
+    if form == "soa":
+        cols = [_t(np.ascontiguousarray(a[:, k])) if n_atoms else torch.zeros(1, device="cuda") for k in range(4)]
+        ctx.forward_3d_soa(*cols, dims, h, origin, tune=tune, out=out)
+    else:
+        if form == "const":
+            tune.atom_source = ktt_b200.ATOMS_CONSTANT
+        elif form == "fp64":
+            tune.precision = ktt_b200.PREC_FP64_MERGE
+        elif form == "comp":
+            tune.precision = ktt_b200.PREC_COMPENSATED
+        ta = _t(a) if n_atoms else torch.zeros((0, 4), device="cuda")
+        ctx.forward_3d(ta, dims, h, origin, tune=tune, out=out)
+    ctx.synchronize()
+    got = _np(out)
+    if n_atoms == 0:
+        assert np.all(got == 0.0)
+    else:
+        rep = errors.report(got, ref)
+        assert rep["rel_norm"] <= TOL_NORM, rep
+
+
+def test_accumulate_semantics(ctx, small_ref):
+    import torch
+    a, dims, h, origin, ref = small_ref
+    base = torch.linspace(-3, 3, dims[0] * dims[1] * dims[2], device="cuda").reshape(dims[2], dims[1], dims[0])
+    out = base.clone()
+    ctx.forward_3d(_t(a), dims, h, origin, out=out, accumulate=True)
+    out2 = ctx.forward_3d(_t(a), dims, h, origin)
+    ctx.synchronize()
+    np.testing.assert_allclose(_np(out), _np(base) + _np(out2), rtol=0, atol=2e-6)
+    # constant-memory path accumulates across its chunks and onto the caller's data
+    out3 = base.clone()
+    t = ktt_b200.Tune(atom_source=ktt_b200.ATOMS_CONSTANT, z_iterations=2, x_points=1)
+    ctx.forward_3d(_t(a), dims, h, origin, tune=t, out=out3, accumulate=True)
+    ctx.synchronize()
+    np.testing.assert_allclose(_np(out3), _np(base) + ref, rtol=0, atol=1e-4)
+
+
+def test_reference_kernel(ctx, small_ref):
+    a, dims, h, origin, ref = small_ref
+    out = ctx.forward_3d_reference(_t(a), dims, h, origin)
+    ctx.synchronize()
+    assert errors.report(_np(out), ref)["rel_norm"] <= TOL_NORM
+
+
+def test_host_buffer_call_matches_device_call(ctx, small_ref):
+    a, dims, h, origin, ref = small_ref
+    host = ctx.forward_3d_host(a, dims, h, origin)
+    dev = _np(ctx.forward_3d(_t(a), dims, h, origin))
+    ctx.synchronize()
+    assert np.array_equal(host, dev)
+
+
+def test_invalid_arguments_rejected_before_launch(ctx, small_ref):
+    import torch
+    a, dims, h, origin, _ = small_ref
+    ta = _t(np.concatenate([np.zeros(1, np.float32), a.reshape(-1)]))
+    mis = ta[1:].view(-1, 4)  # 4-byte offset: not 16-byte aligned
+    with pytest.raises(ktt_b200.CoulombError) as e:
+        ctx.forward_3d(mis, dims, h, origin)
+    assert e.value.status == ktt_b200.COUL_ERR_INVALID_ARGUMENT
+    with pytest.raises(ktt_b200.CoulombError) as e:
+        ctx.forward_3d(_t(a), dims, h, origin, tune=ktt_b200.Tune(z_iterations=3))
+    assert e.value.status == ktt_b200.COUL_ERR_UNSUPPORTED
+    with pytest.raises(ktt_b200.CoulombError) as e:
+        ctx.forward_3d(_t(a), (0, 4, 4), h, origin)
+    assert e.value.status == ktt_b200.COUL_ERR_INVALID_ARGUMENT
+    ctx.synchronize()
+
+
+def test_bounded_wait_expiry_is_reported_and_context_survives(ctx, small_ref):
+    assert ctx.probe_bounded_wait(True, 10_000_000) == ktt_b200.COUL_OK
+    assert ctx.probe_bounded_wait(False, 20_000_000) == ktt_b200.COUL_ERR_TIMEOUT
+    # the context (and the device) stays usable
+    a, dims, h, origin, ref = small_ref
+    out = ctx.forward_3d(_t(a), dims, h, origin)
+    ctx.synchronize()
+    assert errors.report(_np(out), ref)["rel_norm"] <= TOL_NORM
+
+
+def test_full_map_uniform_subset(ctx):
+    """The 256^3 x 65,536-atom map against FP64 on a seeded 0.1% subset, plain FP32 and FP64 merge."""
+    w = workloads.uniform_map()
+    ta = _t(w.atoms)
+    total = int(np.prod(w.dims))
+    idx = workloads.subset_indices(total, 0.001)
+    ref, sabs = oracle.points3d(w.atoms, w.spacing, w.dims, idx, want_sumabs=True)
+    for tune in (ktt_b200.Tune(), ktt_b200.Tune(precision=ktt_b200.PREC_FP64_MERGE, z_iterations=8)):
+        out = ctx.forward_3d(ta, w.dims, w.spacing, tune=tune)
+        ctx.synchronize()
+        rep = errors.report(_np(out).reshape(-1)[idx], ref, sumabs=sabs)
+        assert rep["rel_norm"] <= TOL_NORM, (tune, rep)
