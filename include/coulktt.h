@@ -113,9 +113,12 @@ typedef struct coul_ctx coul_ctx;
 /* ---- context ------------------------------------------------------------ */
 COUL_API int coul_ctx_create(int device, coul_ctx** ctx);
 COUL_API int coul_ctx_destroy(coul_ctx* ctx);
-/* Use an existing cudaStream_t (passed as void*); NULL selects the context's own stream. */
+/* Enqueue every later call of this context on the given cudaStream_t (passed as void*).  NULL is
+   the legacy default stream (PyTorch's default stream), not a private one.  A new context starts
+   on a non-blocking stream of its own, returned by coul_ctx_own_stream. */
 COUL_API int coul_ctx_set_stream(coul_ctx* ctx, void* stream);
 COUL_API void* coul_ctx_get_stream(coul_ctx* ctx);
+COUL_API void* coul_ctx_own_stream(coul_ctx* ctx);
 /* Number of SMs and compute capability of the context's device. */
 COUL_API int coul_ctx_device_info(coul_ctx* ctx, int* sm_count, int* cc_major, int* cc_minor);
 /* Wait for the context's stream; returns COUL_ERR_TIMEOUT if a kernel reported a bounded-wait expiry. */

@@ -117,8 +117,9 @@ def load_library():
         fn = getattr(lib, name)
         fn.argtypes = args
         fn.restype = ci
-    lib.coul_ctx_get_stream.argtypes = [vp]
-    lib.coul_ctx_get_stream.restype = vp
+    for name in ("coul_ctx_get_stream", "coul_ctx_own_stream"):
+        getattr(lib, name).argtypes = [vp]
+        getattr(lib, name).restype = vp
     lib.coul_last_error.restype = ctypes.c_char_p
     lib.coul_status_string.argtypes = [ci]
     lib.coul_status_string.restype = ctypes.c_char_p

@@ -320,11 +320,13 @@ COUL_API int coul_ctx_set_stream(coul_ctx* ctx, void* stream)
 {
     if (ctx == nullptr)
         return set_error(COUL_ERR_INVALID_ARGUMENT, "ctx is NULL");
-    ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
+    ctx->stream = static_cast<cudaStream_t>(stream);
     return COUL_OK;
 }
 
 COUL_API void* coul_ctx_get_stream(coul_ctx* ctx) { return ctx ? static_cast<void*>(ctx->stream) : nullptr; }
+
+COUL_API void* coul_ctx_own_stream(coul_ctx* ctx) { return ctx ? static_cast<void*>(ctx->own_stream) : nullptr; }
 
 COUL_API int coul_ctx_device_info(coul_ctx* ctx, int* sm_count, int* cc_major, int* cc_minor)
 {

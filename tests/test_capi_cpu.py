@@ -5,6 +5,7 @@ import glob
 import os
 import re
 
+import numpy as np
 import pytest
 
 import ktt_b200
@@ -70,3 +71,17 @@ def test_status_strings():
     lib = ktt_b200.load_library()
     assert lib.coul_status_string(0) == b"ok"
     assert lib.coul_status_string(5).startswith(b"device-side wait")
+
+
+def test_fma_pipe_rsqrt_bound_and_constants_match_device_code():
+    """The FMA-pipe reciprocal square root: exhaustive FP32 bound over every input in [1, 4)
+    (the error is periodic over factors of 4), and the constants in the device header are the
+    ones that bound was computed for."""
+    from ktt_b200 import soft_rsqrt as sr
+    lo, hi = sr.error_profile()
+    assert -5e-7 < lo < 0 < hi < 5e-7
+    src = open(os.path.join(REPO, "ktt_b200", "csrc", "coul_device.cuh")).read()
+    assert f"kSoftRsqrtMagic = {sr.MAGIC:#x}u" in src
+    for name, val in (("A1", sr.A1), ("A2", sr.A2), ("Scale", sr.SCALE)):
+        m = re.search(rf"kSoftRsqrt{name} = ([0-9.eE+-]+)f;", src)
+        assert m and np.float32(float(m.group(1))) == val, name
