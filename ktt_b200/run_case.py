@@ -1,6 +1,6 @@
 """Run one forward-map case and report its device time.
 
-    python -m ktt_b200.run_case --dims 128 128 128 --atoms 8192 [--tune '{"z_iterations": 8}'] [--repeat 3]
+    python -m ktt_b200.run_case --dims 128 128 128 --atoms 8192 [--set z_iterations=8 --set rsqrt_soft=2] [--repeat 3]
 
 Seeded uniform atoms in a cube scaled to the grid (q ~ U[-1, 1]), one launch per repeat timed with
 the context's event pair.  Used to drive profiler captures of a single kernel on a small case.
@@ -18,7 +18,8 @@ def main() -> None:
     ap.add_argument("--dims", type=int, nargs=3, default=[128, 128, 128])
     ap.add_argument("--atoms", type=int, default=8192)
     ap.add_argument("--spacing", type=float, default=0.5)
-    ap.add_argument("--tune", type=str, default="{}")
+    ap.add_argument("--set", action="append", default=[], metavar="FIELD=VALUE",
+                    help="coul_tune field, e.g. z_iterations=16 (repeatable)")
     ap.add_argument("--repeat", type=int, default=3)
     ap.add_argument("--seed", type=int, default=2)
     args = ap.parse_args()
@@ -33,7 +34,7 @@ def main() -> None:
     a = np.empty((args.atoms, 4), dtype=np.float32)
     a[:, :3] = rng.uniform(0.0, box, (args.atoms, 3))
     a[:, 3] = rng.uniform(-1.0, 1.0, args.atoms)
-    tune = ktt_b200.Tune(**json.loads(args.tune))
+    tune = ktt_b200.Tune(**{k: int(v) for k, v in (s.split("=", 1) for s in args.set)})
     ctx = ktt_b200.CoulombContext(0)
     atoms = torch.from_numpy(a).cuda()
     out = torch.empty((nz, ny, nx), dtype=torch.float32, device="cuda")
