@@ -43,7 +43,8 @@ def _cxx() -> str:
 
 
 def _newest_header() -> float:
-    heads = glob.glob(os.path.join(CSRC, "**", "*.h*"), recursive=True)
+    heads = glob.glob(os.path.join(CSRC, "**", "*.h"), recursive=True)
+    heads += glob.glob(os.path.join(CSRC, "**", "*.cuh"), recursive=True)
     heads += glob.glob(os.path.join(INCLUDE, "**", "*.h"), recursive=True)
     return max((os.path.getmtime(h) for h in heads), default=0.0)
 

@@ -177,21 +177,50 @@ __device__ __forceinline__ float rsqrt_fma_half(float hx)
     return y * t;
 }
 
+__device__ __forceinline__ float2 splat(float v) { return make_float2(v, v); }
+
+// Two lanes at once with sm_100's packed FP32 instructions, taking nhx = -x/2 so that neither
+// Newton step needs a negation: bits(-x/2) = bits(x/2) | 2^31, whose shift adds 2^30 that the
+// constant absorbs.  Arithmetic is identical to rsqrt_fma_half lane by lane.
+constexpr uint32_t kSoftRsqrtMagicNeg = kSoftRsqrtMagic + 0x40000000u;
+
+__device__ __forceinline__ float2 rsqrt_fma_neghalf_x2(float2 nhx)
+{
+    float2 y = make_float2(__uint_as_float(kSoftRsqrtMagicNeg - (__float_as_uint(nhx.x) >> 1)),
+                           __uint_as_float(kSoftRsqrtMagicNeg - (__float_as_uint(nhx.y) >> 1)));
+    float2 t = __fmul2_rn(y, y);
+    t = __ffma2_rn(nhx, t, splat(kSoftRsqrtA1));
+    y = __fmul2_rn(y, t);
+    t = __fmul2_rn(y, y);
+    t = __ffma2_rn(nhx, t, splat(kSoftRsqrtA2));
+    return __fmul2_rn(y, t);
+}
+
 // ------------------------------------------------------------------------------------------
 // Pair blocks: one atom against a thread's register block of grid points.
+//
+// Points along the blocked axis (z in 3D, y in 2D) are held in pairs, so the per-pair FP32 work
+// -- r^2 = fma(d, d, w) and acc = fma(q, 1/r, acc) -- is issued as packed FFMA2 instructions, one
+// issue slot for two pairs.  The reciprocal square roots go to the MUFU unit one lane at a time,
+// or, for a static share of the lane pairs, to the FMA pipe (rsqrt_fma_neghalf_x2).
 // ------------------------------------------------------------------------------------------
-// Static split of the XP*ZI pairs between the MUFU unit and the FMA pipe: pair p uses the FMA
-// pipe when (p % 8) < SOFT.
+// Static split between the MUFU unit and the FMA pipe: lane pair p uses the FMA pipe when
+// (p % 8) < SOFT.
 template <int SOFT>
 __device__ __forceinline__ constexpr bool pair_is_soft(int p)
 {
     return (p & 7) < SOFT;
 }
 
-// 3D: thread owns points (gx[k], gy, gz[m]); acc[k][m] += q / |r - a|.
-template <int XP, int ZI, int SOFT>
-__device__ __forceinline__ void pair_block_3d(const float (&gx)[XP], float gy, const float (&gz)[ZI], float4 a,
-                                              float (&acc)[XP][ZI])
+__device__ __forceinline__ float2 rsqrt_mufu_x2(float2 r2)
+{
+    return make_float2(rsqrt_mufu(r2.x), rsqrt_mufu(r2.y));
+}
+
+// 3D: thread owns points (gx[k], gy, gz[i].x / gz[i].y); acc[k][i] += q / |r - a| lane-wise.
+template <int XP, int ZH, int SOFT>
+__device__ __forceinline__ void pair_block_3d(const float (&gx)[XP], float gy, const float2 (&gz)[ZH], float4 a,
+                                              float2 (&acc)[XP][ZH])
 {
     const float dy = gy - a.y;
     const float dy2 = dy * dy;
@@ -201,90 +230,96 @@ __device__ __forceinline__ void pair_block_3d(const float (&gx)[XP], float gy, c
         const float dx = gx[k] - a.x;
         dxy[k] = fmaf(dx, dx, dy2);
     }
-    float dz[ZI];
+    float2 dz[ZH];
+    const float2 naz = splat(-a.z);
 #pragma unroll
-    for (int m = 0; m < ZI; ++m)
-        dz[m] = gz[m] - a.z;
+    for (int i = 0; i < ZH; ++i)
+        dz[i] = __fadd2_rn(gz[i], naz);
+    const float2 q2 = splat(a.w);
     if constexpr (SOFT == 0) {
 #pragma unroll
-        for (int k = 0; k < XP; ++k)
+        for (int k = 0; k < XP; ++k) {
+            const float2 w = splat(dxy[k]);
 #pragma unroll
-            for (int m = 0; m < ZI; ++m) {
-                const float r2 = fmaf(dz[m], dz[m], dxy[k]);
-                acc[k][m] = fmaf(a.w, rsqrt_mufu(r2), acc[k][m]);
+            for (int i = 0; i < ZH; ++i) {
+                const float2 r2 = __ffma2_rn(dz[i], dz[i], w);
+                acc[k][i] = __ffma2_rn(q2, rsqrt_mufu_x2(r2), acc[k][i]);
             }
+        }
     } else {
-        // Halved operands for the FMA-pipe pairs: hx = (dz^2 + dxy) / 2 formed in one fma.
-        const float qs = a.w * kSoftRsqrtScale;
-        float hdxy[XP];
+        const float2 qs2 = splat(a.w * kSoftRsqrtScale);
+        float2 nhdz[ZH];
 #pragma unroll
-        for (int k = 0; k < XP; ++k)
-            hdxy[k] = 0.5f * dxy[k];
-        float hdz[ZI];
+        for (int i = 0; i < ZH; ++i)
+            nhdz[i] = __fmul2_rn(dz[i], splat(-0.5f));
 #pragma unroll
-        for (int m = 0; m < ZI; ++m)
-            hdz[m] = 0.5f * dz[m];
+        for (int k = 0; k < XP; ++k) {
+            const float2 w = splat(dxy[k]);
+            const float2 nw = splat(-0.5f * dxy[k]);
 #pragma unroll
-        for (int k = 0; k < XP; ++k)
-#pragma unroll
-            for (int m = 0; m < ZI; ++m) {
-                if (pair_is_soft<SOFT>(k * ZI + m)) {
-                    const float hr2 = fmaf(hdz[m], dz[m], hdxy[k]);
-                    acc[k][m] = fmaf(qs, rsqrt_fma_half(hr2), acc[k][m]);
+            for (int i = 0; i < ZH; ++i) {
+                if (pair_is_soft<SOFT>(k * ZH + i)) {
+                    const float2 nhx = __ffma2_rn(nhdz[i], dz[i], nw);
+                    acc[k][i] = __ffma2_rn(qs2, rsqrt_fma_neghalf_x2(nhx), acc[k][i]);
                 } else {
-                    const float r2 = fmaf(dz[m], dz[m], dxy[k]);
-                    acc[k][m] = fmaf(a.w, rsqrt_mufu(r2), acc[k][m]);
+                    const float2 r2 = __ffma2_rn(dz[i], dz[i], w);
+                    acc[k][i] = __ffma2_rn(q2, rsqrt_mufu_x2(r2), acc[k][i]);
                 }
             }
+        }
     }
 }
 
-// 2D slice (KTT's 2D convention): thread owns points (gx[k], gy[m]) of one slice, the atom's .z
-// holds the squared z distance c; acc[k][m] += q / sqrt(dx^2 + dy^2 + c).
-template <int XP, int YI, int SOFT>
-__device__ __forceinline__ void pair_block_2d(const float (&gx)[XP], const float (&gy)[YI], float4 a,
-                                              float (&acc)[XP][YI])
+// 2D slice (KTT's 2D convention): thread owns points (gx[k], gy[i].x / gy[i].y) of one slice, the
+// atom's .z holds the squared z distance c; acc[k][i] += q / sqrt(dx^2 + dy^2 + c) lane-wise.
+template <int XP, int YH, int SOFT>
+__device__ __forceinline__ void pair_block_2d(const float (&gx)[XP], const float2 (&gy)[YH], float4 a,
+                                              float2 (&acc)[XP][YH])
 {
-    float dyc[YI];
+    float2 dyc[YH];
+    const float2 nay = splat(-a.y);
+    const float2 c2 = splat(a.z);
 #pragma unroll
-    for (int m = 0; m < YI; ++m) {
-        const float dy = gy[m] - a.y;
-        dyc[m] = fmaf(dy, dy, a.z);
+    for (int i = 0; i < YH; ++i) {
+        const float2 dy = __fadd2_rn(gy[i], nay);
+        dyc[i] = __ffma2_rn(dy, dy, c2);
     }
     float dx[XP];
 #pragma unroll
     for (int k = 0; k < XP; ++k)
         dx[k] = gx[k] - a.x;
+    const float2 q2 = splat(a.w);
     if constexpr (SOFT == 0) {
 #pragma unroll
-        for (int k = 0; k < XP; ++k)
+        for (int k = 0; k < XP; ++k) {
+            const float2 u = splat(dx[k]);
 #pragma unroll
-            for (int m = 0; m < YI; ++m) {
-                const float r2 = fmaf(dx[k], dx[k], dyc[m]);
-                acc[k][m] = fmaf(a.w, rsqrt_mufu(r2), acc[k][m]);
+            for (int i = 0; i < YH; ++i) {
+                const float2 r2 = __ffma2_rn(u, u, dyc[i]);
+                acc[k][i] = __ffma2_rn(q2, rsqrt_mufu_x2(r2), acc[k][i]);
             }
+        }
     } else {
-        const float qs = a.w * kSoftRsqrtScale;
-        float hdyc[YI];
+        const float2 qs2 = splat(a.w * kSoftRsqrtScale);
+        float2 nhdyc[YH];
 #pragma unroll
-        for (int m = 0; m < YI; ++m)
-            hdyc[m] = 0.5f * dyc[m];
-        float hdx[XP];
+        for (int i = 0; i < YH; ++i)
+            nhdyc[i] = __fmul2_rn(dyc[i], splat(-0.5f));
 #pragma unroll
-        for (int k = 0; k < XP; ++k)
-            hdx[k] = 0.5f * dx[k];
+        for (int k = 0; k < XP; ++k) {
+            const float2 u = splat(dx[k]);
+            const float2 nhu = splat(-0.5f * dx[k]);
 #pragma unroll
-        for (int k = 0; k < XP; ++k)
-#pragma unroll
-            for (int m = 0; m < YI; ++m) {
-                if (pair_is_soft<SOFT>(k * YI + m)) {
-                    const float hr2 = fmaf(hdx[k], dx[k], hdyc[m]);
-                    acc[k][m] = fmaf(qs, rsqrt_fma_half(hr2), acc[k][m]);
+            for (int i = 0; i < YH; ++i) {
+                if (pair_is_soft<SOFT>(k * YH + i)) {
+                    const float2 nhx = __ffma2_rn(nhu, u, nhdyc[i]);
+                    acc[k][i] = __ffma2_rn(qs2, rsqrt_fma_neghalf_x2(nhx), acc[k][i]);
                 } else {
-                    const float r2 = fmaf(dx[k], dx[k], dyc[m]);
-                    acc[k][m] = fmaf(a.w, rsqrt_mufu(r2), acc[k][m]);
+                    const float2 r2 = __ffma2_rn(u, u, dyc[i]);
+                    acc[k][i] = __ffma2_rn(q2, rsqrt_mufu_x2(r2), acc[k][i]);
                 }
             }
+        }
     }
 }
 

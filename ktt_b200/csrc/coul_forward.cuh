@@ -35,15 +35,17 @@ struct FwdLaunch {
     int vec_store;  // 1 if x-vector stores are aligned for this launch
 };
 
-template <int MODE, int XP, int ZI, int SOFT>
-__device__ __forceinline__ void eval_atom(const float (&gx)[XP], float gy, const float (&gb)[ZI], float4 a,
-                                          float (&dst)[XP][ZI])
+template <int MODE, int XP, int ZH, int SOFT>
+__device__ __forceinline__ void eval_atom(const float (&gx)[XP], float gy, const float2 (&gb)[ZH], float4 a,
+                                          float2 (&dst)[XP][ZH])
 {
     if constexpr (MODE == kModeGrid3d)
-        pair_block_3d<XP, ZI, SOFT>(gx, gy, gb, a, dst);
+        pair_block_3d<XP, ZH, SOFT>(gx, gy, gb, a, dst);
     else
-        pair_block_2d<XP, ZI, SOFT>(gx, gb, a, dst);
+        pair_block_2d<XP, ZH, SOFT>(gx, gb, a, dst);
 }
+
+__device__ __forceinline__ float lane(const float2& v, int l) { return l == 0 ? v.x : v.y; }
 
 // Store XP contiguous values at row[x0 .. x0+XP), vectorised when aligned, guarded at the edge.
 template <int XP>
@@ -108,33 +110,40 @@ __global__ void __launch_bounds__(kMaxThreads) fwd_kernel(const FwdParams p, con
 #pragma unroll
     for (int k = 0; k < XP; ++k)
         gx[k] = fmaf(static_cast<float>(x0 + k), p.h, p.ox);
-    float gb[ZI];
+    // Blocked-axis points in lane pairs: (z0 + 2i, z0 + 2i + 1) in 3D, rows in 2D.  With ZI == 1
+    // the second lane evaluates the next point, which is never stored.
+    constexpr int ZH = (ZI + 1) / 2;
+    float2 gb[ZH];
     float gy;
     if constexpr (MODE == kModeGrid3d) {
         gy = fmaf(static_cast<float>(yrow), p.h, p.oy);
 #pragma unroll
-        for (int m = 0; m < ZI; ++m)
-            gb[m] = fmaf(static_cast<float>(z0 + m), p.h, p.oz);
+        for (int i = 0; i < ZH; ++i)
+            gb[i] = make_float2(fmaf(static_cast<float>(z0 + 2 * i), p.h, p.oz),
+                                fmaf(static_cast<float>(z0 + 2 * i + 1), p.h, p.oz));
     } else {
         gy = 0.0f;
 #pragma unroll
-        for (int m = 0; m < ZI; ++m)
-            gb[m] = fmaf(static_cast<float>(yrow + m), p.h, p.oy);
+        for (int i = 0; i < ZH; ++i)
+            gb[i] = make_float2(fmaf(static_cast<float>(yrow + 2 * i), p.h, p.oy),
+                                fmaf(static_cast<float>(yrow + 2 * i + 1), p.h, p.oy));
     }
 
-    float acc[XP][ZI];
-    float part[XP][ZI];
-    float cmp[XP][ZI];
-    double acc64[XP][ZI];
+    float2 acc[XP][ZH];
+    float2 part[XP][ZH];
+    float2 cmp[XP][ZH];
+    double acc64[XP][2 * ZH];
 #pragma unroll
     for (int k = 0; k < XP; ++k)
 #pragma unroll
-        for (int m = 0; m < ZI; ++m) {
-            acc[k][m] = 0.0f;
+        for (int i = 0; i < ZH; ++i) {
+            acc[k][i] = make_float2(0.0f, 0.0f);
             if constexpr (PREC == kPrecCompensated)
-                cmp[k][m] = 0.0f;
-            if constexpr (PREC == kPrecFp64Merge)
-                acc64[k][m] = 0.0;
+                cmp[k][i] = make_float2(0.0f, 0.0f);
+            if constexpr (PREC == kPrecFp64Merge) {
+                acc64[k][2 * i] = 0.0;
+                acc64[k][2 * i + 1] = 0.0;
+            }
         }
 
     // Fold a sub-tile partial into the accumulator of the chosen form.
@@ -142,14 +151,16 @@ __global__ void __launch_bounds__(kMaxThreads) fwd_kernel(const FwdParams p, con
 #pragma unroll
         for (int k = 0; k < XP; ++k)
 #pragma unroll
-            for (int m = 0; m < ZI; ++m) {
+            for (int i = 0; i < ZH; ++i) {
                 if constexpr (PREC == kPrecCompensated) {
-                    float s, e;
-                    two_sum(acc[k][m], part[k][m], s, e);
-                    acc[k][m] = s;
-                    cmp[k][m] += e;
+                    float s0, e0, s1, e1;
+                    two_sum(acc[k][i].x, part[k][i].x, s0, e0);
+                    two_sum(acc[k][i].y, part[k][i].y, s1, e1);
+                    acc[k][i] = make_float2(s0, s1);
+                    cmp[k][i] = __fadd2_rn(cmp[k][i], make_float2(e0, e1));
                 } else if constexpr (PREC == kPrecFp64Merge) {
-                    acc64[k][m] += static_cast<double>(part[k][m]);
+                    acc64[k][2 * i] += static_cast<double>(part[k][i].x);
+                    acc64[k][2 * i + 1] += static_cast<double>(part[k][i].y);
                 }
             }
     };
@@ -157,8 +168,8 @@ __global__ void __launch_bounds__(kMaxThreads) fwd_kernel(const FwdParams p, con
 #pragma unroll
         for (int k = 0; k < XP; ++k)
 #pragma unroll
-            for (int m = 0; m < ZI; ++m)
-                part[k][m] = 0.0f;
+            for (int i = 0; i < ZH; ++i)
+                part[k][i] = make_float2(0.0f, 0.0f);
     };
 
     if constexpr (SRC == kSrcConstant) {
@@ -166,7 +177,7 @@ __global__ void __launch_bounds__(kMaxThreads) fwd_kernel(const FwdParams p, con
         const int n = static_cast<int>(p.n_atoms);
 #pragma unroll UNR
         for (int j = 0; j < n; ++j)
-            eval_atom<MODE, XP, ZI, SOFT>(gx, gy, gb, c_atoms[j], acc);
+            eval_atom<MODE, XP, ZH, SOFT>(gx, gy, gb, c_atoms[j], acc);
     } else {
         extern __shared__ __align__(128) unsigned char smem_raw[];
         // Stage layout: AoS kTileAtoms float4; SoA four arrays of kTileAtoms floats (x, y, z, q).
@@ -268,13 +279,13 @@ __global__ void __launch_bounds__(kMaxThreads) fwd_kernel(const FwdParams p, con
             if constexpr (PREC == kPrecFp32) {
 #pragma unroll UNR
                 for (int j = 0; j < kTileAtoms; ++j)
-                    eval_atom<MODE, XP, ZI, SOFT>(gx, gy, gb, atom_at(j), acc);
+                    eval_atom<MODE, XP, ZH, SOFT>(gx, gy, gb, atom_at(j), acc);
             } else {
                 for (int j0 = 0; j0 < kTileAtoms; j0 += kSubTile) {
                     clear_part();
 #pragma unroll UNR
                     for (int j = 0; j < kSubTile; ++j)
-                        eval_atom<MODE, XP, ZI, SOFT>(gx, gy, gb, atom_at(j0 + j), part);
+                        eval_atom<MODE, XP, ZH, SOFT>(gx, gy, gb, atom_at(j0 + j), part);
                     merge();
                 }
             }
@@ -293,9 +304,9 @@ __global__ void __launch_bounds__(kMaxThreads) fwd_kernel(const FwdParams p, con
 #pragma unroll
         for (int m = 0; m < ZI; ++m) {
             if constexpr (PREC == kPrecFp32)
-                val[k][m] = acc[k][m];
+                val[k][m] = lane(acc[k][m / 2], m & 1);
             else if constexpr (PREC == kPrecCompensated)
-                val[k][m] = acc[k][m] + cmp[k][m];
+                val[k][m] = lane(acc[k][m / 2], m & 1) + lane(cmp[k][m / 2], m & 1);
             else
                 val[k][m] = static_cast<float>(acc64[k][m]);
         }

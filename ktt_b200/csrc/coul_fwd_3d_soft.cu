@@ -10,18 +10,26 @@ static void add_soft(std::vector<VariantEntry>& v)
 {
     add_variant<8, 2, 1, kSrcShared, 0, PREC, SOFT, kModeGrid3d>(v);
     add_variant<8, 4, 1, kSrcShared, 0, PREC, SOFT, kModeGrid3d>(v);
+    add_variant<16, 1, 1, kSrcShared, 0, PREC, SOFT, kModeGrid3d>(v);
     add_variant<16, 2, 1, kSrcShared, 0, PREC, SOFT, kModeGrid3d>(v);
     add_variant<16, 4, 1, kSrcShared, 0, PREC, SOFT, kModeGrid3d>(v);
+    add_variant<32, 2, 1, kSrcShared, 0, PREC, SOFT, kModeGrid3d>(v);
+}
+
+template <int PREC>
+static void add_soft_shares(std::vector<VariantEntry>& v)
+{
+    add_soft<PREC, 1>(v);
+    add_soft<PREC, 2>(v);
+    add_soft<PREC, 3>(v);
+    add_soft<PREC, 4>(v);
+    add_soft<PREC, 5>(v);
 }
 
 void register_fwd_3d_soft(std::vector<VariantEntry>& v)
 {
-    add_soft<kPrecFp32, 2>(v);
-    add_soft<kPrecFp32, 3>(v);
-    add_soft<kPrecFp32, 4>(v);
-    add_soft<kPrecFp64Merge, 2>(v);
-    add_soft<kPrecFp64Merge, 3>(v);
-    add_soft<kPrecFp64Merge, 4>(v);
+    add_soft_shares<kPrecFp32>(v);
+    add_soft_shares<kPrecFp64Merge>(v);
 }
 
 }  // namespace coul
