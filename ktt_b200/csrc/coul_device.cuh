@@ -146,53 +146,49 @@ __device__ __forceinline__ float rsqrt_mufu(float x)
 // FMA-pipe reciprocal square root.
 //
 // Initial estimate by the integer "magic constant" method (Blinn 1997; Lomont, "Fast Inverse
-// Square-Root", 2003): reinterpret the argument as an integer, halve it and subtract it from a
-// constant, which approximates -log2(x)/2 piecewise linearly.  Two Newton-Raphson-type steps
-//     y <- y * (a_k - hx * y^2),   hx = x / 2
-// follow.  With a_k = 3/2 and Lomont's constant this is the classic iteration (one-signed error
-// in [-4.7e-6, 0]).  Here the constant and a_1 are chosen jointly to minimise the spread of the
-// first step's relative error (+-6.5e-4 instead of [-1.75e-3, 0]); the analytic-constant
-// approach is that of Moroz, Walczyk et al., "Fast calculation of inverse square root with the
-// use of magic constant -- analytical approach" (2018).  a_2 = 3/2 * lambda^2 re-centres the
-// second step on the first step's scale lambda, so the result is 1/sqrt(x) times a constant; the
-// kernels fold the reciprocal of that constant and the centring of the residual one-signed error
-// into the charge (q * kSoftRsqrtScale), at no cost per pair.  Same instruction count as the
-// classic iteration (2 integer + 6 FP32); relative error in [-4.0e-7, +4.5e-7] over all normal
-// inputs.  The derivation and the exhaustive FP32 check live in ktt_b200/soft_rsqrt.py.
+// Square-Root", 2003): reinterpret x as an integer, halve it and subtract it from a constant, which
+// approximates -log2(x)/2 piecewise linearly.  Two steps of the Newton-Raphson form
+//     y <- y * (a_k - x * y^2),   written  y <- y * fma(x, y * y, -a_k)
+// follow; the textbook iteration is y (3/2 - (x/2) y^2) with Lomont's constant (error in
+// [-4.7e-6, 0]).  Writing the steps with -a_k keeps x itself as the argument -- the r^2 the MUFU
+// path forms anyway -- and the two sign flips cancel.  The constant and a_1 are chosen jointly to
+// minimise the spread of the first step's relative error (+-6.5e-4), the analytic-constant
+// approach of Moroz, Walczyk et al., "Fast calculation of inverse square root with the use of magic
+// constant -- analytical approach" (2018); a_2 = 3 lambda^2 re-centres the second step on the first
+// step's scale lambda, so the result is 1/sqrt(x) times a constant, whose reciprocal (with the
+// centring of the residual one-signed error) the kernels fold into the charge: q * kSoftRsqrtScale,
+// no cost per pair.  2 integer + 6 FP32 instructions; relative error in [-3.9e-7, +4.6e-7] over all
+// normal inputs.  Derivation and exhaustive FP32 check: ktt_b200/soft_rsqrt.py.
 // ------------------------------------------------------------------------------------------
-constexpr uint32_t kSoftRsqrtMagic = 0x5f1eec00u;  // for the halved argument hx = x / 2
-constexpr float kSoftRsqrtA1 = 2.3625f;
-constexpr float kSoftRsqrtA2 = 5.8528552055f;
-constexpr float kSoftRsqrtScale = 0.1297434270f;
+constexpr uint32_t kSoftRsqrtMagic = 0x5f1ed000u;
+constexpr float kSoftRsqrtA1 = 2.3597500324f;
+constexpr float kSoftRsqrtA2 = 5.8324427605f;
+constexpr float kSoftRsqrtScale = 0.1844490021f;
 
-// Returns 1/sqrt(2 * hx) / kSoftRsqrtScale (the caller multiplies by kSoftRsqrtScale).
-__device__ __forceinline__ float rsqrt_fma_half(float hx)
+// Returns 1 / (kSoftRsqrtScale * sqrt(x)) (the caller multiplies by kSoftRsqrtScale).
+__device__ __forceinline__ float rsqrt_fma(float x)
 {
-    float y = __uint_as_float(kSoftRsqrtMagic - (__float_as_uint(hx) >> 1));
+    float y = __uint_as_float(kSoftRsqrtMagic - (__float_as_uint(x) >> 1));
     float t = y * y;
-    t = fmaf(-hx, t, kSoftRsqrtA1);
+    t = fmaf(x, t, -kSoftRsqrtA1);
     y = y * t;
     t = y * y;
-    t = fmaf(-hx, t, kSoftRsqrtA2);
+    t = fmaf(x, t, -kSoftRsqrtA2);
     return y * t;
 }
 
 __device__ __forceinline__ float2 splat(float v) { return make_float2(v, v); }
 
-// Two lanes at once with sm_100's packed FP32 instructions, taking nhx = -x/2 so that neither
-// Newton step needs a negation: bits(-x/2) = bits(x/2) | 2^31, whose shift adds 2^30 that the
-// constant absorbs.  Arithmetic is identical to rsqrt_fma_half lane by lane.
-constexpr uint32_t kSoftRsqrtMagicNeg = kSoftRsqrtMagic + 0x40000000u;
-
-__device__ __forceinline__ float2 rsqrt_fma_neghalf_x2(float2 nhx)
+// Two lanes at once with sm_100's packed FP32 instructions; lane-wise identical to rsqrt_fma.
+__device__ __forceinline__ float2 rsqrt_fma_x2(float2 x)
 {
-    float2 y = make_float2(__uint_as_float(kSoftRsqrtMagicNeg - (__float_as_uint(nhx.x) >> 1)),
-                           __uint_as_float(kSoftRsqrtMagicNeg - (__float_as_uint(nhx.y) >> 1)));
+    float2 y = make_float2(__uint_as_float(kSoftRsqrtMagic - (__float_as_uint(x.x) >> 1)),
+                           __uint_as_float(kSoftRsqrtMagic - (__float_as_uint(x.y) >> 1)));
     float2 t = __fmul2_rn(y, y);
-    t = __ffma2_rn(nhx, t, splat(kSoftRsqrtA1));
+    t = __ffma2_rn(x, t, splat(-kSoftRsqrtA1));
     y = __fmul2_rn(y, t);
     t = __fmul2_rn(y, y);
-    t = __ffma2_rn(nhx, t, splat(kSoftRsqrtA2));
+    t = __ffma2_rn(x, t, splat(-kSoftRsqrtA2));
     return __fmul2_rn(y, t);
 }
 
@@ -202,7 +198,7 @@ __device__ __forceinline__ float2 rsqrt_fma_neghalf_x2(float2 nhx)
 // Points along the blocked axis (z in 3D, y in 2D) are held in pairs, so the per-pair FP32 work
 // -- r^2 = fma(d, d, w) and acc = fma(q, 1/r, acc) -- is issued as packed FFMA2 instructions, one
 // issue slot for two pairs.  The reciprocal square roots go to the MUFU unit one lane at a time,
-// or, for a static share of the lane pairs, to the FMA pipe (rsqrt_fma_neghalf_x2).
+// or, for a static share of the lane pairs, to the FMA pipe (rsqrt_fma_x2).
 // ------------------------------------------------------------------------------------------
 // Static split between the MUFU unit and the FMA pipe: lane pair p uses the FMA pipe when
 // (p % 8) < SOFT.
@@ -248,23 +244,16 @@ __device__ __forceinline__ void pair_block_3d(const float (&gx)[XP], float gy, c
         }
     } else {
         const float2 qs2 = splat(a.w * kSoftRsqrtScale);
-        float2 nhdz[ZH];
-#pragma unroll
-        for (int i = 0; i < ZH; ++i)
-            nhdz[i] = __fmul2_rn(dz[i], splat(-0.5f));
 #pragma unroll
         for (int k = 0; k < XP; ++k) {
             const float2 w = splat(dxy[k]);
-            const float2 nw = splat(-0.5f * dxy[k]);
 #pragma unroll
             for (int i = 0; i < ZH; ++i) {
-                if (pair_is_soft<SOFT>(k * ZH + i)) {
-                    const float2 nhx = __ffma2_rn(nhdz[i], dz[i], nw);
-                    acc[k][i] = __ffma2_rn(qs2, rsqrt_fma_neghalf_x2(nhx), acc[k][i]);
-                } else {
-                    const float2 r2 = __ffma2_rn(dz[i], dz[i], w);
+                const float2 r2 = __ffma2_rn(dz[i], dz[i], w);
+                if (pair_is_soft<SOFT>(k * ZH + i))
+                    acc[k][i] = __ffma2_rn(qs2, rsqrt_fma_x2(r2), acc[k][i]);
+                else
                     acc[k][i] = __ffma2_rn(q2, rsqrt_mufu_x2(r2), acc[k][i]);
-                }
             }
         }
     }
@@ -301,23 +290,16 @@ __device__ __forceinline__ void pair_block_2d(const float (&gx)[XP], const float
         }
     } else {
         const float2 qs2 = splat(a.w * kSoftRsqrtScale);
-        float2 nhdyc[YH];
-#pragma unroll
-        for (int i = 0; i < YH; ++i)
-            nhdyc[i] = __fmul2_rn(dyc[i], splat(-0.5f));
 #pragma unroll
         for (int k = 0; k < XP; ++k) {
             const float2 u = splat(dx[k]);
-            const float2 nhu = splat(-0.5f * dx[k]);
 #pragma unroll
             for (int i = 0; i < YH; ++i) {
-                if (pair_is_soft<SOFT>(k * YH + i)) {
-                    const float2 nhx = __ffma2_rn(nhu, u, nhdyc[i]);
-                    acc[k][i] = __ffma2_rn(qs2, rsqrt_fma_neghalf_x2(nhx), acc[k][i]);
-                } else {
-                    const float2 r2 = __ffma2_rn(u, u, dyc[i]);
+                const float2 r2 = __ffma2_rn(u, u, dyc[i]);
+                if (pair_is_soft<SOFT>(k * YH + i))
+                    acc[k][i] = __ffma2_rn(qs2, rsqrt_fma_x2(r2), acc[k][i]);
+                else
                     acc[k][i] = __ffma2_rn(q2, rsqrt_mufu_x2(r2), acc[k][i]);
-                }
             }
         }
     }
