@@ -37,6 +37,7 @@ std::vector<VariantEntry>& registry()
         register_fwd_3d_const(v);
         register_fwd_3d_precise(v);
         register_fwd_3d_soft(v);
+        register_fwd_3d_soft_precise(v);
         register_fwd_2d(v);
     });
     return v;

@@ -410,6 +410,7 @@ void register_fwd_3d_soa(std::vector<VariantEntry>& v);
 void register_fwd_3d_const(std::vector<VariantEntry>& v);
 void register_fwd_3d_precise(std::vector<VariantEntry>& v);
 void register_fwd_3d_soft(std::vector<VariantEntry>& v);
+void register_fwd_3d_soft_precise(std::vector<VariantEntry>& v);
 void register_fwd_2d(std::vector<VariantEntry>& v);
 
 }  // namespace coul

@@ -1,6 +1,7 @@
 // Forward variants: 3D, float4 atoms through TMA-staged shared memory, with a static share of the
-// reciprocal square roots (SOFT of every 8) evaluated by Newton iterations on the FMA pipe so the
-// MUFU unit and the FMA pipe are both busy.  Plain FP32 and FP64-merge accumulation.
+// reciprocal square roots (SOFT of every 8 lane pairs) evaluated by Newton iterations on the FMA
+// pipe so the MUFU unit and the FMA pipe are both busy.  Plain FP32 accumulation (the compensated
+// and FP64-merge forms are in coul_fwd_3d_soft_precise.cu).
 #include "coul_forward.cuh"
 
 namespace coul {
@@ -8,7 +9,11 @@ namespace coul {
 template <int PREC, int SOFT>
 static void add_soft(std::vector<VariantEntry>& v)
 {
+    add_variant<4, 2, 1, kSrcShared, 0, PREC, SOFT, kModeGrid3d>(v);
+    add_variant<4, 4, 1, kSrcShared, 0, PREC, SOFT, kModeGrid3d>(v);
+    add_variant<8, 1, 1, kSrcShared, 0, PREC, SOFT, kModeGrid3d>(v);
     add_variant<8, 2, 1, kSrcShared, 0, PREC, SOFT, kModeGrid3d>(v);
+    add_variant<8, 2, 2, kSrcShared, 0, PREC, SOFT, kModeGrid3d>(v);
     add_variant<8, 4, 1, kSrcShared, 0, PREC, SOFT, kModeGrid3d>(v);
     add_variant<16, 1, 1, kSrcShared, 0, PREC, SOFT, kModeGrid3d>(v);
     add_variant<16, 2, 1, kSrcShared, 0, PREC, SOFT, kModeGrid3d>(v);
@@ -29,7 +34,6 @@ static void add_soft_shares(std::vector<VariantEntry>& v)
 void register_fwd_3d_soft(std::vector<VariantEntry>& v)
 {
     add_soft_shares<kPrecFp32>(v);
-    add_soft_shares<kPrecFp64Merge>(v);
 }
 
 }  // namespace coul
