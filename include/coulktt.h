@@ -130,6 +130,20 @@ COUL_API int coul_elapsed_ms(coul_ctx* ctx, double* ms);
 COUL_API const char* coul_last_error(void);
 COUL_API const char* coul_status_string(int status);
 
+/* ---- device buffers --------------------------------------------------------- */
+/*
+ * Device memory for hosts that do not hold a CUDA runtime of their own (the C++ ktt::Tuner
+ * surface keeps kernel arguments through these; KTT's CUDA engine does the same with its
+ * CudaBuffer class, Source/ComputeEngine/Cuda/Buffers/CudaBuffer.cpp).  Copies are ordered on the
+ * context's stream; upload/download of pageable host memory return when the copy is done.
+ */
+COUL_API int coul_buffer_alloc(coul_ctx* ctx, size_t bytes, void** d_ptr);
+COUL_API int coul_buffer_free(coul_ctx* ctx, void* d_ptr);
+COUL_API int coul_buffer_upload(coul_ctx* ctx, void* d_dst, const void* h_src, size_t bytes);
+COUL_API int coul_buffer_download(coul_ctx* ctx, void* h_dst, const void* d_src, size_t bytes);
+COUL_API int coul_buffer_copy(coul_ctx* ctx, void* d_dst, const void* d_src, size_t bytes);
+COUL_API int coul_buffer_memset(coul_ctx* ctx, void* d_dst, int value, size_t bytes);
+
 /* ---- tuning parameters ---------------------------------------------------- */
 COUL_API void coul_tune_default(coul_tune* tune);
 /* COUL_OK if the configuration maps to a compiled kernel variant that fits the device. */
@@ -166,6 +180,10 @@ COUL_API int coul_forward_3d_reference(coul_ctx* ctx, const float* d_atoms, int6
  */
 COUL_API int coul_forward_2d(coul_ctx* ctx, const float* d_atoms_xy_dz2_q, int64_t n_atoms, float spacing, int nx,
                              int ny, const coul_tune* tune, int accumulate, float* d_out);
+/* Gather four separate atom arrays (KTT's USE_SOA layout: atomInfoX/Y/Z/W) into float4 (x, y, z, q),
+   on the device; d_out must hold n_atoms float4 and be 16-byte aligned. */
+COUL_API int coul_pack_atoms(coul_ctx* ctx, const float* d_x, const float* d_y, const float* d_z, const float* d_q,
+                             int64_t n_atoms, float* d_out);
 /* Convert (x, y, z, q) atoms into the 2D convention (x, y, (z_slice - z)^2, q) on the device. */
 COUL_API int coul_slice_atoms(coul_ctx* ctx, const float* d_xyzq, int64_t n_atoms, float z_slice,
                               float* d_xy_dz2_q);

@@ -86,6 +86,14 @@ __global__ void slice_atoms_kernel(const float4* __restrict__ in, int64_t n, flo
     out[j] = make_float4(a.x, a.y, dz * dz, a.w);
 }
 
+__global__ void pack_atoms_kernel(const float* __restrict__ x, const float* __restrict__ y, const float* __restrict__ z,
+                                  const float* __restrict__ q, int64_t n, float4* __restrict__ out)
+{
+    const int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (j < n)
+        out[j] = make_float4(x[j], y[j], z[j], q[j]);
+}
+
 // Self-test of the bounded-wait machinery: one CTA arms an mbarrier for one arrival and waits on
 // it with a short budget.  With arrive != 0 the arrival happens and the wait succeeds; with
 // arrive == 0 nothing ever arrives, the wait expires, and the kernel records kStatusTimeout in the
@@ -539,6 +547,25 @@ COUL_API int coul_forward_2d(coul_ctx* ctx, const float* d_atoms, int64_t n_atom
     if ((rc = launch_forward(ctx, v, p, kModeSlice2d, tune)))
         return rc;
     return ctx_end_timing(ctx);
+}
+
+COUL_API int coul_pack_atoms(coul_ctx* ctx, const float* d_x, const float* d_y, const float* d_z, const float* d_q,
+                             int64_t n_atoms, float* d_out)
+{
+    if (ctx == nullptr)
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    if (n_atoms < 0 || (n_atoms > 0 && (!d_x || !d_y || !d_z || !d_q || !d_out || !aligned16(d_out))))
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "bad atom arrays");
+    if (n_atoms == 0)
+        return COUL_OK;
+    int rc = ctx_activate(ctx);
+    if (rc)
+        return rc;
+    const int64_t blocks = (n_atoms + 255) / 256;
+    pack_atoms_kernel<<<static_cast<unsigned>(blocks), 256, 0, ctx->stream>>>(d_x, d_y, d_z, d_q, n_atoms,
+                                                                               reinterpret_cast<float4*>(d_out));
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? COUL_OK : cuda_error(e, "pack launch");
 }
 
 COUL_API int coul_slice_atoms(coul_ctx* ctx, const float* d_xyzq, int64_t n_atoms, float z_slice, float* d_out)

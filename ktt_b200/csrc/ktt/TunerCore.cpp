@@ -1,0 +1,1417 @@
+// TunerCore.cpp -- the machinery behind ktt::Tuner (see TunerCore.h for the KTT parts it restates).
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <stdexcept>
+
+#include "Logger.h"
+#include "TunerCore.h"
+
+namespace ktt
+{
+
+namespace
+{
+
+using Clock = std::chrono::steady_clock;
+
+Nanoseconds ElapsedNs(const Clock::time_point start)
+{
+    return static_cast<Nanoseconds>(std::chrono::duration_cast<std::chrono::nanoseconds>(Clock::now() - start).count());
+}
+
+ResultStatus StatusFromCoul(const int rc)
+{
+    switch (rc)
+    {
+    case COUL_ERR_UNSUPPORTED: return ResultStatus::CompilationFailed;
+    case COUL_ERR_DEVICE_LIMITS: return ResultStatus::DeviceLimitsExceeded;
+    default: return ResultStatus::ComputationFailed;
+    }
+}
+
+void CheckCoul(const int rc, const std::string& what)
+{
+    if (rc != COUL_OK)
+    {
+        throw RunFailure(StatusFromCoul(rc), what + ": " + coul_last_error());
+    }
+}
+
+// Atom-loop unroll for KTT's INNER_UNROLL_FACTOR: 0 (no pragma) and 1 are none; values above 8
+// use the 8-way variant (the register-blocked z loop is always fully unrolled here, so KTT's
+// z-loop unroll has no separate counterpart).
+int UnrollFor(const uint64_t factor)
+{
+    if (factor <= 1) return 1;
+    if (factor < 4) return 2;
+    if (factor < 8) return 4;
+    return 8;
+}
+
+} // namespace
+
+// ---- compute layer for custom launchers ------------------------------------------------------
+
+class ComputeLayer : public ComputeInterface
+{
+public:
+    ComputeLayer(TunerCore& core, const KernelData& kernel, const KernelConfiguration& configuration, const KernelRunMode mode) :
+        m_Core(core), m_Kernel(kernel), m_Configuration(configuration), m_Mode(mode)
+    {
+        for (const auto id : kernel.definitions)
+        {
+            m_Global[id] = core.ModifiedSize(kernel, id, ModifierType::Global, configuration);
+            m_Local[id] = core.ModifiedSize(kernel, id, ModifierType::Local, configuration);
+        }
+    }
+
+    void RunKernel(const KernelDefinitionId id) override { RunKernel(id, GetCurrentGlobalSize(id), GetCurrentLocalSize(id)); }
+
+    void RunKernel(const KernelDefinitionId id, const DimensionVector& globalSize, const DimensionVector& localSize) override
+    {
+        const auto start = Clock::now();
+        const Nanoseconds duration = m_Core.LaunchDefinition(m_Kernel, id, m_Configuration, globalSize, localSize);
+        const Nanoseconds wall = ElapsedNs(start);
+        auto it = m_Results.find(id);
+
+        if (it == m_Results.end())
+        {
+            ComputationResult result(m_Core.Definition(id).name);
+            result.SetSizeData(globalSize, localSize);
+            result.SetDurationData(duration, wall > duration ? wall - duration : 0);
+            m_Results.emplace(id, result);
+            m_Order.push_back(id);
+        }
+        else
+        {
+            const Nanoseconds d = it->second.GetDuration() + duration;
+            const Nanoseconds o = it->second.GetOverhead() + (wall > duration ? wall - duration : 0);
+            it->second.SetDurationData(d, o);
+        }
+    }
+
+    ComputeActionId RunKernelAsync(const KernelDefinitionId id, [[maybe_unused]] const QueueId queue) override
+    {
+        RunKernel(id);
+        return m_NextAction++;
+    }
+
+    ComputeActionId RunKernelAsync(const KernelDefinitionId id, [[maybe_unused]] const QueueId queue,
+        const DimensionVector& globalSize, const DimensionVector& localSize) override
+    {
+        RunKernel(id, globalSize, localSize);
+        return m_NextAction++;
+    }
+
+    void WaitForComputeAction([[maybe_unused]] const ComputeActionId id) override { m_Core.Synchronize(); }
+    QueueId GetDefaultQueue() const override { return 0; }
+    std::vector<QueueId> GetAllQueues() const override { return {0}; }
+    void SynchronizeQueue([[maybe_unused]] const QueueId queue) override { m_Core.Synchronize(); }
+    void SynchronizeQueues() override { m_Core.Synchronize(); }
+    void SynchronizeDevice() override { m_Core.Synchronize(); }
+
+    const DimensionVector& GetCurrentGlobalSize(const KernelDefinitionId id) const override { return SizeOf(m_Global, id); }
+    const DimensionVector& GetCurrentLocalSize(const KernelDefinitionId id) const override { return SizeOf(m_Local, id); }
+    const KernelConfiguration& GetCurrentConfiguration() const override { return m_Configuration; }
+    KernelRunMode GetRunMode() const override { return m_Mode; }
+
+    void ChangeArguments(const KernelDefinitionId id, const std::vector<ArgumentId>& arguments) override
+    {
+        m_Core.SetArguments(id, arguments);
+    }
+
+    void SwapArguments(const KernelDefinitionId id, const ArgumentId& first, const ArgumentId& second) override
+    {
+        auto& arguments = m_Core.Definition(id).arguments;
+        auto a = std::find(arguments.begin(), arguments.end(), first);
+        auto b = std::find(arguments.begin(), arguments.end(), second);
+
+        if (a == arguments.end() || b == arguments.end())
+        {
+            throw std::runtime_error("SwapArguments: argument not used by the definition");
+        }
+
+        std::iter_swap(a, b);
+    }
+
+    void UpdateScalarArgument(const ArgumentId& id, const void* data) override
+    {
+        ArgumentData& argument = m_Core.Argument(id);
+
+        if (argument.memoryType != ArgumentMemoryType::Scalar)
+        {
+            throw std::runtime_error("Argument " + id + " is not a scalar");
+        }
+
+        std::memcpy(argument.owned.data(), data, argument.bytes);
+    }
+
+    void UploadBuffer(const ArgumentId& id) override { m_Core.UploadArgument(m_Core.Argument(id), true); }
+
+    void DownloadBuffer(const ArgumentId& id, void* destination, const size_t dataSize) override
+    {
+        m_Core.DownloadArgument(m_Core.Argument(id), destination, dataSize);
+    }
+
+    void UpdateBuffer(const ArgumentId& id, const void* data, const size_t dataSize) override
+    {
+        ArgumentData& argument = m_Core.Argument(id);
+        const size_t bytes = dataSize == 0 ? argument.bytes : std::min(dataSize, argument.bytes);
+
+        if (argument.ownership == ArgumentOwnership::User)
+        {
+            CheckCoul(coul_buffer_upload(m_Core.Context(), argument.userDevice, data, bytes), "UpdateBuffer");
+            return;
+        }
+
+        std::memcpy(argument.HostData(), data, bytes);
+        m_Core.UploadArgument(argument, true);
+    }
+
+    void CopyBuffer(const ArgumentId& destination, const ArgumentId& source, const size_t dataSize) override
+    {
+        ArgumentData& dst = m_Core.Argument(destination);
+        ArgumentData& src = m_Core.Argument(source);
+        m_Core.UploadArgument(dst, false);
+        m_Core.UploadArgument(src, false);
+        const size_t bytes = dataSize == 0 ? std::min(dst.bytes, src.bytes) : dataSize;
+        void* d = dst.ownership == ArgumentOwnership::User ? dst.userDevice : dst.device;
+        const void* s = src.ownership == ArgumentOwnership::User ? src.userDevice : src.device;
+        CheckCoul(coul_buffer_copy(m_Core.Context(), d, s, bytes), "CopyBuffer");
+    }
+
+    void ClearBuffer(const ArgumentId& id) override
+    {
+        ArgumentData& argument = m_Core.Argument(id);
+        m_Core.UploadArgument(argument, false);
+        void* d = argument.ownership == ArgumentOwnership::User ? argument.userDevice : argument.device;
+        CheckCoul(coul_buffer_memset(m_Core.Context(), d, 0, argument.bytes), "ClearBuffer");
+    }
+
+    bool HasBuffer(const ArgumentId& id) override
+    {
+        const ArgumentData& argument = m_Core.Argument(id);
+        return argument.ownership == ArgumentOwnership::User || argument.device != nullptr;
+    }
+
+    std::vector<ComputationResult> Results() const
+    {
+        std::vector<ComputationResult> out;
+
+        for (const auto id : m_Order)
+        {
+            out.push_back(m_Results.at(id));
+        }
+
+        return out;
+    }
+
+private:
+    TunerCore& m_Core;
+    const KernelData& m_Kernel;
+    KernelConfiguration m_Configuration;
+    KernelRunMode m_Mode;
+    std::map<KernelDefinitionId, DimensionVector> m_Global;
+    std::map<KernelDefinitionId, DimensionVector> m_Local;
+    std::map<KernelDefinitionId, ComputationResult> m_Results;
+    std::vector<KernelDefinitionId> m_Order;
+    ComputeActionId m_NextAction = 0;
+
+    static const DimensionVector& SizeOf(const std::map<KernelDefinitionId, DimensionVector>& sizes, const KernelDefinitionId id)
+    {
+        auto it = sizes.find(id);
+
+        if (it == sizes.end())
+        {
+            throw std::runtime_error("Definition " + std::to_string(id) + " is not part of the kernel");
+        }
+
+        return it->second;
+    }
+};
+
+// ---- TunerCore --------------------------------------------------------------------------------
+
+TunerCore::TunerCore(const DeviceIndex device, const ComputeApi api) :
+    m_Device(device), m_Api(api), m_Context(nullptr), m_GlobalSizeType(GlobalSizeType::OpenCL), m_Profiling(false),
+    m_ReadOnlyCache(true), m_ValidationMethod(ValidationMethod::SideBySideComparison), m_ValidationThreshold(1e-4),
+    m_ValidationMode(ValidationMode::OfflineTuning | ValidationMode::OnlineTuning), m_NextDefinition(0), m_NextKernel(0),
+    m_NextArgument(0)
+{
+    if (api != ComputeApi::CUDA)
+    {
+        throw std::runtime_error("This build runs the CUDA compute API only (B200, sm_100a)");
+    }
+}
+
+TunerCore::~TunerCore()
+{
+    if (m_Context != nullptr)
+    {
+        for (auto& [id, argument] : m_Arguments)
+        {
+            if (argument.device != nullptr)
+            {
+                coul_buffer_free(m_Context, argument.device);
+            }
+        }
+
+        if (m_ScratchDevice != nullptr)
+        {
+            coul_buffer_free(m_Context, m_ScratchDevice);
+        }
+
+        coul_ctx_destroy(m_Context);
+    }
+}
+
+coul_ctx* TunerCore::Context()
+{
+    if (m_Context == nullptr)
+    {
+        const int rc = coul_ctx_create(static_cast<int>(m_Device), &m_Context);
+
+        if (rc != COUL_OK)
+        {
+            m_Context = nullptr;
+            throw RunFailure(ResultStatus::ComputationFailed, std::string("device initialisation failed: ") + coul_last_error());
+        }
+    }
+
+    return m_Context;
+}
+
+void TunerCore::Synchronize()
+{
+    if (m_Context != nullptr)
+    {
+        CheckCoul(coul_synchronize(m_Context), "synchronize");
+    }
+}
+
+DeviceInfo TunerCore::GetDeviceInfo()
+{
+    int sm = 0, major = 0, minor = 0;
+    CheckCoul(coul_ctx_device_info(Context(), &sm, &major, &minor), "device info");
+    return DeviceInfo(m_Device, "NVIDIA sm_" + std::to_string(major) + std::to_string(minor) + " (" + std::to_string(sm) + " SMs)",
+        0, static_cast<uint32_t>(sm), static_cast<uint32_t>(major), static_cast<uint32_t>(minor));
+}
+
+std::string TunerCore::DeviceName()
+{
+    try
+    {
+        return GetDeviceInfo().GetName();
+    }
+    catch (const std::exception&)
+    {
+        return "unavailable";
+    }
+}
+
+// -- kernels --
+
+KernelDefinitionId TunerCore::AddDefinition(const std::string& name, const std::string& source, const DimensionVector& global,
+    const DimensionVector& local, const std::vector<std::string>& typeNames)
+{
+    if (GetDefinitionId(name, typeNames) != InvalidKernelDefinitionId)
+    {
+        throw std::runtime_error("Kernel definition with name " + name + " and the same template types already exists");
+    }
+
+    DefinitionData data;
+    data.id = m_NextDefinition++;
+    data.name = name;
+    data.source = source;
+    data.globalSize = global;
+    data.localSize = local;
+    data.typeNames = typeNames;
+    m_Definitions[data.id] = data;
+    return data.id;
+}
+
+KernelDefinitionId TunerCore::GetDefinitionId(const std::string& name, const std::vector<std::string>& typeNames) const
+{
+    for (const auto& [id, data] : m_Definitions)
+    {
+        if (data.name == name && data.typeNames == typeNames)
+        {
+            return id;
+        }
+    }
+
+    return InvalidKernelDefinitionId;
+}
+
+void TunerCore::RemoveDefinition(const KernelDefinitionId id)
+{
+    for (const auto& [kid, kernel] : m_Kernels)
+    {
+        if (std::find(kernel.definitions.cbegin(), kernel.definitions.cend(), id) != kernel.definitions.cend())
+        {
+            throw std::runtime_error("Definition " + std::to_string(id) + " is used by kernel " + kernel.name);
+        }
+    }
+
+    if (m_Definitions.erase(id) == 0)
+    {
+        throw std::runtime_error("Invalid kernel definition id " + std::to_string(id));
+    }
+}
+
+DefinitionData& TunerCore::Definition(const KernelDefinitionId id)
+{
+    auto it = m_Definitions.find(id);
+
+    if (it == m_Definitions.end())
+    {
+        throw std::runtime_error("Invalid kernel definition id " + std::to_string(id));
+    }
+
+    return it->second;
+}
+
+const DefinitionData& TunerCore::Definition(const KernelDefinitionId id) const
+{
+    return const_cast<TunerCore*>(this)->Definition(id);
+}
+
+void TunerCore::SetArguments(const KernelDefinitionId id, const std::vector<ArgumentId>& arguments)
+{
+    for (const auto& a : arguments)
+    {
+        (void)Argument(a);
+    }
+
+    Definition(id).arguments = arguments;
+}
+
+KernelId TunerCore::CreateKernel(const std::string& name, const std::vector<KernelDefinitionId>& definitions,
+    KernelLauncher launcher)
+{
+    if (definitions.empty())
+    {
+        throw std::runtime_error("A kernel needs at least one definition");
+    }
+
+    for (const auto id : definitions)
+    {
+        (void)Definition(id);
+    }
+
+    for (const auto& [id, kernel] : m_Kernels)
+    {
+        if (kernel.name == name)
+        {
+            throw std::runtime_error("Kernel with name " + name + " already exists");
+        }
+    }
+
+    KernelData& kernel = m_Kernels[m_NextKernel];
+    kernel.id = m_NextKernel++;
+    kernel.name = name;
+    kernel.definitions = definitions;
+    kernel.launcher = std::move(launcher);
+    return kernel.id;
+}
+
+void TunerCore::RemoveKernel(const KernelId id)
+{
+    if (m_Kernels.erase(id) == 0)
+    {
+        throw std::runtime_error("Invalid kernel id " + std::to_string(id));
+    }
+}
+
+KernelData& TunerCore::Kernel(const KernelId id)
+{
+    auto it = m_Kernels.find(id);
+
+    if (it == m_Kernels.end())
+    {
+        throw std::runtime_error("Invalid kernel id " + std::to_string(id));
+    }
+
+    return it->second;
+}
+
+const KernelData& TunerCore::Kernel(const KernelId id) const { return const_cast<TunerCore*>(this)->Kernel(id); }
+void TunerCore::SetLauncher(const KernelId id, KernelLauncher launcher) { Kernel(id).launcher = std::move(launcher); }
+
+void TunerCore::AddParameter(const KernelId id, const std::string& name, const std::vector<ParameterValue>& values,
+    const std::string& group)
+{
+    KernelData& kernel = Kernel(id);
+
+    for (const auto& p : kernel.parameters)
+    {
+        if (p.name == name)
+        {
+            throw std::runtime_error("Kernel parameter with name " + name + " already exists");
+        }
+    }
+
+    if (values.empty())
+    {
+        throw std::runtime_error("Kernel parameter " + name + " needs at least one value");
+    }
+
+    const auto type = ParameterPair::GetTypeFromValue(values.front());
+
+    for (const auto& v : values)
+    {
+        if (ParameterPair::GetTypeFromValue(v) != type)
+        {
+            throw std::runtime_error("All values of kernel parameter " + name + " must have the same type");
+        }
+    }
+
+    kernel.parameters.push_back({name, values, group});
+    kernel.space.reset();
+}
+
+void TunerCore::AddModifier(const KernelId id, ModifierData modifier)
+{
+    KernelData& kernel = Kernel(id);
+
+    for (const auto& name : modifier.parameters)
+    {
+        const bool known = std::any_of(kernel.parameters.cbegin(), kernel.parameters.cend(),
+            [&](const KernelParameterInfo& p) { return p.name == name; });
+
+        if (!known)
+        {
+            throw std::runtime_error("Thread modifier refers to unknown parameter " + name);
+        }
+    }
+
+    kernel.modifiers.push_back(std::move(modifier));
+}
+
+void TunerCore::AddConstraint(const KernelId id, const std::vector<std::string>& parameters, GenericConstraintFunction function,
+    const bool basic)
+{
+    KernelData& kernel = Kernel(id);
+    std::string group;
+    bool first = true;
+
+    for (const auto& name : parameters)
+    {
+        auto it = std::find_if(kernel.parameters.cbegin(), kernel.parameters.cend(),
+            [&](const KernelParameterInfo& p) { return p.name == name; });
+
+        if (it == kernel.parameters.cend())
+        {
+            throw std::runtime_error("Constraint refers to unknown parameter " + name);
+        }
+
+        if (basic && ParameterPair::GetTypeFromValue(it->values.front()) != ParameterValueType::UnsignedInt)
+        {
+            throw std::runtime_error("Kernel parameter with name " + name
+                + " does not have unsigned integer values and cannot be used by non-generic kernel constraints");
+        }
+
+        if (!first && it->group != group)
+        {
+            throw std::runtime_error("Constraint can only be added between parameters that belong to the same group");
+        }
+
+        group = it->group;
+        first = false;
+    }
+
+    kernel.constraints.push_back({parameters, std::move(function)});
+    kernel.space.reset();
+}
+
+// -- arguments --
+
+ArgumentId TunerCore::AddArgument(ArgumentData argument, const ArgumentId& customId)
+{
+    if (argument.memoryType == ArgumentMemoryType::Vector && argument.bytes == 0)
+    {
+        throw std::runtime_error("Vector argument must have a non-zero size");
+    }
+
+    ArgumentId id = customId;
+
+    if (id.empty())
+    {
+        do
+        {
+            id = std::to_string(m_NextArgument++);
+        } while (m_Arguments.count(id) != 0);
+    }
+    else if (m_Arguments.count(id) != 0)
+    {
+        throw std::runtime_error("Argument with id " + id + " already exists");
+    }
+
+    argument.id = id;
+    m_Arguments[id] = std::move(argument);
+    return id;
+}
+
+void TunerCore::RemoveArgument(const ArgumentId& id)
+{
+    for (const auto& [did, definition] : m_Definitions)
+    {
+        if (std::find(definition.arguments.cbegin(), definition.arguments.cend(), id) != definition.arguments.cend())
+        {
+            throw std::runtime_error("Argument " + id + " is used by definition " + definition.name);
+        }
+    }
+
+    auto it = m_Arguments.find(id);
+
+    if (it == m_Arguments.end())
+    {
+        throw std::runtime_error("Invalid argument id " + id);
+    }
+
+    if (it->second.device != nullptr && m_Context != nullptr)
+    {
+        coul_buffer_free(m_Context, it->second.device);
+    }
+
+    m_Arguments.erase(it);
+    m_Validation.erase(id);
+}
+
+ArgumentData& TunerCore::Argument(const ArgumentId& id)
+{
+    auto it = m_Arguments.find(id);
+
+    if (it == m_Arguments.end())
+    {
+        throw std::runtime_error("Invalid argument id " + id);
+    }
+
+    return it->second;
+}
+
+void TunerCore::UploadArgument(ArgumentData& argument, const bool force)
+{
+    if (argument.memoryType != ArgumentMemoryType::Vector || argument.ownership == ArgumentOwnership::User)
+    {
+        return;
+    }
+
+    coul_ctx* ctx = Context();
+
+    if (argument.device == nullptr || argument.deviceBytes < argument.bytes)
+    {
+        if (argument.device != nullptr)
+        {
+            coul_buffer_free(ctx, argument.device);
+            argument.device = nullptr;
+        }
+
+        CheckCoul(coul_buffer_alloc(ctx, argument.bytes, &argument.device), "buffer allocation for argument " + argument.id);
+        argument.deviceBytes = argument.bytes;
+        argument.deviceCurrent = false;
+    }
+
+    if (force || !argument.deviceCurrent)
+    {
+        CheckCoul(coul_buffer_upload(ctx, argument.device, argument.HostData(), argument.bytes), "upload of argument " + argument.id);
+        argument.deviceCurrent = true;
+    }
+}
+
+void TunerCore::DownloadArgument(ArgumentData& argument, void* destination, size_t bytes)
+{
+    if (argument.memoryType != ArgumentMemoryType::Vector)
+    {
+        throw std::runtime_error("Argument " + argument.id + " is not a vector");
+    }
+
+    bytes = bytes == 0 ? argument.bytes : std::min(bytes, argument.bytes);
+    UploadArgument(argument, false);
+    const void* source = argument.ownership == ArgumentOwnership::User ? argument.userDevice : argument.device;
+    CheckCoul(coul_buffer_download(Context(), destination, source, bytes), "download of argument " + argument.id);
+}
+
+std::vector<ArgumentId> TunerCore::KernelArguments(const KernelData& kernel) const
+{
+    std::vector<ArgumentId> ids;
+
+    for (const auto d : kernel.definitions)
+    {
+        for (const auto& a : Definition(d).arguments)
+        {
+            if (std::find(ids.cbegin(), ids.cend(), a) == ids.cend())
+            {
+                ids.push_back(a);
+            }
+        }
+    }
+
+    return ids;
+}
+
+void TunerCore::ResetWritableArguments(const KernelData& kernel)
+{
+    // Writable arguments start every run from the host data (KTT re-uploads them per run,
+    // Source/KernelRunner/KernelRunner.cpp:63-90); read-only ones stay cached on the device.
+    for (const auto& id : KernelArguments(kernel))
+    {
+        ArgumentData& argument = Argument(id);
+
+        if (argument.accessType != ArgumentAccessType::ReadOnly || !m_ReadOnlyCache)
+        {
+            argument.deviceCurrent = false;
+        }
+    }
+}
+
+// -- sizes and launches --
+
+DimensionVector TunerCore::ModifiedSize(const KernelData& kernel, const KernelDefinitionId id, const ModifierType type,
+    const KernelConfiguration& configuration) const
+{
+    // Modifiers per dimension in the order they were added (Source/Kernel/Kernel.cpp:275-308).
+    const DefinitionData& definition = Definition(id);
+    DimensionVector size = type == ModifierType::Global ? definition.globalSize : definition.localSize;
+
+    for (const auto dimension : {ModifierDimension::X, ModifierDimension::Y, ModifierDimension::Z})
+    {
+        size_t value = size.GetSize(dimension);
+
+        for (const auto& modifier : kernel.modifiers)
+        {
+            if (modifier.type != type || modifier.dimension != dimension
+                || std::find(modifier.definitions.cbegin(), modifier.definitions.cend(), id) == modifier.definitions.cend())
+            {
+                continue;
+            }
+
+            std::vector<uint64_t> values;
+
+            for (const auto& name : modifier.parameters)
+            {
+                bool found = false;
+
+                for (const auto& pair : configuration.GetPairs())
+                {
+                    if (pair.GetName() == name)
+                    {
+                        values.push_back(pair.GetValueUint());
+                        found = true;
+                        break;
+                    }
+                }
+
+                if (!found)
+                {
+                    throw std::runtime_error("Configuration lacks parameter " + name + " used by a thread modifier");
+                }
+            }
+
+            value = static_cast<size_t>(modifier.function(value, values));
+        }
+
+        size.SetSize(dimension, value);
+    }
+
+    return size;
+}
+
+Nanoseconds TunerCore::LaunchDefinition(const KernelData& kernel, const KernelDefinitionId id,
+    const KernelConfiguration& configuration, [[maybe_unused]] const DimensionVector& global, const DimensionVector& local)
+{
+    (void)kernel;
+    const DefinitionData& definition = Definition(id);
+    const auto& args = definition.arguments;
+    coul_ctx* ctx = Context();
+
+    auto parameter = [&](const char* name, const int64_t fallback) -> int64_t
+    {
+        for (const auto& pair : configuration.GetPairs())
+        {
+            if (pair.GetName() == name)
+            {
+                return static_cast<int64_t>(pair.GetValueUint());
+            }
+        }
+
+        return fallback;
+    };
+
+    auto vector = [&](const size_t i) -> float*
+    {
+        ArgumentData& argument = Argument(args.at(i));
+
+        if (argument.memoryType != ArgumentMemoryType::Vector)
+        {
+            throw RunFailure(ResultStatus::ComputationFailed, "argument " + std::to_string(i) + " of " + definition.name
+                + " must be a vector");
+        }
+
+        UploadArgument(argument, false);
+        return static_cast<float*>(argument.ownership == ArgumentOwnership::User ? argument.userDevice : argument.device);
+    };
+
+    auto scalar = [&](const size_t i) -> double
+    {
+        const ArgumentData& argument = Argument(args.at(i));
+
+        if (argument.memoryType != ArgumentMemoryType::Scalar)
+        {
+            throw RunFailure(ResultStatus::ComputationFailed, "argument " + std::to_string(i) + " of " + definition.name
+                + " must be a scalar");
+        }
+
+        const void* p = argument.owned.data();
+
+        switch (argument.dataType)
+        {
+        case ArgumentDataType::Int: return *static_cast<const int32_t*>(p);
+        case ArgumentDataType::UnsignedInt: return *static_cast<const uint32_t*>(p);
+        case ArgumentDataType::Long: return static_cast<double>(*static_cast<const int64_t*>(p));
+        case ArgumentDataType::UnsignedLong: return static_cast<double>(*static_cast<const uint64_t*>(p));
+        case ArgumentDataType::Float: return *static_cast<const float*>(p);
+        case ArgumentDataType::Double: return *static_cast<const double*>(p);
+        default: throw RunFailure(ResultStatus::ComputationFailed, "unsupported scalar type of argument " + argument.id);
+        }
+    };
+
+    auto packedAtoms = [&](const size_t first, const int64_t n) -> const float*
+    {
+        // KTT's USE_SOA layouts carry the same atoms in four arrays; gather them into float4 on the device.
+        if (parameter("USE_SOA", 0) == 0)
+        {
+            return vector(first);
+        }
+
+        const size_t bytes = static_cast<size_t>(std::max<int64_t>(n, 1)) * 16;
+
+        if (m_ScratchBytes < bytes)
+        {
+            if (m_ScratchDevice != nullptr)
+            {
+                coul_buffer_free(ctx, m_ScratchDevice);
+                m_ScratchDevice = nullptr;
+                m_ScratchBytes = 0;
+            }
+
+            CheckCoul(coul_buffer_alloc(ctx, bytes, &m_ScratchDevice), "scratch allocation");
+            m_ScratchBytes = bytes;
+        }
+
+        CheckCoul(coul_pack_atoms(ctx, vector(first + 1), vector(first + 2), vector(first + 3), vector(first + 4), n,
+                      static_cast<float*>(m_ScratchDevice)),
+            "pack of four-array atoms");
+        return static_cast<const float*>(m_ScratchDevice);
+    };
+
+    coul_tune tune;
+    coul_tune_default(&tune);
+    tune.block_x = static_cast<int>(parameter("WORK_GROUP_SIZE_X", static_cast<int64_t>(local.GetSizeX())));
+    tune.block_y = static_cast<int>(parameter("WORK_GROUP_SIZE_Y", static_cast<int64_t>(local.GetSizeY())));
+    tune.unroll = UnrollFor(static_cast<uint64_t>(parameter("INNER_UNROLL_FACTOR", 1)));
+    tune.atom_source = static_cast<int>(parameter("USE_CONSTANT_MEMORY", 0));
+    tune.precision = static_cast<int>(parameter("PRECISION", 0));
+    tune.rsqrt_soft = static_cast<int>(parameter("RSQRT_SOFT", 0));
+
+    const bool threeD = definition.globalSize.GetSizeZ() > 1;
+    int rc = COUL_OK;
+
+    if (definition.name == "directCoulombSum" && args.size() == 9 && threeD)
+    {
+        // Examples/CoulombSum3d/CoulombSum3d.cu: (atomInfo, X, Y, Z, W, numberOfAtoms, gridSpacing, gridSize, energyGrid)
+        const int64_t n = static_cast<int64_t>(scalar(5));
+        const int g = static_cast<int>(scalar(7));
+        coul_grid grid{g, g, g, static_cast<float>(scalar(6)), {0.0f, 0.0f, 0.0f}};
+        tune.z_iterations = static_cast<int>(parameter("Z_ITERATIONS", 1));
+        tune.x_points = static_cast<int>(parameter("X_POINTS", parameter("VECTOR_SIZE", 1)));
+
+        if (parameter("USE_SOA", 0) == 1)
+        {
+            rc = coul_forward_3d_soa(ctx, vector(1), vector(2), vector(3), vector(4), n, &grid, &tune, 1, vector(8));
+        }
+        else
+        {
+            rc = coul_forward_3d(ctx, vector(0), n, &grid, &tune, 1, vector(8));
+        }
+    }
+    else if (definition.name == "directCoulombSum" && (args.size() == 8 || args.size() == 9))
+    {
+        // 2D slice (Examples/CoulombSum2d/CoulombSum2d.cl): (atomInfo, X, Y, Z, W, numberOfAtoms, gridSpacing, energyGrid),
+        // or one slice of a 3D map (Examples/CoulombSum3dIterative/CoulombSum3dIterative.cl) with zIndex before energyGrid.
+        const int64_t n = static_cast<int64_t>(scalar(5));
+        const int nx = static_cast<int>(definition.globalSize.GetSizeX());
+        const int ny = static_cast<int>(definition.globalSize.GetSizeY());
+        const int64_t zIndex = args.size() == 9 ? static_cast<int64_t>(scalar(7)) : 0;
+        float* out = vector(args.size() - 1) + zIndex * static_cast<int64_t>(nx) * ny;
+        tune.z_iterations = static_cast<int>(parameter("Y_ITERATIONS", 2));
+        tune.x_points = static_cast<int>(parameter("X_POINTS", parameter("OUTER_UNROLL_FACTOR", 1)));
+        tune.atom_source = COUL_ATOMS_SHARED_TMA;
+        rc = coul_forward_2d(ctx, packedAtoms(0, n), n, static_cast<float>(scalar(6)), nx, ny, &tune, 1, out);
+    }
+    else if (definition.name == "directCoulombSumReference" && args.size() == 5)
+    {
+        // Examples/CoulombSum3d/CoulombSum3dReference.cu: (atomInfo, numberOfAtoms, gridSpacing, gridSize, energyGrid)
+        const int g = static_cast<int>(scalar(3));
+        coul_grid grid{g, g, g, static_cast<float>(scalar(2)), {0.0f, 0.0f, 0.0f}};
+        rc = coul_forward_3d_reference(ctx, vector(0), static_cast<int64_t>(scalar(1)), &grid, 1, vector(4));
+    }
+    else if (definition.name == "directCoulombSumReference" && args.size() == 4 && threeD)
+    {
+        // Examples/CoulombSum3dIterative/CoulombSum3dIterativeReference.cl: 3D map, sizes from the global size
+        coul_grid grid{static_cast<int>(definition.globalSize.GetSizeX()), static_cast<int>(definition.globalSize.GetSizeY()),
+            static_cast<int>(definition.globalSize.GetSizeZ()), static_cast<float>(scalar(2)), {0.0f, 0.0f, 0.0f}};
+        rc = coul_forward_3d_reference(ctx, vector(0), static_cast<int64_t>(scalar(1)), &grid, 1, vector(3));
+    }
+    else if (definition.name == "directCoulombSumReference" && args.size() == 4)
+    {
+        // Examples/CoulombSum2d/CoulombSum2dReference.cl: 2D slice, assigns (=) instead of accumulating
+        coul_tune reference;
+        coul_tune_default(&reference);
+        reference.z_iterations = 2;
+        reference.x_points = 1;
+        rc = coul_forward_2d(ctx, vector(0), static_cast<int64_t>(scalar(1)), static_cast<float>(scalar(2)),
+            static_cast<int>(definition.globalSize.GetSizeX()), static_cast<int>(definition.globalSize.GetSizeY()), &reference, 0,
+            vector(3));
+    }
+    else
+    {
+        throw RunFailure(ResultStatus::CompilationFailed, "no sm_100a implementation of kernel " + definition.name + " with "
+            + std::to_string(args.size()) + " arguments");
+    }
+
+    CheckCoul(rc, "launch of " + definition.name);
+    CheckCoul(coul_synchronize(ctx), "execution of " + definition.name);
+    double ms = 0.0;
+    CheckCoul(coul_elapsed_ms(ctx, &ms), "timing of " + definition.name);
+    return static_cast<Nanoseconds>(std::llround(ms * 1e6));
+}
+
+// -- validation --
+
+void TunerCore::SetValidationMethod(const ValidationMethod method, const double threshold)
+{
+    if (threshold < 0.0)
+    {
+        throw std::runtime_error("Validation threshold must be non-negative");
+    }
+
+    m_ValidationMethod = method;
+    m_ValidationThreshold = threshold;
+}
+
+ValidationData& TunerCore::Validation(const ArgumentId& id)
+{
+    (void)Argument(id);
+    return m_Validation[id];
+}
+
+void TunerCore::ComputeReference(const ArgumentId& id, ValidationData& data)
+{
+    ArgumentData& argument = Argument(id);
+    const size_t elements = data.range ? data.range : argument.bytes / argument.elementSize;
+    data.reference.assign(elements * argument.elementSize, 0);
+
+    if (data.computation)
+    {
+        data.computation(data.reference.data());
+    }
+    else if (data.referenceKernel != InvalidKernelId)
+    {
+        KernelResult result = Run(data.referenceKernel, data.referenceConfiguration, {}, KernelRunMode::ResultValidation);
+
+        if (!result.IsValid())
+        {
+            throw std::runtime_error("Reference kernel failed for argument " + id);
+        }
+
+        DownloadArgument(argument, data.reference.data(), data.reference.size());
+    }
+    else if (!data.referenceArgument.empty())
+    {
+        const ArgumentData& other = Argument(data.referenceArgument);
+        std::memcpy(data.reference.data(), other.HostData(), std::min(other.bytes, data.reference.size()));
+    }
+
+    data.computed = true;
+}
+
+bool TunerCore::Compare(const ArgumentData& argument, const ValidationData& data, const void* result, const size_t elements) const
+{
+    // ResultValidator (Source/KernelRunner/ResultValidator.inl:53-108): floating-point arguments by the
+    // configured method and threshold, integer ones exactly, or by the user's comparator.
+    if (data.comparator)
+    {
+        const auto* r = static_cast<const uint8_t*>(result);
+        const auto* e = data.reference.data();
+
+        for (size_t i = 0; i < elements; ++i)
+        {
+            if (!data.comparator(r + i * argument.elementSize, e + i * argument.elementSize))
+            {
+                log::Warning("Results differ for argument with id " + argument.id + " at index " + std::to_string(i));
+                return false;
+            }
+        }
+
+        return true;
+    }
+
+    auto check = [&](auto typed) -> bool
+    {
+        using T = decltype(typed);
+        const T* r = static_cast<const T*>(result);
+        const T* e = reinterpret_cast<const T*>(data.reference.data());
+
+        if constexpr (std::is_floating_point_v<T>)
+        {
+            if (m_ValidationMethod == ValidationMethod::AbsoluteDifference)
+            {
+                double sum = 0.0;
+
+                for (size_t i = 0; i < elements; ++i)
+                {
+                    sum += std::fabs(static_cast<double>(r[i]) - static_cast<double>(e[i]));
+                }
+
+                if (sum > m_ValidationThreshold)
+                {
+                    log::Warning("Results differ for argument with id " + argument.id + ", absolute difference is "
+                        + std::to_string(sum));
+                    return false;
+                }
+
+                return true;
+            }
+
+            for (size_t i = 0; i < elements; ++i)
+            {
+                const double difference = std::fabs(static_cast<double>(r[i]) - static_cast<double>(e[i]));
+                const bool fail = m_ValidationMethod == ValidationMethod::SideBySideComparison
+                    ? !(difference <= m_ValidationThreshold)
+                    : (difference > 1e-4 && difference / static_cast<double>(e[i]) > m_ValidationThreshold);
+
+                if (fail)
+                {
+                    log::Warning("Results differ for argument with id " + argument.id + " at index " + std::to_string(i)
+                        + ", reference value: " + std::to_string(e[i]) + ", result value: " + std::to_string(r[i])
+                        + ", difference: " + std::to_string(difference));
+                    return false;
+                }
+            }
+
+            return true;
+        }
+        else
+        {
+            for (size_t i = 0; i < elements; ++i)
+            {
+                if (r[i] != e[i])
+                {
+                    log::Warning("Results differ for argument with id " + argument.id + " at index " + std::to_string(i));
+                    return false;
+                }
+            }
+
+            return true;
+        }
+    };
+
+    switch (argument.dataType)
+    {
+    case ArgumentDataType::Float: return check(float{});
+    case ArgumentDataType::Double: return check(double{});
+    case ArgumentDataType::Int: return check(int32_t{});
+    case ArgumentDataType::UnsignedInt: return check(uint32_t{});
+    case ArgumentDataType::Long: return check(int64_t{});
+    case ArgumentDataType::UnsignedLong: return check(uint64_t{});
+    case ArgumentDataType::Short: return check(int16_t{});
+    case ArgumentDataType::UnsignedShort: return check(uint16_t{});
+    case ArgumentDataType::Char: return check(int8_t{});
+    case ArgumentDataType::UnsignedChar: return check(uint8_t{});
+    default: return std::memcmp(result, data.reference.data(), elements * argument.elementSize) == 0;
+    }
+}
+
+bool TunerCore::ValidateOutputs(const KernelData& kernel, const KernelConfiguration& configuration, KernelResult& result)
+{
+    (void)configuration;
+    const auto ids = KernelArguments(kernel);
+
+    for (auto& [id, data] : m_Validation)
+    {
+        if (std::find(ids.cbegin(), ids.cend(), id) == ids.cend())
+        {
+            continue;
+        }
+
+        ArgumentData& argument = Argument(id);
+        const size_t elements = data.range ? data.range : argument.bytes / argument.elementSize;
+        std::vector<uint8_t> values(elements * argument.elementSize);
+        DownloadArgument(argument, values.data(), values.size());
+
+        if (!data.computed)
+        {
+            ComputeReference(id, data);
+            // the reference run reset the writable arguments; nothing else depends on them now
+        }
+
+        if (!Compare(argument, data, values.data(), elements))
+        {
+            result.SetStatus(ResultStatus::ValidationFailed);
+            return false;
+        }
+    }
+
+    return true;
+}
+
+// -- running --
+
+KernelResult TunerCore::Run(const KernelId id, const KernelConfiguration& configuration,
+    const std::vector<BufferOutputDescriptor>& output, const KernelRunMode mode)
+{
+    const KernelData& kernel = Kernel(id);
+    KernelResult result(kernel.name, configuration);
+    const auto start = Clock::now();
+    std::vector<ComputationResult> computations;
+
+    try
+    {
+        ResetWritableArguments(kernel);
+
+        if (kernel.launcher)
+        {
+            ComputeLayer layer(*this, kernel, configuration, mode);
+            kernel.launcher(layer);
+            computations = layer.Results();
+        }
+        else
+        {
+            for (const auto definition : kernel.definitions)
+            {
+                const DimensionVector global = ModifiedSize(kernel, definition, ModifierType::Global, configuration);
+                const DimensionVector local = ModifiedSize(kernel, definition, ModifierType::Local, configuration);
+                const auto launchStart = Clock::now();
+                const Nanoseconds duration = LaunchDefinition(kernel, definition, configuration, global, local);
+                const Nanoseconds wall = ElapsedNs(launchStart);
+                ComputationResult computation(Definition(definition).name);
+                computation.SetSizeData(global, local);
+                computation.SetDurationData(duration, wall > duration ? wall - duration : 0);
+                computations.push_back(computation);
+            }
+        }
+    }
+    catch (const RunFailure& failure)
+    {
+        log::Warning("Kernel run failed for kernel " + kernel.name + ", configuration " + configuration.GetString() + ": "
+            + failure.what());
+        result.SetStatus(failure.status);
+        result.SetFailedKernelOverhead(ElapsedNs(start));
+        return result;
+    }
+    catch (const std::exception& failure)
+    {
+        log::Warning("Kernel run failed for kernel " + kernel.name + ": " + failure.what());
+        result.SetStatus(ResultStatus::ComputationFailed);
+        result.SetFailedKernelOverhead(ElapsedNs(start));
+        return result;
+    }
+
+    result.SetResults(computations);
+    const bool validate = (mode == KernelRunMode::Running && HasFlag(m_ValidationMode, ValidationMode::Running))
+        || (mode == KernelRunMode::OfflineTuning && HasFlag(m_ValidationMode, ValidationMode::OfflineTuning))
+        || (mode == KernelRunMode::OnlineTuning && HasFlag(m_ValidationMode, ValidationMode::OnlineTuning));
+
+    if (validate)
+    {
+        const auto validationStart = Clock::now();
+
+        try
+        {
+            ValidateOutputs(kernel, configuration, result);
+        }
+        catch (const std::exception& failure)
+        {
+            log::Warning(std::string("Validation failed: ") + failure.what());
+            result.SetStatus(ResultStatus::ValidationFailed);
+        }
+
+        result.SetValidationOverhead(ElapsedNs(validationStart));
+    }
+
+    const auto transferStart = Clock::now();
+
+    for (const auto& descriptor : output)
+    {
+        DownloadArgument(Argument(descriptor.GetArgumentId()), descriptor.GetOutputDestination(), descriptor.GetOutputSize());
+    }
+
+    result.SetDataMovementOverhead(ElapsedNs(transferStart));
+    return result;
+}
+
+ConfigurationSpace& TunerCore::Space(const KernelId id)
+{
+    KernelData& kernel = Kernel(id);
+
+    if (!kernel.space)
+    {
+        log::Info("Generating configurations for kernel " + kernel.name);
+        kernel.space = std::make_unique<ConfigurationSpace>(kernel.parameters, kernel.constraints);
+        log::Info("Total count of " + std::to_string(kernel.space->GetConfigurationsCount())
+            + " configurations was generated");
+    }
+
+    return *kernel.space;
+}
+
+void TunerCore::ClearSpace(const KernelId id)
+{
+    KernelData& kernel = Kernel(id);
+
+    if (kernel.searcher && kernel.searcher->IsInitialized())
+    {
+        kernel.searcher->Reset();
+    }
+
+    kernel.space.reset();
+    kernel.searcherActive = false;
+}
+
+void TunerCore::SetSearcher(const KernelId id, std::unique_ptr<Searcher> searcher)
+{
+    ClearSpace(id);
+    Kernel(id).searcher = std::move(searcher);
+}
+
+std::vector<KernelResult> TunerCore::Tune(const KernelId id, std::unique_ptr<StopCondition> stop)
+{
+    // The offline tuning loop of Source/TuningRunner/TuningRunner.cpp:17-82.
+    KernelData& kernel = Kernel(id);
+    ClearSpace(id);
+    ConfigurationSpace& space = Space(id);
+
+    if (!kernel.searcher)
+    {
+        kernel.searcher = std::make_unique<DeterministicSearcher>();
+    }
+
+    kernel.searcher->Initialize(space);
+
+    if (stop)
+    {
+        stop->Initialize(space.GetConfigurationsCount());
+    }
+
+    std::vector<KernelResult> results;
+    Nanoseconds searcherOverhead = 0;
+
+    while (!space.IsExhausted())
+    {
+        const KernelConfiguration configuration = kernel.searcher->GetCurrentConfiguration();
+        KernelResult result = Run(id, configuration, {}, KernelRunMode::OfflineTuning);
+        result.SetSearcherOverhead(searcherOverhead);
+        space.MarkExplored(space.GetIndex(configuration));
+
+        if (result.IsValid())
+        {
+            space.UpdateBest(configuration, result.GetTotalDuration());
+        }
+
+        log::Info("Tuned configuration " + std::to_string(results.size()) + ": " + configuration.GetString() + " -> "
+            + (result.IsValid() ? std::to_string(result.GetTotalDuration() / 1000) + " us" : std::string("failed")));
+        results.push_back(result);
+
+        if (stop)
+        {
+            stop->Update(result);
+
+            if (stop->IsFulfilled())
+            {
+                log::Info(stop->GetStatusString());
+                break;
+            }
+        }
+
+        if (space.IsExhausted())
+        {
+            break;
+        }
+
+        const auto searcherStart = Clock::now();
+        const bool more = kernel.searcher->CalculateNextConfiguration(result);
+        searcherOverhead = ElapsedNs(searcherStart);
+
+        if (!more)
+        {
+            break;
+        }
+    }
+
+    kernel.searcher->Reset();
+    return results;
+}
+
+KernelResult TunerCore::TuneIteration(const KernelId id, const std::vector<BufferOutputDescriptor>& output,
+    const bool recompute)
+{
+    // One step of online tuning (Tuner::TuneIteration, Source/Tuner.h:677): the searcher's current
+    // configuration is run with output, then the searcher moves on; once the space is exhausted
+    // the best configuration keeps being run.
+    KernelData& kernel = Kernel(id);
+    ConfigurationSpace& space = Space(id);
+
+    if (recompute)
+    {
+        for (auto& [aid, data] : m_Validation)
+        {
+            data.computed = false;
+        }
+    }
+
+    if (!kernel.searcher)
+    {
+        kernel.searcher = std::make_unique<DeterministicSearcher>();
+    }
+
+    if (!kernel.searcher->IsInitialized() && !space.IsExhausted())
+    {
+        kernel.searcher->Initialize(space);
+        kernel.searcherActive = true;
+    }
+
+    if (!kernel.searcherActive || space.IsExhausted())
+    {
+        return Run(id, space.GetBestConfiguration(), output, KernelRunMode::Running);
+    }
+
+    const KernelConfiguration configuration = kernel.searcher->GetCurrentConfiguration();
+    KernelResult result = Run(id, configuration, output, KernelRunMode::OnlineTuning);
+    space.MarkExplored(space.GetIndex(configuration));
+
+    if (result.IsValid())
+    {
+        space.UpdateBest(configuration, result.GetTotalDuration());
+    }
+
+    if (space.IsExhausted() || !kernel.searcher->CalculateNextConfiguration(result))
+    {
+        kernel.searcherActive = false;
+    }
+
+    return result;
+}
+
+std::vector<KernelResult> TunerCore::SimulateTuning(const KernelId id, const std::vector<KernelResult>& recorded,
+    const uint64_t iterations)
+{
+    // Replays recorded results through the searcher without running anything
+    // (Source/TuningRunner/TuningRunner.cpp:131-201).
+    KernelData& kernel = Kernel(id);
+    ClearSpace(id);
+    ConfigurationSpace& space = Space(id);
+
+    if (!kernel.searcher)
+    {
+        kernel.searcher = std::make_unique<DeterministicSearcher>();
+    }
+
+    kernel.searcher->Initialize(space);
+    std::vector<KernelResult> results;
+
+    while (!space.IsExhausted() && (iterations == 0 || results.size() < iterations))
+    {
+        const KernelConfiguration configuration = kernel.searcher->GetCurrentConfiguration();
+        auto it = std::find_if(recorded.cbegin(), recorded.cend(),
+            [&](const KernelResult& r) { return r.GetConfiguration() == configuration; });
+        KernelResult result = it != recorded.cend() ? *it : KernelResult(kernel.name, configuration);
+
+        if (it == recorded.cend())
+        {
+            log::Warning("No recorded result for configuration " + configuration.GetString());
+            result.SetStatus(ResultStatus::ComputationFailed);
+        }
+
+        space.MarkExplored(space.GetIndex(configuration));
+
+        if (result.IsValid())
+        {
+            space.UpdateBest(configuration, result.GetTotalDuration());
+        }
+
+        results.push_back(result);
+
+        if (space.IsExhausted() || !kernel.searcher->CalculateNextConfiguration(result))
+        {
+            break;
+        }
+    }
+
+    kernel.searcher->Reset();
+    return results;
+}
+
+KernelConfiguration TunerCore::CreateConfiguration(const KernelId id, const ParameterInput& input) const
+{
+    const KernelData& kernel = Kernel(id);
+    std::vector<ParameterPair> pairs;
+
+    for (const auto& [name, value] : input)
+    {
+        auto it = std::find_if(kernel.parameters.cbegin(), kernel.parameters.cend(),
+            [&](const KernelParameterInfo& p) { return p.name == name; });
+
+        if (it == kernel.parameters.cend())
+        {
+            throw std::runtime_error("Kernel " + kernel.name + " has no parameter " + name);
+        }
+
+        const ParameterPair pair(name, value);
+        const bool known = std::any_of(it->values.cbegin(), it->values.cend(),
+            [&](const ParameterValue& v) { return pair.HasSameValue(ParameterPair(name, v)); });
+
+        if (!known)
+        {
+            throw std::runtime_error("Value " + pair.GetValueString() + " is not a value of parameter " + name);
+        }
+
+        pairs.push_back(pair);
+    }
+
+    for (const auto& p : kernel.parameters)
+    {
+        const bool given = std::any_of(pairs.cbegin(), pairs.cend(), [&](const ParameterPair& q) { return q.GetName() == p.name; });
+
+        if (!given)
+        {
+            pairs.emplace_back(p.name, p.values.front());
+        }
+    }
+
+    return KernelConfiguration(pairs);
+}
+
+std::string TunerCore::GetDefinitionSource(const KernelDefinitionId id, const KernelConfiguration& configuration) const
+{
+    return configuration.GeneratePrefix() + Definition(id).source;
+}
+
+std::string TunerCore::GetKernelSource(const KernelId id, const KernelConfiguration& configuration) const
+{
+    const KernelData& kernel = Kernel(id);
+    std::string source;
+
+    for (const auto d : kernel.definitions)
+    {
+        source += GetDefinitionSource(d, configuration);
+    }
+
+    return source;
+}
+
+} // namespace ktt
