@@ -62,3 +62,13 @@ def test_prefix_golden_matches_reference_test():
     g = json.load(open(os.path.join(GOLDEN, "ktt_prefix.json")))
     assert g["expected"] == "#define param_two 5\n#define param_one 2\n"
     assert g["pairs"] == [["param_two", 5], ["param_one", 2]]
+
+
+def test_gpu_programs_compile(tmp_path):
+    """The GPU test programs build against the public headers (they run in test_tuner_gpu.py)."""
+    from ktt_b200 import build as kb
+    kb.build()
+    lib = os.path.join(REPO, "ktt_b200")
+    subprocess.run([_cxx(), "-std=c++17", "-O1", "-Wall", "-I", os.path.join(REPO, "include"),
+                    os.path.join(REPO, "tests", "cpp", "tuner_gpu_tests.cpp"), "-o", str(tmp_path / "t"), "-L", lib,
+                    "-lktt_b200", "-lcoulktt", f"-Wl,-rpath,{lib}"], check=True)
