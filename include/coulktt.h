@@ -195,6 +195,39 @@ COUL_API int coul_slice_atoms(coul_ctx* ctx, const float* d_xyzq, int64_t n_atom
 COUL_API int coul_forward_3d_host(coul_ctx* ctx, const float* h_atoms, int64_t n_atoms, const coul_grid* grid,
                                   const coul_tune* tune, float* h_out);
 
+/* ---- batched: many molecules in one persistent launch ------------------------------ */
+/*
+ * A batch of molecules with uneven atom counts and grids, computed by one persistent launch that
+ * pulls (molecule, tile) work items from a device queue, molecules in decreasing order of pair
+ * count.  Replaces the one-launch-per-problem pattern of KTT's custom launchers
+ * (Examples/CoulombSum3dIterative/CoulombSum3dIterative.cpp:146-184).  The batch keeps the
+ * molecule table and the queue counter on the device; the caller keeps its atom and output
+ * buffers alive while the batch exists.
+ */
+typedef struct coul_molecule {
+    const float* d_atoms; /* n_atoms float4 (x, y, z, q), 16-byte aligned */
+    int64_t n_atoms;
+    coul_grid grid;
+    float* d_out;         /* nx * ny * nz floats, x fastest */
+} coul_molecule;
+
+typedef struct coul_batch coul_batch;
+
+enum {
+    COUL_BATCH_PERSISTENT = 0, /* queue reset + one persistent launch */
+    COUL_BATCH_GRAPH = 1,      /* the same two steps captured once into a CUDA graph and replayed */
+    COUL_BATCH_SEPARATE = 2    /* baseline: one plain forward launch per molecule */
+};
+
+/* tune selects the tile shape (z_iterations, x_points, unroll, precision, rsqrt_soft, block). */
+COUL_API int coul_batch_create(coul_ctx* ctx, const coul_molecule* molecules, int n_molecules, const coul_tune* tune,
+                               coul_batch** batch);
+COUL_API int coul_batch_destroy(coul_batch* batch);
+/* Enqueue one evaluation of every molecule's map (accumulate as in coul_forward_3d); timed like
+   the forward calls (coul_elapsed_ms covers the whole batch). */
+COUL_API int coul_batch_run(coul_ctx* ctx, coul_batch* batch, int mode, int accumulate);
+COUL_API int coul_batch_info(const coul_batch* batch, int64_t* work_items, int* grid_ctas, double* total_pairs);
+
 /* ---- roofline ------------------------------------------------------------------ */
 /*
  * Measures, on the context's device at its current clocks, the whole-GPU rate of MUFU reciprocal

@@ -306,3 +306,57 @@ class CoulombContext:
         _check(self._lib.coul_forward_3d_host(self._ctx, a.ctypes.data, a.shape[0], ctypes.byref(g), ctypes.byref(t),
                                               out.ctypes.data))
         return out
+
+
+BATCH_PERSISTENT = 0
+BATCH_GRAPH = 1
+BATCH_SEPARATE = 2
+
+
+class Batch:
+    """Many molecules evaluated by one persistent launch from a (molecule, tile) work queue.
+
+    molecules: list of (atoms (n, 4) float32 CUDA tensor, dims (nx, ny, nz), spacing, origin).
+    The batch allocates one output map per molecule (``outputs``, shapes (nz, ny, nx)).
+    """
+
+    def __init__(self, ctx: "CoulombContext", molecules, tune: Tune | None = None):
+        import torch
+        from ._signatures import Molecule
+        self._ctx = ctx
+        self._lib = ctx._lib
+        self.atoms = [m[0] for m in molecules]
+        self.outputs = []
+        arr = (Molecule * len(molecules))()
+        for i, (atoms, dims, spacing, origin) in enumerate(molecules):
+            CoulombContext._check_atoms(atoms)
+            nx, ny, nz = (int(d) for d in dims)
+            out = torch.empty((nz, ny, nx), dtype=torch.float32, device=atoms.device)
+            self.outputs.append(out)
+            arr[i].d_atoms = atoms.data_ptr()
+            arr[i].n_atoms = atoms.shape[0]
+            arr[i].grid = _grid(dims, spacing, origin)
+            arr[i].d_out = out.data_ptr()
+        self.tune = tune or Tune(z_iterations=8, x_points=2, unroll=2, rsqrt_soft=2)
+        t = self.tune.c()
+        self._handle = ctypes.c_void_p()
+        ctx._bind_stream()
+        _check(self._lib.coul_batch_create(ctx.handle, arr, len(molecules), ctypes.byref(t), ctypes.byref(self._handle)))
+        items, ctas, pairs = ctypes.c_int64(), ctypes.c_int(), ctypes.c_double()
+        _check(self._lib.coul_batch_info(self._handle, ctypes.byref(items), ctypes.byref(ctas), ctypes.byref(pairs)))
+        self.work_items, self.grid_ctas, self.total_pairs = items.value, ctas.value, pairs.value
+
+    def run(self, mode: int = BATCH_PERSISTENT, accumulate: bool = False) -> None:
+        self._ctx._bind_stream()
+        _check(self._lib.coul_batch_run(self._ctx.handle, self._handle, int(mode), 1 if accumulate else 0))
+
+    def close(self) -> None:
+        if self._handle:
+            self._lib.coul_batch_destroy(self._handle)
+            self._handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,375 @@
+// coul_batched.cu -- many molecules with uneven atom counts and grids in one persistent launch.
+//
+// KTT maps the same situation onto one launch per problem from a custom launcher (the 256 slice
+// launches of Examples/CoulombSum3dIterative/CoulombSum3dIterative.cpp:146-184).  Here every tile of
+// every molecule's grid is a work item; items are numbered molecule by molecule, molecules in
+// decreasing order of pair count (longest-processing-time first, so the smallest items fill the
+// tail).  A persistent kernel -- as many CTAs as fit on the GPU at once -- claims items from a
+// device counter with one atomic add per item and runs each through the same per-tile code as the
+// forward kernel, the TMA atom ring carrying over from item to item.  The counter is reset by a
+// memset in the same stream before each launch; the pair (memset, launch) can be captured once into
+// a CUDA graph and replayed.  The plain alternative -- one forward launch per molecule -- is kept as
+// the baseline.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <numeric>
+#include <vector>
+
+#include "coul_internal.h"
+
+namespace coul {
+
+struct MolDesc {
+    const float4* atoms;
+    int64_t n_atoms;
+    float* out;
+    int64_t tile_begin;  // first work item of this molecule
+    int nx, ny, nz;
+    int tiles_x, tiles_y;
+    int vec_ok;
+    float h, ox, oy, oz;
+};
+
+struct BatchParams {
+    const MolDesc* mols;
+    int n_mol;
+    int64_t total_items;
+    unsigned long long* counter;
+    int accumulate;
+    int* status;
+};
+
+template <int ZI, int XP, int UNR, int PREC, int SOFT>
+__global__ void __launch_bounds__(kMaxThreads) batched_kernel(const BatchParams b)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + kStages * kTileAtoms * 16);
+    __shared__ long long s_item;
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    ring_init(full, tid);
+    uint32_t gstage = 0;
+
+    for (;;) {
+        if (tid == 0)
+            s_item = static_cast<long long>(atomicAdd(b.counter, 1ull));
+        __syncthreads();
+        const long long item = s_item;
+        __syncthreads();
+        if (item >= b.total_items)
+            return;
+
+        // the molecule: last one whose first item is <= item
+        int lo = 0, hi = b.n_mol - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) / 2;
+            if (b.mols[mid].tile_begin <= item)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        const MolDesc m = b.mols[lo];
+        const long long local = item - m.tile_begin;
+        const int tile_x = static_cast<int>(local % m.tiles_x);
+        const long long rest = local / m.tiles_x;
+        const int tile_y = static_cast<int>(rest % m.tiles_y);
+        const int tile_z = static_cast<int>(rest / m.tiles_y);
+
+        FwdParams p{};
+        p.atoms = m.atoms;
+        p.n_atoms = m.n_atoms;
+        p.nx = m.nx;
+        p.ny = m.ny;
+        p.nz = m.nz;
+        p.h = m.h;
+        p.ox = m.ox;
+        p.oy = m.oy;
+        p.oz = m.oz;
+        p.out = m.out;
+        p.accumulate = b.accumulate;
+        p.status = b.status;
+        const int x0 = (tile_x * blockDim.x + threadIdx.x) * XP;
+        const int yrow = tile_y * blockDim.y + threadIdx.y;
+        const int z0 = tile_z * ZI;
+        if (!tile_pass<ZI, XP, UNR, kSrcShared, 0, PREC, SOFT, kModeGrid3d>(p, x0, yrow, z0, m.vec_ok, smem_raw, full,
+                                                                              gstage))
+            return;
+    }
+}
+
+struct BatchVariant {
+    int zi, xp, unroll, prec, soft;
+    const void* kernel;
+};
+
+template <int ZI, int XP, int UNR, int PREC, int SOFT>
+static BatchVariant batch_variant()
+{
+    return BatchVariant{ZI, XP, UNR, PREC, SOFT, reinterpret_cast<const void*>(&batched_kernel<ZI, XP, UNR, PREC, SOFT>)};
+}
+
+// Tile shapes compiled for the persistent kernel (the forward kernel's best shapes on B200).
+static const std::vector<BatchVariant>& batch_variants()
+{
+    static const std::vector<BatchVariant> v{
+        batch_variant<8, 2, 2, kPrecFp32, 2>(),      batch_variant<8, 2, 1, kPrecFp32, 2>(),
+        batch_variant<8, 2, 2, kPrecFp32, 0>(),      batch_variant<8, 2, 1, kPrecFp32, 0>(),
+        batch_variant<4, 2, 1, kPrecFp32, 2>(),      batch_variant<4, 4, 1, kPrecFp32, 2>(),
+        batch_variant<8, 4, 1, kPrecFp32, 2>(),      batch_variant<16, 1, 1, kPrecFp32, 2>(),
+        batch_variant<16, 2, 1, kPrecFp32, 2>(),     batch_variant<8, 2, 1, kPrecFp64Merge, 2>(),
+        batch_variant<8, 2, 1, kPrecCompensated, 2>(),
+    };
+    return v;
+}
+
+}  // namespace coul
+
+using namespace coul;
+
+struct coul_batch {
+    coul_ctx* ctx = nullptr;
+    coul_tune tune{};
+    std::vector<coul_molecule> molecules;  // as given (for the separate-launch baseline)
+    std::vector<int> order;                // molecule indices in work-list order
+    MolDesc* d_mols = nullptr;
+    unsigned long long* d_counter = nullptr;
+    int64_t total_items = 0;
+    double total_pairs = 0.0;
+    const BatchVariant* variant = nullptr;
+    int grid_ctas = 0;
+    size_t smem = 0;
+    cudaStream_t capture_stream = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    int graph_accumulate = -1;
+};
+
+static void batch_release(coul_batch* b)
+{
+    if (b == nullptr)
+        return;
+    if (b->graph_exec)
+        cudaGraphExecDestroy(b->graph_exec);
+    if (b->graph)
+        cudaGraphDestroy(b->graph);
+    if (b->capture_stream)
+        cudaStreamDestroy(b->capture_stream);
+    if (b->d_mols)
+        cudaFree(b->d_mols);
+    if (b->d_counter)
+        cudaFree(b->d_counter);
+    delete b;
+}
+
+static cudaError_t launch_batched(coul_batch* b, cudaStream_t stream, int accumulate)
+{
+    cudaError_t e = cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned long long), stream);
+    if (e != cudaSuccess)
+        return e;
+    BatchParams p{b->d_mols, static_cast<int>(b->order.size()), b->total_items, b->d_counter, accumulate,
+                  b->ctx->d_status};
+    void* args[] = {&p};
+    const dim3 block(static_cast<unsigned>(b->tune.block_x), static_cast<unsigned>(b->tune.block_y), 1);
+    return cudaLaunchKernel(b->variant->kernel, dim3(static_cast<unsigned>(b->grid_ctas)), block, args, b->smem, stream);
+}
+
+extern "C" {
+
+COUL_API int coul_batch_create(coul_ctx* ctx, const coul_molecule* molecules, int n_molecules, const coul_tune* tune,
+                               coul_batch** out)
+{
+    if (ctx == nullptr || out == nullptr || tune == nullptr || (n_molecules > 0 && molecules == nullptr) ||
+        n_molecules < 0)
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "bad batch arguments");
+    *out = nullptr;
+    const int threads = tune->block_x * tune->block_y;
+    if (tune->block_x < 1 || tune->block_y < 1 || threads > kMaxThreads)
+        return set_error(COUL_ERR_DEVICE_LIMITS, "block shape outside 1..256 threads");
+    const int unroll = tune->unroll <= 1 ? 1 : tune->unroll;
+    const BatchVariant* variant = nullptr;
+    for (const auto& v : batch_variants())
+        if (v.zi == tune->z_iterations && v.xp == tune->x_points && v.unroll == unroll && v.prec == tune->precision &&
+            v.soft == tune->rsqrt_soft)
+            variant = &v;
+    if (variant == nullptr || tune->atom_source != COUL_ATOMS_SHARED_TMA)
+        return set_error(COUL_ERR_UNSUPPORTED, "no compiled persistent variant for this tile shape");
+    for (int i = 0; i < n_molecules; ++i) {
+        const coul_molecule& m = molecules[i];
+        int rc = validate_grid(&m.grid);
+        if (rc)
+            return rc;
+        if (m.n_atoms < 0 || m.d_out == nullptr || (m.n_atoms > 0 && (m.d_atoms == nullptr || !aligned16(m.d_atoms))))
+            return set_error(COUL_ERR_INVALID_ARGUMENT, "molecule " + std::to_string(i) + ": bad atoms or output");
+        if (m.grid.nx > (1 << 24) || m.grid.ny > (1 << 24) || m.grid.nz > (1 << 24))
+            return set_error(COUL_ERR_INVALID_ARGUMENT, "molecule " + std::to_string(i) + ": grid too large");
+    }
+    int rc = ctx_activate(ctx);
+    if (rc)
+        return rc;
+
+    auto* b = new coul_batch();
+    b->ctx = ctx;
+    b->tune = *tune;
+    b->tune.unroll = unroll;
+    b->variant = variant;
+    b->molecules.assign(molecules, molecules + n_molecules);
+    b->order.resize(static_cast<size_t>(n_molecules));
+    std::iota(b->order.begin(), b->order.end(), 0);
+    auto pairs = [&](int i) {
+        const coul_molecule& m = molecules[i];
+        return static_cast<double>(m.grid.nx) * m.grid.ny * m.grid.nz * static_cast<double>(m.n_atoms);
+    };
+    std::stable_sort(b->order.begin(), b->order.end(), [&](int a, int c) { return pairs(a) > pairs(c); });
+
+    std::vector<MolDesc> descs;
+    int64_t next = 0;
+    const int64_t span_x = static_cast<int64_t>(tune->block_x) * tune->x_points;
+    for (const int i : b->order) {
+        const coul_molecule& m = molecules[i];
+        MolDesc d{};
+        d.atoms = reinterpret_cast<const float4*>(m.d_atoms);
+        d.n_atoms = m.n_atoms;
+        d.out = m.d_out;
+        d.nx = m.grid.nx;
+        d.ny = m.grid.ny;
+        d.nz = m.grid.nz;
+        d.h = m.grid.spacing;
+        d.ox = m.grid.origin[0];
+        d.oy = m.grid.origin[1];
+        d.oz = m.grid.origin[2];
+        d.tiles_x = static_cast<int>((m.grid.nx + span_x - 1) / span_x);
+        d.tiles_y = (m.grid.ny + tune->block_y - 1) / tune->block_y;
+        const int tiles_z = (m.grid.nz + tune->z_iterations - 1) / tune->z_iterations;
+        const int xp = tune->x_points;
+        d.vec_ok = (xp > 1 && m.grid.nx % xp == 0 &&
+                    (reinterpret_cast<uintptr_t>(m.d_out) % (sizeof(float) * (xp >= 4 ? 4 : xp))) == 0)
+                       ? 1
+                       : 0;
+        d.tile_begin = next;
+        next += static_cast<int64_t>(d.tiles_x) * d.tiles_y * tiles_z;
+        b->total_pairs += pairs(i);
+        descs.push_back(d);
+    }
+    b->total_items = next;
+
+    cudaError_t e;
+    int blocks_per_sm = 0;
+    b->smem = kStages * kTileAtoms * 16 + kStages * 8;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, b->variant->kernel, threads, b->smem)) !=
+            cudaSuccess ||
+        blocks_per_sm < 1) {
+        batch_release(b);
+        return e != cudaSuccess ? cuda_error(e, "occupancy query")
+                                : set_error(COUL_ERR_DEVICE_LIMITS, "persistent kernel does not fit on an SM");
+    }
+    b->grid_ctas = blocks_per_sm * ctx->sm_count;
+    if ((e = cudaMalloc(&b->d_mols, sizeof(MolDesc) * std::max<size_t>(descs.size(), 1))) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_counter, sizeof(unsigned long long))) != cudaSuccess ||
+        (!descs.empty() && (e = cudaMemcpy(b->d_mols, descs.data(), sizeof(MolDesc) * descs.size(),
+                                           cudaMemcpyHostToDevice)) != cudaSuccess) ||
+        (e = cudaStreamCreateWithFlags(&b->capture_stream, cudaStreamNonBlocking)) != cudaSuccess) {
+        batch_release(b);
+        return set_error(COUL_ERR_OUT_OF_MEMORY, std::string("batch set-up: ") + cudaGetErrorString(e));
+    }
+    *out = b;
+    return COUL_OK;
+}
+
+COUL_API int coul_batch_destroy(coul_batch* batch)
+{
+    if (batch == nullptr)
+        return COUL_OK;
+    if (batch->ctx)
+        cudaSetDevice(batch->ctx->device);
+    if (batch->ctx && batch->ctx->stream)
+        cudaStreamSynchronize(batch->ctx->stream);
+    batch_release(batch);
+    return COUL_OK;
+}
+
+COUL_API int coul_batch_info(const coul_batch* batch, int64_t* work_items, int* grid_ctas, double* total_pairs)
+{
+    if (batch == nullptr)
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "batch is NULL");
+    if (work_items)
+        *work_items = batch->total_items;
+    if (grid_ctas)
+        *grid_ctas = batch->grid_ctas;
+    if (total_pairs)
+        *total_pairs = batch->total_pairs;
+    return COUL_OK;
+}
+
+COUL_API int coul_batch_run(coul_ctx* ctx, coul_batch* b, int mode, int accumulate)
+{
+    if (ctx == nullptr || b == nullptr || b->ctx != ctx)
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "batch does not belong to this context");
+    int rc = ctx_activate(ctx);
+    if (rc)
+        return rc;
+    accumulate = accumulate ? 1 : 0;
+    cudaError_t e = cudaSuccess;
+    if (mode == COUL_BATCH_GRAPH && (b->graph_exec == nullptr || b->graph_accumulate != accumulate)) {
+        // Capture (counter reset, persistent launch) once on a private stream; replay on any stream.
+        if (b->graph_exec) {
+            cudaGraphExecDestroy(b->graph_exec);
+            b->graph_exec = nullptr;
+        }
+        if (b->graph) {
+            cudaGraphDestroy(b->graph);
+            b->graph = nullptr;
+        }
+        if ((e = cudaStreamBeginCapture(b->capture_stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+            return cuda_error(e, "graph capture");
+        const cudaError_t le = launch_batched(b, b->capture_stream, accumulate);
+        e = cudaStreamEndCapture(b->capture_stream, &b->graph);
+        if (le != cudaSuccess)
+            return cuda_error(le, "captured launch");
+        if (e != cudaSuccess)
+            return cuda_error(e, "graph capture end");
+        if ((e = cudaGraphInstantiate(&b->graph_exec, b->graph, 0)) != cudaSuccess)
+            return cuda_error(e, "graph instantiation");
+        b->graph_accumulate = accumulate;
+    }
+    if ((rc = ctx_begin_timing(ctx)))
+        return rc;
+    switch (mode) {
+    case COUL_BATCH_PERSISTENT:
+        e = launch_batched(b, ctx->stream, accumulate);
+        break;
+    case COUL_BATCH_GRAPH:
+        e = cudaGraphLaunch(b->graph_exec, ctx->stream);
+        break;
+    case COUL_BATCH_SEPARATE: {
+        // The baseline: one plain forward launch per molecule, same tile shape.
+        coul_tune t = b->tune;
+        const VariantEntry* v = nullptr;
+        if ((rc = validate_tune(&t, kModeGrid3d, 0, &v)))
+            return rc;
+        for (const auto& m : b->molecules) {
+            FwdParams p{};
+            p.atoms = reinterpret_cast<const float4*>(m.d_atoms);
+            p.n_atoms = m.n_atoms;
+            p.nx = m.grid.nx;
+            p.ny = m.grid.ny;
+            p.nz = m.grid.nz;
+            p.h = m.grid.spacing;
+            p.ox = m.grid.origin[0];
+            p.oy = m.grid.origin[1];
+            p.oz = m.grid.origin[2];
+            p.out = m.d_out;
+            p.accumulate = accumulate;
+            if ((rc = launch_forward(ctx, v, p, kModeGrid3d, &t)))
+                return rc;
+        }
+        break;
+    }
+    default:
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "unknown batch mode");
+    }
+    if (e != cudaSuccess)
+        return cuda_error(e, "batched launch");
+    return ctx_end_timing(ctx);
+}
+
+}  // extern "C"

@@ -90,21 +90,31 @@ __device__ __forceinline__ void store_points(float* __restrict__ row, int x0, in
     }
 }
 
+// Shared-memory ring of the TMA-staged atom stream: kStages stages of kTileAtoms float4 (or four
+// float arrays), followed by one mbarrier per stage.
+__device__ __forceinline__ void ring_init(uint64_t* full, const int tid)
+{
+    if (tid == 0) {
+#pragma unroll
+        for (int s = 0; s < kStages; ++s)
+            mbar_init(&full[s], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+}
+
+// One thread's work for one tile: accumulate the potential of its register block of points
+// (x0.., yrow, z0.. in 3D; x0.., rows yrow.. in 2D) over all atoms of p, then store it.  With
+// SRC == kSrcShared the atoms come through the CTA's TMA ring (tiles / full); gstage counts the
+// ring's stages across calls, so a persistent kernel can run many tiles through one ring.  Every
+// thread of the CTA must call this together (it synchronises per stage).  Returns false when a
+// bounded wait on the ring expired (the status word is set; nothing was stored).
 template <int ZI, int XP, int UNR, int SRC, int SOA, int PREC, int SOFT, int MODE>
-__global__ void __launch_bounds__(kMaxThreads) fwd_kernel(const FwdParams p, const int vec_ok)
+__device__ __forceinline__ bool tile_pass(const FwdParams& p, const int x0, const int yrow, const int z0, const int vec_ok,
+                                          unsigned char* tiles, uint64_t* full, uint32_t& gstage)
 {
     static_assert(XP == 1 || XP == 2 || XP == 4 || XP == 8, "XP must be 1, 2, 4 or 8");
     static_assert(kTileAtoms % kSubTile == 0, "sub-tiles must divide the stage");
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    const int x0 = (blockIdx.x * blockDim.x + tx) * XP;
-    int yrow, z0;
-    if constexpr (MODE == kModeGrid3d) {
-        yrow = blockIdx.y * blockDim.y + ty;
-        z0 = blockIdx.z * ZI;
-    } else {
-        yrow = (blockIdx.y * blockDim.y + ty) * ZI;
-        z0 = 0;
-    }
 
     float gx[XP];
 #pragma unroll
@@ -174,17 +184,16 @@ __global__ void __launch_bounds__(kMaxThreads) fwd_kernel(const FwdParams p, con
 
     if constexpr (SRC == kSrcConstant) {
         static_assert(PREC == kPrecFp32 && SOA == 0, "constant-memory variants are plain FP32 AoS");
+        (void)tiles;
+        (void)full;
+        (void)gstage;
         const int n = static_cast<int>(p.n_atoms);
 #pragma unroll UNR
         for (int j = 0; j < n; ++j)
             eval_atom<MODE, XP, ZH, SOFT>(gx, gy, gb, c_atoms[j], acc);
     } else {
-        extern __shared__ __align__(128) unsigned char smem_raw[];
-        // Stage layout: AoS kTileAtoms float4; SoA four arrays of kTileAtoms floats (x, y, z, q).
-        unsigned char* tiles = smem_raw;
-        uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + kStages * kTileAtoms * 16);
         const int nthreads = blockDim.x * blockDim.y;
-        const int tid = ty * blockDim.x + tx;
+        const int tid = threadIdx.y * blockDim.x + threadIdx.x;
         const int64_t n = p.n_atoms;
         const int64_t nst = (n + kTileAtoms - 1) / kTileAtoms;
 
@@ -194,7 +203,7 @@ __global__ void __launch_bounds__(kMaxThreads) fwd_kernel(const FwdParams p, con
         };
         // Producer: one thread arms the stage's barrier with the byte count and starts the copies.
         auto issue = [&](int64_t s) {
-            const int buf = static_cast<int>(s % kStages);
+            const int buf = static_cast<int>((gstage + static_cast<uint32_t>(s)) % kStages);
             const int64_t base = s * kTileAtoms;
             const int cnt = stage_count(s);
             unsigned char* dst = tiles + buf * kTileAtoms * 16;
@@ -216,20 +225,14 @@ __global__ void __launch_bounds__(kMaxThreads) fwd_kernel(const FwdParams p, con
         };
 
         if (tid == 0) {
-#pragma unroll
-            for (int s = 0; s < kStages; ++s)
-                mbar_init(&full[s], 1);
-            fence_mbar_init();
-        }
-        __syncthreads();
-        if (tid == 0) {
             for (int64_t s = 0; s < nst && s < kStages; ++s)
                 issue(s);
         }
 
         for (int64_t s = 0; s < nst; ++s) {
-            const int buf = static_cast<int>(s % kStages);
-            const uint32_t parity = static_cast<uint32_t>((s / kStages) & 1);
+            const uint32_t g = gstage + static_cast<uint32_t>(s);
+            const int buf = static_cast<int>(g % kStages);
+            const uint32_t parity = static_cast<uint32_t>((g / kStages) & 1);
             const bool ok = mbar_wait_bounded(&full[buf], parity);
             const int cnt = stage_count(s);
             unsigned char* tile = tiles + buf * kTileAtoms * 16;
@@ -262,10 +265,12 @@ __global__ void __launch_bounds__(kMaxThreads) fwd_kernel(const FwdParams p, con
                 // and leave without storing.
                 if (tid == 0) {
                     report_status(p.status, kStatusTimeout);
-                    for (int64_t r = s; r < nst && r < s + kStages; ++r)
-                        (void)mbar_wait_bounded(&full[r % kStages], static_cast<uint32_t>((r / kStages) & 1));
+                    for (int64_t r = s; r < nst && r < s + kStages; ++r) {
+                        const uint32_t gr = gstage + static_cast<uint32_t>(r);
+                        (void)mbar_wait_bounded(&full[gr % kStages], static_cast<uint32_t>((gr / kStages) & 1));
+                    }
                 }
-                return;
+                return false;
             }
 
             auto atom_at = [&](int j) -> float4 {
@@ -296,6 +301,7 @@ __global__ void __launch_bounds__(kMaxThreads) fwd_kernel(const FwdParams p, con
             if (tid == 0 && s + kStages < nst)
                 issue(s + kStages);
         }
+        gstage += static_cast<uint32_t>(nst);
     }
 
     float val[XP][ZI];
@@ -331,6 +337,31 @@ __global__ void __launch_bounds__(kMaxThreads) fwd_kernel(const FwdParams p, con
     (void)part;
     (void)cmp;
     (void)acc64;
+    return true;
+}
+
+// One tile per CTA: the block's position in the launch grid selects the tile.
+template <int ZI, int XP, int UNR, int SRC, int SOA, int PREC, int SOFT, int MODE>
+__global__ void __launch_bounds__(kMaxThreads) fwd_kernel(const FwdParams p, const int vec_ok)
+{
+    const int x0 = (blockIdx.x * blockDim.x + threadIdx.x) * XP;
+    int yrow, z0;
+    if constexpr (MODE == kModeGrid3d) {
+        yrow = blockIdx.y * blockDim.y + threadIdx.y;
+        z0 = blockIdx.z * ZI;
+    } else {
+        yrow = (blockIdx.y * blockDim.y + threadIdx.y) * ZI;
+        z0 = 0;
+    }
+    uint32_t gstage = 0;
+    if constexpr (SRC == kSrcShared) {
+        extern __shared__ __align__(128) unsigned char smem_raw[];
+        uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + kStages * kTileAtoms * 16);
+        ring_init(full, threadIdx.y * blockDim.x + threadIdx.x);
+        (void)tile_pass<ZI, XP, UNR, SRC, SOA, PREC, SOFT, MODE>(p, x0, yrow, z0, vec_ok, smem_raw, full, gstage);
+    } else {
+        (void)tile_pass<ZI, XP, UNR, SRC, SOA, PREC, SOFT, MODE>(p, x0, yrow, z0, vec_ok, nullptr, nullptr, gstage);
+    }
 }
 
 // ------------------------------------------------------------------------------------------

@@ -1,0 +1,68 @@
+"""The batched persistent path: (molecule, tile) work items from a device queue, one launch,
+optionally replayed from a CUDA graph, against one plain launch per molecule and the FP64 oracle."""
+import numpy as np
+import pytest
+
+import oracle
+from ktt_b200 import errors, workloads
+import ktt_b200
+
+pytestmark = pytest.mark.gpu
+
+
+def _small_batch(seed=21, n_mol=24, lo=50, hi=3000):
+    return workloads.molecule_batch(seed=seed, n_mol=n_mol, lo=lo, hi=hi)
+
+
+@pytest.mark.parametrize("tune", [
+    ktt_b200.Tune(z_iterations=8, x_points=2, unroll=2, rsqrt_soft=2),
+    ktt_b200.Tune(z_iterations=16, x_points=1, rsqrt_soft=2, block_x=64, block_y=2),
+    ktt_b200.Tune(z_iterations=8, x_points=2, precision=ktt_b200.PREC_FP64_MERGE, rsqrt_soft=2),
+])
+def test_persistent_graph_and_separate_agree_bitwise(ctx, tune):
+    import torch
+    mols = _small_batch()
+    inputs = [(torch.from_numpy(m.atoms).cuda(), m.dims, m.spacing, m.origin) for m in mols]
+    b = ktt_b200.Batch(ctx, inputs, tune)
+    assert b.work_items > 0 and b.grid_ctas >= ctx.sm_count
+    maps = {}
+    for mode in (ktt_b200.BATCH_SEPARATE, ktt_b200.BATCH_PERSISTENT, ktt_b200.BATCH_GRAPH):
+        for o in b.outputs:
+            o.fill_(float("nan"))
+        b.run(mode)
+        ctx.synchronize()
+        maps[mode] = [o.cpu().numpy().copy() for o in b.outputs]
+    for a, p, g in zip(maps[ktt_b200.BATCH_SEPARATE], maps[ktt_b200.BATCH_PERSISTENT], maps[ktt_b200.BATCH_GRAPH]):
+        assert np.array_equal(a.view(np.uint32), p.view(np.uint32))
+        assert np.array_equal(a.view(np.uint32), g.view(np.uint32))
+    # graph replay again (accumulate) adds the same map on top
+    b.run(ktt_b200.BATCH_GRAPH, accumulate=True)
+    ctx.synchronize()
+    for o, ref in zip(b.outputs, maps[ktt_b200.BATCH_GRAPH]):
+        np.testing.assert_allclose(o.cpu().numpy(), 2 * ref, rtol=1e-6, atol=1e-6)
+    b.close()
+
+
+def test_batched_against_oracle(ctx):
+    import torch
+    mols = _small_batch(seed=22, n_mol=10)
+    inputs = [(torch.from_numpy(m.atoms).cuda(), m.dims, m.spacing, m.origin) for m in mols]
+    b = ktt_b200.Batch(ctx, inputs)
+    b.run(ktt_b200.BATCH_GRAPH)
+    ctx.synchronize()
+    for m, out in zip(mols, b.outputs):
+        total = int(np.prod(m.dims))
+        idx = workloads.subset_indices(total, min(1.0, 3000 / total), seed=5)
+        ref = oracle.points3d(m.atoms, m.spacing, m.dims, idx, origin=m.origin)
+        rep = errors.report(out.cpu().numpy().reshape(-1)[idx], ref)
+        assert rep["rel_norm"] <= 1e-5, rep
+    b.close()
+
+
+def test_batch_rejects_unsupported_shape(ctx):
+    import torch
+    mols = _small_batch(n_mol=2)
+    inputs = [(torch.from_numpy(m.atoms).cuda(), m.dims, m.spacing, m.origin) for m in mols]
+    with pytest.raises(ktt_b200.CoulombError) as e:
+        ktt_b200.Batch(ctx, inputs, ktt_b200.Tune(z_iterations=32, x_points=4, rsqrt_soft=1))
+    assert e.value.status == ktt_b200.COUL_ERR_UNSUPPORTED
