@@ -228,6 +228,31 @@ COUL_API int coul_batch_destroy(coul_batch* batch);
 COUL_API int coul_batch_run(coul_ctx* ctx, coul_batch* batch, int mode, int accumulate);
 COUL_API int coul_batch_info(const coul_batch* batch, int64_t* work_items, int* grid_ctas, double* total_pairs);
 
+/*
+ * The batched map without any device allocation.  No counterpart in the reference (KTT allocates
+ * a buffer for every kernel argument).  For callers that must not allocate device memory from a
+ * library: a host application that gives all free device memory to its own pool at start-up, a
+ * latency-critical loop that cannot take the device-wide synchronisation of cudaFree, a plug-in
+ * whose host owns every allocation.  Computes the same maps as coul_batch_create + coul_batch_run
+ * (COUL_BATCH_PERSISTENT) on the current device and the given cudaStream_t (NULL = legacy default
+ * stream), but keeps the work-queue counter and the molecule table in a fixed static device array
+ * of the library (73,984 bytes, held by every GPU that loads the library until the process exits) and
+ * calls no cudaMalloc, cudaFree or other allocating routine.  The caller passes the atom and output
+ * buffers as in coul_molecule, and optionally d_status, an int in device memory that the kernel sets
+ * to non-zero if a bounded device-side wait expires (the caller clears it).
+ *   - at most 1024 molecules per call (larger batches are rejected with COUL_ERR_INVALID_ARGUMENT);
+ *   - tile shapes (z_iterations/x_points/unroll/precision/rsqrt_soft, any block up to 256 threads):
+ *     8/2/2/0/2, 8/2/1/0/0, 16/1/1/0/2; others return COUL_ERR_UNSUPPORTED;
+ *   - the first call on a device looks up the device address of the static array
+ *     (cudaGetSymbolAddress) with that device current; make that first call before any stream
+ *     capture;
+ *   - every call shares the one array and leaves its table behind; calls whose kernels overlap on
+ *     the GPU (different streams without ordering) race on it and give wrong maps.
+ * Returns after enqueueing (the molecule table is copied from host memory before it returns).
+ */
+COUL_API int coul_batch_run_static(void* stream, const coul_molecule* molecules, int n_molecules,
+                                   const coul_tune* tune, int accumulate, int* d_status);
+
 /* ---- roofline ------------------------------------------------------------------ */
 /*
  * Measures, on the context's device at its current clocks, the whole-GPU rate of MUFU reciprocal
