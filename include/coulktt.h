@@ -195,6 +195,20 @@ COUL_API int coul_slice_atoms(coul_ctx* ctx, const float* d_xyzq, int64_t n_atom
 COUL_API int coul_forward_3d_host(coul_ctx* ctx, const float* h_atoms, int64_t n_atoms, const coul_grid* grid,
                                   const coul_tune* tune, float* h_out);
 
+/* ---- adjoint: gradient of a loss on the map ----------------------------------------- */
+/*
+ * Given G = dL/dV on the nx*ny*nz grid (d_grad_map, x fastest) for the map of coul_forward_3d,
+ * writes d_grad_q[j] = dL/dq_j = sum_i G_i / r_ij and d_grad_xyz[3j..3j+2] = dL/dr_j =
+ * q_j sum_i G_i (r_i - r_j) / r_ij^3 (either output may be NULL).  1/r is recomputed, nothing is
+ * stored per pair; partial sums are FP64 and added in a fixed order (deterministic).  For the weighted
+ * least-squares loss L = 0.5 sum_i w_i (V_i - T_i)^2 pass G_i = w_i (V_i - T_i).  No counterpart in KTT
+ * (it tunes forward kernels only); the PyTorch binding wraps forward + adjoint as an autograd function.
+ * Asynchronous on the context's stream; keeps an FP64 workspace of 32 * n_atoms * chunks bytes in the
+ * context (chunks ~ 24 * SMs / atom tiles).
+ */
+COUL_API int coul_adjoint_3d(coul_ctx* ctx, const float* d_atoms, int64_t n_atoms, const coul_grid* grid,
+                             const float* d_grad_map, float* d_grad_q, float* d_grad_xyz);
+
 /* ---- batched: many molecules in one persistent launch ------------------------------ */
 /*
  * A batch of molecules with uneven atom counts and grids, computed by one persistent launch that

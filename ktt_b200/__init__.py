@@ -308,6 +308,62 @@ class CoulombContext:
         return out
 
 
+def adjoint_3d(ctx: "CoulombContext", atoms, dims, spacing, grad_map, origin=None):
+    """dL/dr and dL/dq for G = dL/dV on the map: returns an (n, 4) tensor (dx, dy, dz, dq)."""
+    import torch
+    CoulombContext._check_atoms(atoms)
+    nx, ny, nz = (int(d) for d in dims)
+    g = grad_map.contiguous().to(torch.float32)
+    if g.numel() != nx * ny * nz or not g.is_cuda:
+        raise CoulombError(COUL_ERR_INVALID_ARGUMENT, "grad_map must be a CUDA tensor with nx*ny*nz elements")
+    n = atoms.shape[0]
+    grad_q = torch.empty(n, dtype=torch.float32, device=atoms.device)
+    grad_xyz = torch.empty((n, 3), dtype=torch.float32, device=atoms.device)
+    ctx._bind_stream()
+    grid = _grid(dims, spacing, origin)
+    _check(ctx._lib.coul_adjoint_3d(ctx.handle, _ptr(atoms), n, ctypes.byref(grid), _ptr(g), _ptr(grad_q),
+                                    _ptr(grad_xyz)))
+    return torch.cat([grad_xyz, grad_q[:, None]], dim=1)
+
+
+def _autograd_function():
+    import torch
+
+    class CoulombMapFunction(torch.autograd.Function):
+        """V = map(atoms) with atoms (n, 4) = (x, y, z, q); backward through the sm_100a adjoint
+        kernel (1/r recomputed, FP64 partial sums) -- gradients for positions and charges."""
+
+        @staticmethod
+        def forward(fctx, atoms, ctx, dims, spacing, origin, tune):
+            a = atoms.detach().contiguous()
+            out = ctx.forward_3d(a, dims, spacing, origin, tune=tune)
+            fctx.save_for_backward(a)
+            fctx.coul = (ctx, dims, spacing, origin)
+            return out
+
+        @staticmethod
+        def backward(fctx, grad_out):
+            (a,) = fctx.saved_tensors
+            ctx, dims, spacing, origin = fctx.coul
+            grad = adjoint_3d(ctx, a, dims, spacing, grad_out, origin)
+            return grad, None, None, None, None, None
+
+    return CoulombMapFunction
+
+
+_MAP_FUNCTION = None
+
+
+def coulomb_map(atoms, ctx: "CoulombContext", dims, spacing, origin=None, tune: Tune | None = None):
+    """Differentiable potential map: a torch.autograd.Function over the forward and adjoint kernels.
+
+    atoms: (n, 4) float32 CUDA tensor (x, y, z, q), may require grad; returns (nz, ny, nx)."""
+    global _MAP_FUNCTION
+    if _MAP_FUNCTION is None:
+        _MAP_FUNCTION = _autograd_function()
+    return _MAP_FUNCTION.apply(atoms, ctx, tuple(int(d) for d in dims), float(spacing), origin, tune)
+
+
 BATCH_PERSISTENT = 0
 BATCH_GRAPH = 1
 BATCH_SEPARATE = 2

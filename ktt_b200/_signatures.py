@@ -18,6 +18,7 @@ def register(lib) -> None:
         "coul_batch_run": [vp, vp, ci, ci],
         "coul_batch_info": [vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ci), ctypes.POINTER(ctypes.c_double)],
         "coul_pack_atoms": [vp, vp, vp, vp, vp, ctypes.c_int64, vp],
+        "coul_adjoint_3d": [vp, vp, ctypes.c_int64, ctypes.POINTER(_Grid), vp, vp, vp],
         "coul_buffer_alloc": [vp, ctypes.c_size_t, ctypes.POINTER(vp)],
         "coul_buffer_free": [vp, vp],
         "coul_buffer_upload": [vp, vp, vp, ctypes.c_size_t],

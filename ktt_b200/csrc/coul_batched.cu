@@ -42,6 +42,9 @@ static const std::vector<BatchVariant>& batch_variants()
         batch_variant<8, 4, 1, kPrecFp32, 2>(),      batch_variant<16, 1, 1, kPrecFp32, 2>(),
         batch_variant<16, 2, 1, kPrecFp32, 2>(),     batch_variant<8, 2, 1, kPrecFp64Merge, 2>(),
         batch_variant<8, 2, 1, kPrecCompensated, 2>(),
+        // narrow x spans for small grids (less tile padding on 57..149-point rows)
+        batch_variant<8, 1, 2, kPrecFp32, 2>(),      batch_variant<8, 1, 1, kPrecFp32, 2>(),
+        batch_variant<8, 1, 2, kPrecFp32, 0>(),      batch_variant<4, 1, 2, kPrecFp32, 2>(),
     };
     return v;
 }

@@ -12,6 +12,8 @@ static void add_soft(std::vector<VariantEntry>& v)
     add_variant<4, 2, 1, kSrcShared, 0, PREC, SOFT, kModeGrid3d>(v);
     add_variant<4, 4, 1, kSrcShared, 0, PREC, SOFT, kModeGrid3d>(v);
     add_variant<8, 1, 1, kSrcShared, 0, PREC, SOFT, kModeGrid3d>(v);
+    add_variant<8, 1, 2, kSrcShared, 0, PREC, SOFT, kModeGrid3d>(v);
+    add_variant<4, 1, 2, kSrcShared, 0, PREC, SOFT, kModeGrid3d>(v);
     add_variant<8, 2, 1, kSrcShared, 0, PREC, SOFT, kModeGrid3d>(v);
     add_variant<8, 2, 2, kSrcShared, 0, PREC, SOFT, kModeGrid3d>(v);
     add_variant<8, 4, 1, kSrcShared, 0, PREC, SOFT, kModeGrid3d>(v);

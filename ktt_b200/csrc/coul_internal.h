@@ -26,6 +26,7 @@ struct coul_ctx {
     int cc_major = 0;
     int cc_minor = 0;
     std::vector<std::function<void()>> cleanups;  // frees buffers owned by other units (run at destroy)
+    void* adjoint_workspace = nullptr;            // FP64 partials of coul_adjoint_3d (coul_adjoint.cu)
 };
 
 namespace coul {

@@ -1,0 +1,108 @@
+"""The adjoint kernel and its torch.autograd.Function against FP64 references.
+
+L = 0.5 sum_i w_i (V_i - T_i)^2 with w = 0 within 1.5 A of any atom.  The GPU gradient (forward map
+in the FP64-merge form, adjoint with FP64 partial sums) is compared with the oracle's FP64 gradient
+and with FP64 central finite differences (h = 1e-4) of the oracle's FP64 loss; tolerance 1e-4
+relative (normwise over the checked atoms, per component kind).
+"""
+import numpy as np
+import pytest
+
+import oracle
+from ktt_b200 import workloads
+import ktt_b200
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-4
+FORWARD = dict(z_iterations=8, x_points=2, precision=ktt_b200.PREC_FP64_MERGE)
+
+
+def _gpu_loss_and_grad(ctx, atoms, dims, h, target, weight, origin=None):
+    import torch
+    a = torch.from_numpy(atoms).cuda().requires_grad_(True)
+    t = torch.from_numpy(target.reshape(dims[::-1])).cuda()
+    w = torch.from_numpy(weight.reshape(dims[::-1])).cuda()
+    v = ktt_b200.coulomb_map(a, ctx, dims, h, origin, ktt_b200.Tune(**FORWARD))
+    loss = 0.5 * (w.double() * (v.double() - t.double()) ** 2).sum()
+    loss.backward()
+    return float(loss.item()), a.grad.cpu().numpy().astype(np.float64)
+
+
+def _rel(got, ref):
+    return float(np.max(np.abs(got - ref)) / max(np.max(np.abs(ref)), 1e-300))
+
+
+def test_adjoint_small_against_fp64_gradient(ctx):
+    rng = np.random.default_rng(3)
+    n, dims, h, origin = 300, (40, 33, 27), 0.5, (-2.0, 1.0, 0.5)
+    atoms = np.empty((n, 4), dtype=np.float32)
+    atoms[:, :3] = rng.uniform(0.0, 16.0, (n, 3))
+    atoms[:, 3] = rng.uniform(-1, 1, n)
+    target = rng.normal(0, 1, dims[::-1]).astype(np.float32)
+    weight = workloads.exclusion_weights(atoms, dims, h, 1.5, origin)
+    loss, grad = _gpu_loss_and_grad(ctx, atoms, dims, h, target, weight, origin)
+    ref_loss, dq, dr = oracle.adjoint3d(atoms, h, dims, target, weight, origin=origin)
+    assert abs(loss - ref_loss) <= 1e-5 * ref_loss
+    assert _rel(grad[:, 3], dq) <= TOL
+    assert _rel(grad[:, :3], dr) <= TOL
+
+
+def test_adjoint_config5_finite_differences_and_reference(ctx):
+    """8,192 atoms in a 64 A cube, 128^3 grid at 0.5 A; the target map from charges perturbed by
+    N(0, 0.1); FD and FP64 gradient on 64 seeded atoms."""
+    import torch
+    atoms, q_target, dims, h, excl = workloads.adjoint_problem()
+    weight = workloads.exclusion_weights(atoms, dims, h, excl)
+    target_atoms = atoms.copy()
+    target_atoms[:, 3] = q_target
+    target = ctx.forward_3d(torch.from_numpy(target_atoms).cuda(), dims, h,
+                            tune=ktt_b200.Tune(**FORWARD)).cpu().numpy()
+    loss, grad = _gpu_loss_and_grad(ctx, atoms, dims, h, target, weight)
+
+    sel = np.sort(np.random.default_rng(17).choice(atoms.shape[0], 64, replace=False))
+    ref_loss, dq, dr, vmap = oracle.adjoint3d(atoms, h, dims, target, weight, sel=sel, want_map=True)
+    assert abs(loss - ref_loss) <= 1e-5 * ref_loss
+    assert _rel(grad[sel, 3], dq) <= TOL
+    assert _rel(grad[sel, :3], dr) <= TOL
+
+    eps = 1e-4
+    fd = np.empty((sel.size, 4))
+    for n_, j in enumerate(sel):
+        base = atoms[j].astype(np.float64)
+        for c in range(4):
+            plus, minus = base.copy(), base.copy()
+            plus[c] += eps
+            minus[c] -= eps
+            lp = oracle.loss_perturbed(atoms, int(j), plus, h, dims, target, vmap, weight)
+            lm = oracle.loss_perturbed(atoms, int(j), minus, h, dims, target, vmap, weight)
+            fd[n_, c] = (lp - lm) / (2 * eps)
+    assert _rel(grad[sel, 3], fd[:, 3]) <= TOL
+    assert _rel(grad[sel, :3], fd[:, :3]) <= TOL
+
+
+def test_adam_charge_fitting(ctx):
+    """100 Adam steps on the charges through the autograd function: the loss falls by orders of
+    magnitude and the charges move toward the ones that made the target map."""
+    import torch
+    atoms, q_target, dims, h, excl = workloads.adjoint_problem(seed=6, n_atoms=4096, n=96, box=48.0)
+    weight = torch.from_numpy(workloads.exclusion_weights(atoms, dims, h, excl)).cuda()
+    target_atoms = atoms.copy()
+    target_atoms[:, 3] = q_target
+    tune = ktt_b200.Tune(**FORWARD)
+    target = ctx.forward_3d(torch.from_numpy(target_atoms).cuda(), dims, h, tune=tune)
+    xyz = torch.from_numpy(atoms[:, :3].copy()).cuda()
+    q = torch.from_numpy(atoms[:, 3].copy()).cuda().requires_grad_(True)
+    opt = torch.optim.Adam([q], lr=0.02)
+    losses = []
+    for _ in range(100):
+        opt.zero_grad()
+        v = ktt_b200.coulomb_map(torch.cat([xyz, q[:, None]], dim=1), ctx, dims, h, None, tune)
+        loss = 0.5 * (weight * (v - target) ** 2).sum()
+        loss.backward()
+        opt.step()
+        losses.append(float(loss.item()))
+    q_err0 = np.abs(atoms[:, 3] - q_target).mean()
+    q_err = np.abs(q.detach().cpu().numpy() - q_target).mean()
+    assert losses[-1] < 0.02 * losses[0], losses[::10]
+    assert q_err < 0.5 * q_err0, (q_err, q_err0)
