@@ -77,6 +77,17 @@ class Tune:
         return {f.name: int(getattr(self, f.name)) for f in fields(self)}
 
 
+def tuned(name: str, key: str = "tune") -> Tune | None:
+    """A configuration the autotuner stored under ktt_b200/tuned/<name>.json (None if absent)."""
+    import json
+    path = os.path.join(os.path.dirname(__file__), "tuned", name + ".json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        entry = json.load(f).get(key)
+    return Tune(**entry) if entry else None
+
+
 _lib = None
 
 
@@ -393,7 +404,8 @@ class Batch:
             arr[i].n_atoms = atoms.shape[0]
             arr[i].grid = _grid(dims, spacing, origin)
             arr[i].d_out = out.data_ptr()
-        self.tune = tune or Tune(z_iterations=8, x_points=2, unroll=2, rsqrt_soft=2)
+        self.tune = tune or tuned("b200_batch", "batched") or Tune(z_iterations=8, x_points=2, unroll=2,
+                                                                  rsqrt_soft=2)
         t = self.tune.c()
         self._handle = ctypes.c_void_p()
         ctx._bind_stream()

@@ -1,16 +1,96 @@
 """Measure the batched persistent path on the uneven-molecule batch.
 
-    python -m ktt_b200.run_batch [--molecules 512] [--repeat 3] [--set field=value ...]
+    python -m ktt_b200.run_batch [--molecules 512] [--repeat 3] [--margin 8] [--set field=value ...]
+    python -m ktt_b200.run_batch --autotune [--save ktt_b200/tuned/b200_batch.json]
 
 512 molecules with atom counts log-uniform in [200, 20000] (seeded), atoms uniform in a cube of side
-(n / 0.1)^(1/3) A, grids = bounding box + 8 A margin at 0.5 A.  Prints one JSON line with the
-device time and pair rate of: one persistent launch, its CUDA-graph replay, and one plain launch
-per molecule.
+(n / 0.1)^(1/3) A, grids = bounding box + `margin` A on every side at 0.5 A.  Prints one JSON line
+with the device time and pair rate of: one persistent launch, its CUDA-graph replay, one launch of
+the same kernel form per molecule, and one synchronous launch per molecule of KTT's kernel form
+(atoms in __constant__ memory, all rsqrts on MUFU, FP32; what a KTT user's per-molecule Tuner::Run
+loop launches).
+
+--autotune searches the batched kernel's tile space (the compiled batch variants x CTA shapes) on
+the batch itself, exhaustively or on a seeded random sample of --budget configurations, each timed
+as a graph replay; the KTT-form baseline's (z_iterations, x_points, CTA shape) is searched the
+same way, so both arms run at their best tile shape.
 """
 from __future__ import annotations
 
 import argparse
 import json
+import os
+import random
+
+# compiled batch variants: (z_iterations, x_points, unroll, precision, rsqrt_soft)
+BATCH_FORMS = [(8, 2, 2, 0, 2), (8, 2, 1, 0, 2), (8, 2, 2, 0, 0), (8, 2, 1, 0, 0), (4, 2, 1, 0, 2),
+               (4, 4, 1, 0, 2), (8, 4, 1, 0, 2), (16, 1, 1, 0, 2), (16, 2, 1, 0, 2), (8, 1, 2, 0, 2),
+               (8, 1, 1, 0, 2), (8, 1, 2, 0, 0), (4, 1, 2, 0, 2)]
+CTA_SHAPES = [(8, 16), (16, 8), (32, 4), (8, 8), (16, 16), (4, 32), (8, 32), (32, 8)]
+KTT_FORMS = [(zi, xp) for zi in (4, 8, 16) for xp in (1, 2, 4)]
+KTT_CTA_SHAPES = [(32, 4), (16, 8), (32, 8), (64, 4)]
+DEFAULT_TUNED = os.path.join(os.path.dirname(__file__), "tuned", "b200_batch.json")
+
+
+def _tune(ktt_b200, zi, xp, un, prec, soft, bx, by):
+    return ktt_b200.Tune(block_x=bx, block_y=by, z_iterations=zi, x_points=xp, unroll=un,
+                         precision=prec, rsqrt_soft=soft)
+
+
+def _time_graph(ctx, batch, ktt_b200, repeat):
+    batch.run(ktt_b200.BATCH_GRAPH)
+    ctx.synchronize()
+    ms = []
+    for _ in range(repeat):
+        batch.run(ktt_b200.BATCH_GRAPH)
+        ms.append(ctx.elapsed_ms())
+    return min(ms)
+
+
+def _time_ktt_form(ctx, inputs, outs, tune, repeat):
+    """One forward call per molecule, synchronised after each, as Tuner::Run does; device time of
+    the whole loop from one event pair around it."""
+    import torch
+    stream = torch.cuda.current_stream()
+    best = float("inf")
+    for r in range(repeat + 1):
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        for (atoms, dims, h, origin), out in zip(inputs, outs):
+            ctx.forward_3d(atoms, dims, h, origin, tune=tune, out=out)
+            ctx.synchronize()
+        stop.record(stream)
+        stop.synchronize()
+        if r:
+            best = min(best, start.elapsed_time(stop))
+    return best
+
+
+def autotune(ctx, inputs, ktt_b200, budget, seed, repeat=1):
+    space = [f + s for f in BATCH_FORMS for s in CTA_SHAPES if s[0] * s[1] <= 256]
+    if budget and budget < len(space):
+        space = random.Random(seed).sample(space, budget)
+    trials = []
+    for cfg in space:
+        tune = _tune(ktt_b200, *cfg)
+        batch = ktt_b200.Batch(ctx, inputs, tune)
+        ms = _time_graph(ctx, batch, ktt_b200, repeat)
+        trials.append({"tune": tune.as_dict(), "ms": ms, "gpairs_per_s": batch.total_pairs / (ms * 1e-3) / 1e9})
+        batch.close()
+        print(json.dumps({"trial": trials[-1]}), flush=True)
+    return min(trials, key=lambda t: t["ms"]), len(space)
+
+
+def autotune_ktt_form(ctx, inputs, outs, ktt_b200, pairs):
+    trials = []
+    for zi, xp in KTT_FORMS:
+        for bx, by in KTT_CTA_SHAPES:
+            tune = ktt_b200.Tune(block_x=bx, block_y=by, z_iterations=zi, x_points=xp,
+                                 atom_source=ktt_b200.ATOMS_CONSTANT)
+            ms = _time_ktt_form(ctx, inputs, outs, tune, 1)
+            trials.append({"tune": tune.as_dict(), "ms": ms, "gpairs_per_s": pairs / (ms * 1e-3) / 1e9})
+            print(json.dumps({"ktt_form_trial": trials[-1]}), flush=True)
+    return min(trials, key=lambda t: t["ms"])
 
 
 def main() -> None:
@@ -18,7 +98,12 @@ def main() -> None:
     ap.add_argument("--molecules", type=int, default=512)
     ap.add_argument("--repeat", type=int, default=3)
     ap.add_argument("--seed", type=int, default=4)
+    ap.add_argument("--margin", type=float, default=8.0, help="A of margin on every side of the bounding box")
     ap.add_argument("--set", action="append", default=[], metavar="FIELD=VALUE")
+    ap.add_argument("--autotune", action="store_true")
+    ap.add_argument("--budget", type=int, default=0, help="random sample size for --autotune (0 = all)")
+    ap.add_argument("--save", default="", help="write the autotuned configurations to this JSON file")
+    ap.add_argument("--tuned", default=DEFAULT_TUNED, help="tuned configurations to start from")
     args = ap.parse_args()
 
     import torch
@@ -26,18 +111,39 @@ def main() -> None:
     import ktt_b200
     from ktt_b200 import workloads
 
-    mols = workloads.molecule_batch(seed=args.seed, n_mol=args.molecules)
+    mols = workloads.molecule_batch(seed=args.seed, n_mol=args.molecules, margin=args.margin)
     ctx = ktt_b200.CoulombContext(0)
     inputs = [(torch.from_numpy(m.atoms).cuda(), m.dims, m.spacing, m.origin) for m in mols]
-    tune = ktt_b200.Tune(z_iterations=8, x_points=2, unroll=2, rsqrt_soft=2)
+    outs = [torch.empty((m.dims[2], m.dims[1], m.dims[0]), dtype=torch.float32, device="cuda") for m in mols]
+    pairs = float(sum(m.pairs for m in mols))
+
+    tuned = {}
+    if args.tuned and os.path.exists(args.tuned):
+        with open(args.tuned) as f:
+            tuned = json.load(f)
+    out = {"molecules": len(mols), "margin_per_side": args.margin}
+    if args.autotune:
+        best, searched = autotune(ctx, inputs, ktt_b200, args.budget, args.seed)
+        ktt_best = autotune_ktt_form(ctx, inputs, outs, ktt_b200, pairs)
+        tuned = {"batched": best["tune"], "ktt_form": ktt_best["tune"],
+                 "searched": searched, "workload": f"{len(mols)} molecules, seed {args.seed}, margin {args.margin}"}
+        out["autotune"] = {"configurations": searched, "best": best, "ktt_form_best": ktt_best}
+        if args.save:
+            with open(args.save, "w") as f:
+                json.dump(tuned, f, indent=1)
+                f.write("\n")
+    tune = ktt_b200.Tune(**tuned.get("batched", {})) if tuned else \
+        ktt_b200.Tune(block_x=8, block_y=16, z_iterations=8, x_points=2, unroll=2, rsqrt_soft=2)
+    ktt_tune = ktt_b200.Tune(**tuned["ktt_form"]) if "ktt_form" in tuned else \
+        ktt_b200.Tune(block_x=32, block_y=4, z_iterations=8, x_points=2, atom_source=ktt_b200.ATOMS_CONSTANT)
     for s in args.set:
         k, v = s.split("=", 1)
         setattr(tune, k, int(v))
     batch = ktt_b200.Batch(ctx, inputs, tune)
-    out = {"molecules": len(mols), "pairs": batch.total_pairs, "work_items": batch.work_items,
-           "grid_ctas": batch.grid_ctas, "tune": tune.as_dict(),
-           "atoms_min": min(m.atoms.shape[0] for m in mols), "atoms_max": max(m.atoms.shape[0] for m in mols),
-           "grid_min": min(min(m.dims) for m in mols), "grid_max": max(max(m.dims) for m in mols)}
+    out.update({"pairs": batch.total_pairs, "work_items": batch.work_items,
+                "grid_ctas": batch.grid_ctas, "tune": tune.as_dict(), "ktt_form_tune": ktt_tune.as_dict(),
+                "atoms_min": min(m.atoms.shape[0] for m in mols), "atoms_max": max(m.atoms.shape[0] for m in mols),
+                "grid_min": min(min(m.dims) for m in mols), "grid_max": max(max(m.dims) for m in mols)})
     for name, mode in (("separate", ktt_b200.BATCH_SEPARATE), ("persistent", ktt_b200.BATCH_PERSISTENT),
                        ("graph", ktt_b200.BATCH_GRAPH)):
         batch.run(mode)  # warm-up (and graph instantiation)
@@ -47,7 +153,10 @@ def main() -> None:
             batch.run(mode)
             ms.append(ctx.elapsed_ms())
         out[name] = {"ms": min(ms), "gpairs_per_s": batch.total_pairs / (min(ms) * 1e-3) / 1e9}
+    ms = _time_ktt_form(ctx, inputs, outs, ktt_tune, args.repeat)
+    out["ktt_form_separate"] = {"ms": ms, "gpairs_per_s": pairs / (ms * 1e-3) / 1e9}
     out["speedup_graph_vs_separate"] = out["separate"]["ms"] / out["graph"]["ms"]
+    out["speedup_graph_vs_ktt_form"] = out["ktt_form_separate"]["ms"] / out["graph"]["ms"]
     print(json.dumps(out))
     batch.close()
     ctx.close()

@@ -1,0 +1,91 @@
+"""The single-slice 2D case: one z slice of a 256 x 256 grid at 0.5 A, 4,000 atoms.
+
+    python -m ktt_b200.run_slice2d [--repeat 50]
+
+Atoms x, y ~ U[0, 128), z ~ U[0, 32), q ~ U[-1, 1]; the slice at z = 16 A.  For each 2D tile shape:
+device time of the slice kernel (median of --repeat event-timed launches), pair rate, error against
+the FP64 oracle over the whole slice.  Then the whole call as a KTT user makes it (host atoms in,
+dz^2 slicing on the device, host slice out; wall clock, median) for the fastest shape, and the FP64
+oracle's own time on the host.  One JSON line per measurement.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+import numpy as np
+
+SHAPES = [(bx, by, xp, yi) for (bx, by) in ((32, 4), (32, 2), (64, 2), (16, 8), (32, 8))
+          for xp in (1, 2, 4) for yi in (1, 2, 4)]
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--repeat", type=int, default=50)
+    args = ap.parse_args()
+
+    import torch
+
+    import ktt_b200
+    import oracle
+    from ktt_b200 import errors, workloads
+
+    case = workloads.slice_2d()
+    nx, ny, h = case.nx, case.ny, case.spacing
+    t0 = time.perf_counter()
+    ref = oracle.slice2d(case.ktt_atoms(), h, nx, ny)
+    oracle_s = time.perf_counter() - t0
+    pairs = float(nx * ny * case.atoms.shape[0])
+
+    ctx = ktt_b200.CoulombContext(0)
+    atoms = torch.from_numpy(case.atoms).cuda()
+    d_sliced = ctx.slice_atoms(atoms, case.z_slice)
+    out = torch.empty((ny, nx), dtype=torch.float32, device="cuda")
+    results = []
+    for bx, by, xp, yi in SHAPES:
+        tune = ktt_b200.Tune(block_x=bx, block_y=by, x_points=xp, z_iterations=yi)
+        try:
+            ctx.forward_2d(d_sliced, h, nx, ny, tune=tune, out=out)
+        except ktt_b200.CoulombError:
+            continue
+        ms = []
+        for _ in range(args.repeat):
+            ctx.forward_2d(d_sliced, h, nx, ny, tune=tune, out=out)
+            ms.append(ctx.elapsed_ms())
+        ctx.synchronize()
+        rep = errors.report(out.double().cpu().numpy(), ref)
+        med = float(np.median(ms))
+        line = {"tune": tune.as_dict(), "ms_median": med, "ms_min": min(ms),
+                "gpairs_per_s": pairs / (med * 1e-3) / 1e9, "rel_norm": rep["rel_norm"]}
+        results.append(line)
+        print(json.dumps(line), flush=True)
+    best = min(results, key=lambda r: r["ms_median"])
+    tune = ktt_b200.Tune(**best["tune"])
+
+    host_out = np.empty((ny, nx), dtype=np.float32)
+    pinned_in = torch.from_numpy(case.atoms).pin_memory()
+    pinned_out = torch.empty((ny, nx), dtype=torch.float32).pin_memory()
+    wall = []
+    for _ in range(args.repeat):
+        t0 = time.perf_counter()
+        d_atoms = pinned_in.to("cuda", non_blocking=True)
+        s = ctx.slice_atoms(d_atoms, case.z_slice)
+        ctx.forward_2d(s, h, nx, ny, tune=tune, out=out)
+        pinned_out.copy_(out, non_blocking=True)
+        ctx.synchronize()
+        torch.cuda.synchronize()
+        host_out[...] = pinned_out.numpy()
+        wall.append(time.perf_counter() - t0)
+    rep = errors.report(host_out, ref)
+    print(json.dumps({"best_tune": best["tune"], "kernel_ms_median": best["ms_median"],
+                      "kernel_gpairs_per_s": best["gpairs_per_s"],
+                      "host_call_ms_median": float(np.median(wall)) * 1e3,
+                      "host_call_gpairs_per_s": pairs / float(np.median(wall)) / 1e9,
+                      "host_call_rel_norm": rep["rel_norm"],
+                      "oracle_fp64_ms": oracle_s * 1e3, "oracle_threads": oracle.max_threads()}), flush=True)
+    ctx.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -81,28 +81,62 @@ def test_adjoint_config5_finite_differences_and_reference(ctx):
     assert _rel(grad[sel, :3], fd[:, :3]) <= TOL
 
 
+def _adam_fp64(a_mat, w, target, q0, lr, steps, b1=0.9, b2=0.999, eps=1e-8):
+    """Adam (the update torch.optim.Adam makes) on L(q) = 0.5 sum w (A q - T)^2 in FP64; the map is
+    linear in the charges, A[i, j] = 1 / |r_i - r_j|.  Returns the loss before each step."""
+    q = q0.astype(np.float64).copy()
+    m = np.zeros_like(q)
+    v = np.zeros_like(q)
+    losses = []
+    for s in range(1, steps + 1):
+        r = a_mat @ q - target
+        losses.append(0.5 * float((w * r * r).sum()))
+        g = a_mat.T @ (w * r)
+        m = b1 * m + (1 - b1) * g
+        v = b2 * v + (1 - b2) * g * g
+        q -= lr * (m / (1 - b1 ** s)) / (np.sqrt(v / (1 - b2 ** s)) + eps)
+    return np.array(losses), q
+
+
 def test_adam_charge_fitting(ctx):
-    """100 Adam steps on the charges through the autograd function: the loss falls by orders of
-    magnitude and the charges move toward the ones that made the target map."""
+    """100 Adam steps (lr 0.005) on the charges of 512 atoms through the autograd function.  The loss
+    falls below 15% of its start (the fit of charges to a smooth 1/r map is ill-posed, so the charges
+    themselves are only required not to drift away), and the loss trajectory follows the same Adam run
+    made in FP64 on the explicit 110,592 x 512 map matrix within 1% at every tenth step."""
     import torch
-    atoms, q_target, dims, h, excl = workloads.adjoint_problem(seed=6, n_atoms=4096, n=96, box=48.0)
-    weight = torch.from_numpy(workloads.exclusion_weights(atoms, dims, h, excl)).cuda()
+    steps, lr = 100, 0.005
+    atoms, q_target, dims, h, excl = workloads.adjoint_problem(seed=6, n_atoms=512, n=48, box=24.0)
+    w_np = workloads.exclusion_weights(atoms, dims, h, excl)
+    weight = torch.from_numpy(w_np).cuda().double()
     target_atoms = atoms.copy()
     target_atoms[:, 3] = q_target
     tune = ktt_b200.Tune(**FORWARD)
-    target = ctx.forward_3d(torch.from_numpy(target_atoms).cuda(), dims, h, tune=tune)
+    target = ctx.forward_3d(torch.from_numpy(target_atoms).cuda(), dims, h, tune=tune).double()
     xyz = torch.from_numpy(atoms[:, :3].copy()).cuda()
     q = torch.from_numpy(atoms[:, 3].copy()).cuda().requires_grad_(True)
-    opt = torch.optim.Adam([q], lr=0.02)
+    opt = torch.optim.Adam([q], lr=lr)
     losses = []
-    for _ in range(100):
+    for _ in range(steps):
         opt.zero_grad()
         v = ktt_b200.coulomb_map(torch.cat([xyz, q[:, None]], dim=1), ctx, dims, h, None, tune)
-        loss = 0.5 * (weight * (v - target) ** 2).sum()
+        loss = 0.5 * (weight * (v.double() - target) ** 2).sum()
         loss.backward()
         opt.step()
         losses.append(float(loss.item()))
+    losses = np.array(losses)
+
+    g = np.arange(dims[0], dtype=np.float64) * h
+    zz, yy, xx = np.meshgrid(g, g, g, indexing="ij")
+    pts = np.stack([xx.ravel(), yy.ravel(), zz.ravel()], 1)
+    a_mat = np.empty((pts.shape[0], atoms.shape[0]))
+    for j in range(atoms.shape[0]):
+        a_mat[:, j] = 1.0 / np.sqrt(((pts - atoms[j, :3].astype(np.float64)) ** 2).sum(1))
+    ref_losses, _ = _adam_fp64(a_mat, w_np.ravel().astype(np.float64),
+                               a_mat @ q_target.astype(np.float64), atoms[:, 3], lr, steps)
+
     q_err0 = np.abs(atoms[:, 3] - q_target).mean()
     q_err = np.abs(q.detach().cpu().numpy() - q_target).mean()
-    assert losses[-1] < 0.02 * losses[0], losses[::10]
-    assert q_err < 0.5 * q_err0, (q_err, q_err0)
+    assert losses[-1] < 0.15 * losses[0], losses[::10]
+    assert q_err <= q_err0, (q_err, q_err0)
+    rel = np.abs(losses[::10] - ref_losses[::10]) / ref_losses[::10]
+    assert rel.max() <= 1e-2, (losses[::10], ref_losses[::10])
