@@ -164,7 +164,7 @@ def _load_traffic() -> dict | None:
 def run_ours(args) -> None:
     import torch
     import ktt_b200
-    from ktt_b200 import errors, workloads
+    from ktt_b200 import errors, sharding, workloads
 
     world, rank, local = _dist()
     if world > 1:
@@ -178,15 +178,10 @@ def run_ours(args) -> None:
     dev = torch.device("cuda", torch.cuda.current_device())
 
     def barrier():
-        if world > 1:
-            torch.distributed.barrier()
+        sharding.barrier()
 
     def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
+        return sharding.max_over_ranks(x, device=dev)
 
     ctx = ktt_b200.CoulombContext(dev.index)
     w = workloads.uniform_map(seed=2 + rank)  # each rank: its own map (weak scaling)

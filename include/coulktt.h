@@ -161,6 +161,16 @@ COUL_API int coul_variant_get(int i, coul_tune* tune, int* is_2d, int* is_soa);
  */
 COUL_API int coul_forward_3d(coul_ctx* ctx, const float* d_atoms, int64_t n_atoms, const coul_grid* grid,
                              const coul_tune* tune, int accumulate, float* d_out);
+/*
+ * One z slab of the 3D map: the points z in [z_begin, z_end) of the full grid `grid`, written to
+ * d_out as (z_end - z_begin) x ny x nx values (x fastest).  The points' coordinates are those of
+ * the full grid, so the slabs of a z-sharded map (one per GPU) put together equal the single-GPU
+ * map bit for bit when every z_begin is a multiple of tune->z_iterations (otherwise a point may
+ * take its rsqrt from the other pipe and differ in the last bits).  No counterpart in the reference (KTT runs one map per kernel launch); it is
+ * the sharding unit of the multi-GPU path.
+ */
+COUL_API int coul_forward_3d_slab(coul_ctx* ctx, const float* d_atoms, int64_t n_atoms, const coul_grid* grid,
+                                  int z_begin, int z_end, const coul_tune* tune, int accumulate, float* d_out);
 /* Same with the atom coordinates and charges in four separate arrays. */
 COUL_API int coul_forward_3d_soa(coul_ctx* ctx, const float* d_x, const float* d_y, const float* d_z,
                                  const float* d_q, int64_t n_atoms, const coul_grid* grid, const coul_tune* tune,

@@ -116,6 +116,7 @@ def load_library():
         "coul_variant_count": [],
         "coul_variant_get": [ci, T, ctypes.POINTER(ci), ctypes.POINTER(ci)],
         "coul_forward_3d": [vp, vp, i64, G, T, ci, vp],
+        "coul_forward_3d_slab": [vp, vp, i64, G, ci, ci, T, ci, vp],
         "coul_forward_3d_soa": [vp, vp, vp, vp, vp, i64, G, T, ci, vp],
         "coul_forward_3d_reference": [vp, vp, i64, G, ci, vp],
         "coul_forward_2d": [vp, vp, i64, cf, ci, ci, T, ci, vp],
@@ -263,6 +264,21 @@ class CoulombContext:
         t = (tune or Tune()).c()
         _check(self._lib.coul_forward_3d(self._ctx, _ptr(atoms), atoms.shape[0], ctypes.byref(g), ctypes.byref(t),
                                          1 if accumulate else 0, _ptr(out)))
+        return out
+
+    def forward_3d_slab(self, atoms, dims, spacing, z_begin: int, z_end: int, origin=None,
+                        tune: Tune | None = None, out=None, accumulate: bool = False):
+        """Slab z in [z_begin, z_end) of the map of dims = (nx, ny, nz): shape (z_end - z_begin, ny, nx),
+        the full grid's point coordinates (slabs starting at multiples of tune.z_iterations put together
+        equal forward_3d bit for bit)."""
+        self._check_atoms(atoms)
+        nx, ny, nz = (int(d) for d in dims)
+        out = self._out(out, (int(z_end) - int(z_begin), ny, nx), atoms.device)
+        self._bind_stream()
+        g = _grid(dims, spacing, origin)
+        t = (tune or Tune()).c()
+        _check(self._lib.coul_forward_3d_slab(self._ctx, _ptr(atoms), atoms.shape[0], ctypes.byref(g), int(z_begin),
+                                              int(z_end), ctypes.byref(t), 1 if accumulate else 0, _ptr(out)))
         return out
 
     def forward_3d_soa(self, x, y, z, q, dims, spacing, origin=None, tune: Tune | None = None, out=None,

@@ -216,7 +216,7 @@ int launch_forward(coul_ctx* ctx, const VariantEntry* v, const FwdParams& prm, i
     int64_t gy, gz;
     if (mode == kModeGrid3d) {
         gy = (prm.ny + t->block_y - 1) / t->block_y;
-        gz = (prm.nz + t->z_iterations - 1) / t->z_iterations;
+        gz = (prm.nz - prm.z_base + t->z_iterations - 1) / t->z_iterations;
     } else {
         const int64_t by = static_cast<int64_t>(t->block_y) * t->z_iterations;
         gy = (prm.ny + by - 1) / by;
@@ -428,13 +428,17 @@ COUL_API int coul_variant_get(int i, coul_tune* t, int* is_2d, int* is_soa)
 
 static int forward_3d_common(coul_ctx* ctx, const float* d_atoms, const float* d_x, const float* d_y,
                              const float* d_z, const float* d_q, int soa, int64_t n_atoms, const coul_grid* grid,
-                             const coul_tune* tune, int accumulate, float* d_out)
+                             int z_begin, int z_end, const coul_tune* tune, int accumulate, float* d_out)
 {
     if (ctx == nullptr)
         return set_error(COUL_ERR_INVALID_ARGUMENT, "ctx is NULL");
     int rc = validate_grid(grid);
     if (rc)
         return rc;
+    if (z_end < 0)
+        z_end = grid->nz;
+    if (z_begin < 0 || z_begin >= z_end || z_end > grid->nz)
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "slab [z_begin, z_end) must be a non-empty range inside the grid");
     const VariantEntry* v = nullptr;
     if ((rc = validate_tune(tune, kModeGrid3d, soa, &v)))
         return rc;
@@ -460,7 +464,8 @@ static int forward_3d_common(coul_ctx* ctx, const float* d_atoms, const float* d
     p.n_atoms = n_atoms;
     p.nx = grid->nx;
     p.ny = grid->ny;
-    p.nz = grid->nz;
+    p.nz = z_end;
+    p.z_base = z_begin;
     p.h = grid->spacing;
     p.ox = grid->origin[0];
     p.oy = grid->origin[1];
@@ -477,8 +482,15 @@ static int forward_3d_common(coul_ctx* ctx, const float* d_atoms, const float* d
 COUL_API int coul_forward_3d(coul_ctx* ctx, const float* d_atoms, int64_t n_atoms, const coul_grid* grid,
                              const coul_tune* tune, int accumulate, float* d_out)
 {
-    return forward_3d_common(ctx, d_atoms, nullptr, nullptr, nullptr, nullptr, 0, n_atoms, grid, tune, accumulate,
-                             d_out);
+    return forward_3d_common(ctx, d_atoms, nullptr, nullptr, nullptr, nullptr, 0, n_atoms, grid, 0, -1, tune,
+                             accumulate, d_out);
+}
+
+COUL_API int coul_forward_3d_slab(coul_ctx* ctx, const float* d_atoms, int64_t n_atoms, const coul_grid* grid,
+                                  int z_begin, int z_end, const coul_tune* tune, int accumulate, float* d_out)
+{
+    return forward_3d_common(ctx, d_atoms, nullptr, nullptr, nullptr, nullptr, 0, n_atoms, grid, z_begin, z_end,
+                             tune, accumulate, d_out);
 }
 
 COUL_API int coul_forward_3d_soa(coul_ctx* ctx, const float* d_x, const float* d_y, const float* d_z,
@@ -487,7 +499,7 @@ COUL_API int coul_forward_3d_soa(coul_ctx* ctx, const float* d_x, const float* d
 {
     if (tune && tune->atom_source != COUL_ATOMS_SHARED_TMA)
         return set_error(COUL_ERR_UNSUPPORTED, "the four-array atom layout is staged through shared memory only");
-    return forward_3d_common(ctx, nullptr, d_x, d_y, d_z, d_q, 1, n_atoms, grid, tune, accumulate, d_out);
+    return forward_3d_common(ctx, nullptr, d_x, d_y, d_z, d_q, 1, n_atoms, grid, 0, -1, tune, accumulate, d_out);
 }
 
 COUL_API int coul_forward_3d_reference(coul_ctx* ctx, const float* d_atoms, int64_t n_atoms, const coul_grid* grid,

@@ -43,6 +43,8 @@ struct FwdParams {
     const float* sq;
     int64_t n_atoms;
     int nx, ny, nz;
+    int z_base;  // 3D: global z index of the output's first slice (0 for a whole map; slabs of a
+                 // sharded map start later); points z in [z_base, nz) are evaluated
     float h, ox, oy, oz;
     float* out;
     int accumulate;

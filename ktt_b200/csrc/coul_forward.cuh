@@ -326,8 +326,8 @@ __device__ __forceinline__ bool tile_pass(const FwdParams& p, const int x0, cons
         if constexpr (MODE == kModeGrid3d) {
             const int z = z0 + m;
             if (z < p.nz && yrow < p.ny)
-                store_points<XP>(p.out + (static_cast<int64_t>(z) * p.ny + yrow) * p.nx, x0, p.nx, v, p.accumulate,
-                                 vec_ok);
+                store_points<XP>(p.out + (static_cast<int64_t>(z - p.z_base) * p.ny + yrow) * p.nx, x0, p.nx, v,
+                                 p.accumulate, vec_ok);
         } else {
             const int yy = yrow + m;
             if (yy < p.ny)
@@ -348,7 +348,7 @@ __global__ void __launch_bounds__(kMaxThreads) fwd_kernel(const FwdParams p, con
     int yrow, z0;
     if constexpr (MODE == kModeGrid3d) {
         yrow = blockIdx.y * blockDim.y + threadIdx.y;
-        z0 = blockIdx.z * ZI;
+        z0 = p.z_base + static_cast<int>(blockIdx.z) * ZI;
     } else {
         yrow = (blockIdx.y * blockDim.y + threadIdx.y) * ZI;
         z0 = 0;
