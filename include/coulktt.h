@@ -100,6 +100,10 @@ typedef struct coul_tune {
     int precision;    /* COUL_PREC_* */
     int rsqrt_soft;   /* of every 8 reciprocal square roots, how many run as FMA-pipe
                          Newton iterations instead of on the MUFU unit (0 = all MUFU) */
+    int atom_split;   /* 0 or 1: one CTA per point tile; 2..8: a thread-block cluster of that many
+                         CTAs shares each point tile, each streaming 1/atom_split of the atoms, the
+                         partial sums reduced over distributed shared memory (for slices and small
+                         maps with too few tiles to fill the GPU; FP32, shared-memory atoms) */
 } coul_tune;
 
 typedef struct coul_grid {
@@ -148,6 +152,8 @@ COUL_API int coul_buffer_memset(coul_ctx* ctx, void* d_dst, int value, size_t by
 COUL_API void coul_tune_default(coul_tune* tune);
 /* COUL_OK if the configuration maps to a compiled kernel variant that fits the device. */
 COUL_API int coul_tune_supported(const coul_tune* tune);
+/* The same check for coul_forward_2d (2D-slice variants). */
+COUL_API int coul_tune_supported_2d(const coul_tune* tune);
 /* Number of compiled forward variants, and the i-th one (for the tuner's space checks): its
    tuning fields (block shape left at the default), whether it is a 2D-slice variant, and whether
    it reads the four-array atom layout. */

@@ -45,7 +45,7 @@ class CoulombError(RuntimeError):
 class _Tune(ctypes.Structure):
     _fields_ = [("block_x", ctypes.c_int), ("block_y", ctypes.c_int), ("z_iterations", ctypes.c_int),
                 ("x_points", ctypes.c_int), ("unroll", ctypes.c_int), ("atom_source", ctypes.c_int),
-                ("precision", ctypes.c_int), ("rsqrt_soft", ctypes.c_int)]
+                ("precision", ctypes.c_int), ("rsqrt_soft", ctypes.c_int), ("atom_split", ctypes.c_int)]
 
 
 class _Grid(ctypes.Structure):
@@ -59,7 +59,8 @@ class Tune:
 
     block_x [WORK_GROUP_SIZE_X], block_y [WORK_GROUP_SIZE_Y], z_iterations [Z_ITERATIONS],
     x_points [VECTOR_SIZE / OUTER_UNROLL_FACTOR], unroll [INNER_UNROLL_FACTOR],
-    atom_source [USE_CONSTANT_MEMORY], precision, rsqrt_soft.
+    atom_source [USE_CONSTANT_MEMORY], precision, rsqrt_soft, atom_split (CTAs per cluster sharing a
+    point tile in the atom-split form; 0 = off).
     """
     block_x: int = 32
     block_y: int = 4
@@ -69,6 +70,7 @@ class Tune:
     atom_source: int = ATOMS_SHARED_TMA
     precision: int = PREC_FP32
     rsqrt_soft: int = 0
+    atom_split: int = 0
 
     def c(self) -> _Tune:
         return _Tune(*(int(getattr(self, f.name)) for f in fields(self)))
@@ -113,6 +115,7 @@ def load_library():
         "coul_synchronize": [vp],
         "coul_elapsed_ms": [vp, ctypes.POINTER(ctypes.c_double)],
         "coul_tune_supported": [T],
+        "coul_tune_supported_2d": [T],
         "coul_variant_count": [],
         "coul_variant_get": [ci, T, ctypes.POINTER(ci), ctypes.POINTER(ci)],
         "coul_forward_3d": [vp, vp, i64, G, T, ci, vp],
@@ -172,6 +175,12 @@ def variants() -> list[tuple[Tune, bool, bool]]:
 def tune_supported(tune: Tune) -> bool:
     lib = load_library()
     return lib.coul_tune_supported(ctypes.byref(tune.c())) == COUL_OK
+
+
+def tune_supported_2d(tune: Tune) -> bool:
+    """Whether coul_forward_2d has a compiled variant for this configuration."""
+    lib = load_library()
+    return lib.coul_tune_supported_2d(ctypes.byref(tune.c())) == COUL_OK
 
 
 def _grid(dims, spacing, origin) -> _Grid:

@@ -39,6 +39,7 @@ std::vector<VariantEntry>& registry()
         register_fwd_3d_soft(v);
         register_fwd_3d_soft_precise(v);
         register_fwd_2d(v);
+        register_fwd_split(v);
     });
     return v;
 }
@@ -174,16 +175,23 @@ int validate_tune(const coul_tune* t, int mode, int soa, const VariantEntry** ou
         return set_error(COUL_ERR_INVALID_ARGUMENT, "unknown precision");
     if (t->rsqrt_soft < 0 || t->rsqrt_soft > 8)
         return set_error(COUL_ERR_INVALID_ARGUMENT, "rsqrt_soft must be in 0..8");
+    if (t->atom_split < 0 || t->atom_split > kMaxSplit)
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "atom_split must be in 0.." + std::to_string(kMaxSplit));
+    const int split = t->atom_split >= 2 ? 1 : 0;
+    if (split && (t->atom_source != COUL_ATOMS_SHARED_TMA || soa || t->precision != COUL_PREC_FP32))
+        return set_error(COUL_ERR_UNSUPPORTED,
+                         "the atom-split form streams float4 atoms through shared memory with FP32 accumulation");
     const int unroll = t->unroll <= 1 ? 1 : t->unroll;
-    const VariantKey key{t->z_iterations, t->x_points, unroll, t->atom_source, soa, t->precision, t->rsqrt_soft, mode};
+    const VariantKey key{t->z_iterations, t->x_points, unroll, t->atom_source, soa, t->precision, t->rsqrt_soft, mode,
+                         split};
     const VariantEntry* e = find_variant(key);
     if (e == nullptr) {
         char buf[256];
         std::snprintf(buf, sizeof buf,
                       "no compiled variant for z_iterations=%d x_points=%d unroll=%d atom_source=%d soa=%d "
-                      "precision=%d rsqrt_soft=%d mode=%s",
+                      "precision=%d rsqrt_soft=%d atom_split=%d mode=%s",
                       t->z_iterations, t->x_points, unroll, t->atom_source, soa, t->precision, t->rsqrt_soft,
-                      mode == kModeGrid3d ? "3d" : "2d");
+                      t->atom_split, mode == kModeGrid3d ? "3d" : "2d");
         return set_error(COUL_ERR_UNSUPPORTED, buf);
     }
     if (out)
@@ -226,6 +234,12 @@ int launch_forward(coul_ctx* ctx, const VariantEntry* v, const FwdParams& prm, i
         return set_error(COUL_ERR_DEVICE_LIMITS, "grid too large for one launch");
     L.grid = dim3(static_cast<unsigned>(gx), static_cast<unsigned>(gy), static_cast<unsigned>(gz));
     L.smem = (t->atom_source == COUL_ATOMS_SHARED_TMA) ? (kStages * kTileAtoms * 16 + kStages * 8) : 0;
+    if (v->key.split) {
+        L.split = t->atom_split;
+        L.smem = split_smem_bytes(t->block_x * t->block_y, t->z_iterations * t->x_points);
+        if (static_cast<int64_t>(L.grid.x) * L.split > 2147483647LL)
+            return set_error(COUL_ERR_DEVICE_LIMITS, "grid too large for one launch");
+    }
     const int xp = t->x_points;
     L.vec_store = (xp > 1 && prm.nx % xp == 0 &&
                    (reinterpret_cast<uintptr_t>(prm.out) % (sizeof(float) * (xp >= 4 ? 4 : xp))) == 0)
@@ -401,9 +415,12 @@ COUL_API void coul_tune_default(coul_tune* t)
     t->atom_source = COUL_ATOMS_SHARED_TMA;
     t->precision = COUL_PREC_FP32;
     t->rsqrt_soft = 0;
+    t->atom_split = 0;
 }
 
 COUL_API int coul_tune_supported(const coul_tune* t) { return validate_tune(t, kModeGrid3d, 0, nullptr); }
+
+COUL_API int coul_tune_supported_2d(const coul_tune* t) { return validate_tune(t, kModeSlice2d, 0, nullptr); }
 
 COUL_API int coul_variant_count(void) { return static_cast<int>(registry().size()); }
 
@@ -419,6 +436,7 @@ COUL_API int coul_variant_get(int i, coul_tune* t, int* is_2d, int* is_soa)
     t->atom_source = k.src;
     t->precision = k.prec;
     t->rsqrt_soft = k.soft;
+    t->atom_split = k.split ? 2 : 0;
     if (is_2d)
         *is_2d = k.mode == kModeSlice2d ? 1 : 0;
     if (is_soa)

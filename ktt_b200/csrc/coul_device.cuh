@@ -135,6 +135,43 @@ __device__ __forceinline__ void report_status(int* status, int code)
         atomicCAS(status, kStatusOk, code);
 }
 
+// Thread-block clusters: this CTA's rank and the cluster's size, the cluster-wide barrier (a
+// hardware barrier: every thread of every CTA of the cluster arrives, release/acquire ordering of
+// shared-memory writes), and loads from a peer CTA's shared memory (distributed shared memory).
+__device__ __forceinline__ uint32_t cluster_rank()
+{
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+
+__device__ __forceinline__ uint32_t cluster_size()
+{
+    uint32_t n;
+    asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(n));
+    return n;
+}
+
+__device__ __forceinline__ void cluster_sync()
+{
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+// Address of `p` (this CTA's shared memory) in the shared-memory window of cluster CTA `rank`.
+__device__ __forceinline__ uint32_t cluster_map(const void* p, uint32_t rank)
+{
+    uint32_t a;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(a) : "r"(smem_u32(p)), "r"(rank));
+    return a;
+}
+
+__device__ __forceinline__ float ld_cluster_f32(uint32_t addr)
+{
+    float v;
+    asm volatile("ld.shared::cluster.f32 %0, [%1];" : "=f"(v) : "r"(addr) : "memory");
+    return v;
+}
+
 // MUFU reciprocal square root (approximate, flush-to-zero), the instruction KTT's kernels reach
 // through rsqrt()/half_rsqrt() under fast-math.
 __device__ __forceinline__ float rsqrt_mufu(float x)

@@ -29,10 +29,11 @@ static __constant__ float4 c_atoms[kConstAtoms];
 
 struct FwdLaunch {
     FwdParams p;
-    dim3 grid;
+    dim3 grid;  // one entry per point tile (the atom-split form multiplies grid.x by `split`)
     dim3 block;
     size_t smem;
     int vec_store;  // 1 if x-vector stores are aligned for this launch
+    int split;      // atom-split form: CTAs per cluster sharing one point tile (0 / 1 = one CTA per tile)
 };
 
 template <int MODE, int XP, int ZH, int SOFT>
@@ -104,14 +105,15 @@ __device__ __forceinline__ void ring_init(uint64_t* full, const int tid)
 }
 
 // One thread's work for one tile: accumulate the potential of its register block of points
-// (x0.., yrow, z0.. in 3D; x0.., rows yrow.. in 2D) over all atoms of p, then store it.  With
+// (x0.., yrow, z0.. in 3D; x0.., rows yrow.. in 2D) over all atoms of p into val[x][z].  With
 // SRC == kSrcShared the atoms come through the CTA's TMA ring (tiles / full); gstage counts the
 // ring's stages across calls, so a persistent kernel can run many tiles through one ring.  Every
-// thread of the CTA must call this together (it synchronises per stage).  Returns false when a
-// bounded wait on the ring expired (the status word is set; nothing was stored).
+// thread of the CTA must call this together (it synchronises per stage).  Returns false (on every
+// thread) when a bounded wait on the ring expired; the status word is then set and val is invalid.
 template <int ZI, int XP, int UNR, int SRC, int SOA, int PREC, int SOFT, int MODE>
-__device__ __forceinline__ bool tile_pass(const FwdParams& p, const int x0, const int yrow, const int z0, const int vec_ok,
-                                          unsigned char* tiles, uint64_t* full, uint32_t& gstage)
+__device__ __forceinline__ bool tile_accumulate(const FwdParams& p, const int x0, const int yrow, const int z0,
+                                                unsigned char* tiles, uint64_t* full, uint32_t& gstage,
+                                                float (&val)[XP][ZI])
 {
     static_assert(XP == 1 || XP == 2 || XP == 4 || XP == 8, "XP must be 1, 2, 4 or 8");
     static_assert(kTileAtoms % kSubTile == 0, "sub-tiles must divide the stage");
@@ -304,7 +306,6 @@ __device__ __forceinline__ bool tile_pass(const FwdParams& p, const int x0, cons
         gstage += static_cast<uint32_t>(nst);
     }
 
-    float val[XP][ZI];
 #pragma unroll
     for (int k = 0; k < XP; ++k)
 #pragma unroll
@@ -316,7 +317,17 @@ __device__ __forceinline__ bool tile_pass(const FwdParams& p, const int x0, cons
             else
                 val[k][m] = static_cast<float>(acc64[k][m]);
         }
+    (void)part;
+    (void)cmp;
+    (void)acc64;
+    return true;
+}
 
+// Store one thread's register block (edge-guarded; vectorised along x when vec_ok).
+template <int ZI, int XP, int MODE>
+__device__ __forceinline__ void store_tile(const FwdParams& p, const int x0, const int yrow, const int z0,
+                                           const int vec_ok, const float (&val)[XP][ZI])
+{
 #pragma unroll
     for (int m = 0; m < ZI; ++m) {
         float v[XP];
@@ -334,9 +345,17 @@ __device__ __forceinline__ bool tile_pass(const FwdParams& p, const int x0, cons
                 store_points<XP>(p.out + static_cast<int64_t>(yy) * p.nx, x0, p.nx, v, p.accumulate, vec_ok);
         }
     }
-    (void)part;
-    (void)cmp;
-    (void)acc64;
+}
+
+// tile_accumulate then store_tile.  Returns false when a bounded wait expired (nothing stored).
+template <int ZI, int XP, int UNR, int SRC, int SOA, int PREC, int SOFT, int MODE>
+__device__ __forceinline__ bool tile_pass(const FwdParams& p, const int x0, const int yrow, const int z0, const int vec_ok,
+                                          unsigned char* tiles, uint64_t* full, uint32_t& gstage)
+{
+    float val[XP][ZI];
+    if (!tile_accumulate<ZI, XP, UNR, SRC, SOA, PREC, SOFT, MODE>(p, x0, yrow, z0, tiles, full, gstage, val))
+        return false;
+    store_tile<ZI, XP, MODE>(p, x0, yrow, z0, vec_ok, val);
     return true;
 }
 
@@ -364,17 +383,86 @@ __global__ void __launch_bounds__(kMaxThreads) fwd_kernel(const FwdParams p, con
     }
 }
 
+// Atom-split form for maps with too few points to fill the GPU one tile per CTA (a 2D slice, a
+// small 3D map): a thread-block cluster of S CTAs shares one point tile, CTA rank r takes the r-th
+// of S contiguous atom ranges through its own TMA ring, and rank 0 sums the S partial blocks from
+// the peers' shared memory in rank order (deterministic) and stores them.  The cluster size is a
+// launch-time choice (2..8, the portable cluster limit); plain FP32 accumulation, AoS atoms.
+template <int ZI, int XP, int UNR, int SOFT, int MODE>
+__global__ void __launch_bounds__(kMaxThreads) split_kernel(const FwdParams p, const int vec_ok)
+{
+    const uint32_t S = cluster_size();
+    const uint32_t r = cluster_rank();
+    const int tile_x = static_cast<int>(blockIdx.x / S);
+    const int x0 = (tile_x * static_cast<int>(blockDim.x) + static_cast<int>(threadIdx.x)) * XP;
+    int yrow, z0;
+    if constexpr (MODE == kModeGrid3d) {
+        yrow = blockIdx.y * blockDim.y + threadIdx.y;
+        z0 = p.z_base + static_cast<int>(blockIdx.z) * ZI;
+    } else {
+        yrow = (blockIdx.y * blockDim.y + threadIdx.y) * ZI;
+        z0 = 0;
+    }
+    const int nthreads = blockDim.x * blockDim.y;
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+
+    FwdParams q = p;
+    const int64_t chunk = (p.n_atoms + S - 1) / S;
+    const int64_t begin = chunk * r < p.n_atoms ? chunk * r : p.n_atoms;
+    q.atoms = p.atoms + begin;
+    q.n_atoms = (p.n_atoms - begin) < chunk ? (p.n_atoms - begin) : chunk;
+
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + kStages * kTileAtoms * 16);
+    float* red = reinterpret_cast<float*>(smem_raw + kStages * kTileAtoms * 16 + kStages * 8);
+    ring_init(full, tid);
+    uint32_t gstage = 0;
+    float val[XP][ZI];
+    (void)tile_accumulate<ZI, XP, UNR, kSrcShared, 0, kPrecFp32, SOFT, MODE>(q, x0, yrow, z0, smem_raw, full, gstage,
+                                                                            val);
+    // A CTA whose ring wait expired has set the status word; the cluster still meets at both
+    // barriers so no CTA waits on one that left.
+#pragma unroll
+    for (int k = 0; k < XP; ++k)
+#pragma unroll
+        for (int m = 0; m < ZI; ++m)
+            red[(k * ZI + m) * nthreads + tid] = val[k][m];
+    cluster_sync();
+    if (r == 0) {
+        for (uint32_t peer = 1; peer < S; ++peer) {
+            const uint32_t base = cluster_map(red, peer);
+#pragma unroll
+            for (int k = 0; k < XP; ++k)
+#pragma unroll
+                for (int m = 0; m < ZI; ++m)
+                    val[k][m] += ld_cluster_f32(base + 4u * static_cast<uint32_t>((k * ZI + m) * nthreads + tid));
+        }
+        store_tile<ZI, XP, MODE>(p, x0, yrow, z0, vec_ok, val);
+    }
+    cluster_sync();  // the peers' shared memory stays valid until rank 0 has read it
+}
+
 // ------------------------------------------------------------------------------------------
 // Launchers and the variant registry
 // ------------------------------------------------------------------------------------------
 struct VariantKey {
     int zi, xp, unroll, src, soa, prec, soft, mode;
+    int split;  // 1 for the atom-split (cluster) form
     bool operator==(const VariantKey& o) const
     {
         return zi == o.zi && xp == o.xp && unroll == o.unroll && src == o.src && soa == o.soa && prec == o.prec &&
-               soft == o.soft && mode == o.mode;
+               soft == o.soft && mode == o.mode && split == o.split;
     }
 };
+
+constexpr int kMaxSplit = 8;  // portable thread-block cluster size
+
+// Dynamic shared memory of the atom-split form: the TMA ring, its barriers, the partial block.
+inline size_t split_smem_bytes(int threads, int values_per_thread)
+{
+    return static_cast<size_t>(kStages) * kTileAtoms * 16 + kStages * 8 +
+           static_cast<size_t>(threads) * values_per_thread * sizeof(float);
+}
 
 using FwdLaunchFn = cudaError_t (*)(const FwdLaunch&, cudaStream_t);
 
@@ -420,8 +508,44 @@ cudaError_t launch_fwd(const FwdLaunch& L, cudaStream_t stream)
 template <int ZI, int XP, int UNR, int SRC, int SOA, int PREC, int SOFT, int MODE>
 void add_variant(std::vector<VariantEntry>& v)
 {
-    v.push_back(VariantEntry{VariantKey{ZI, XP, UNR, SRC, SOA, PREC, SOFT, MODE},
+    v.push_back(VariantEntry{VariantKey{ZI, XP, UNR, SRC, SOA, PREC, SOFT, MODE, 0},
                              &launch_fwd<ZI, XP, UNR, SRC, SOA, PREC, SOFT, MODE>, 0});
+}
+
+// Cluster launch of the atom-split form: grid.x tiles x `split` CTAs, clusters of `split` along x.
+template <int ZI, int XP, int UNR, int SOFT, int MODE>
+cudaError_t launch_split(const FwdLaunch& L, cudaStream_t stream)
+{
+    auto kernel = split_kernel<ZI, XP, UNR, SOFT, MODE>;
+    const unsigned S = static_cast<unsigned>(L.split);
+    if (S < 2 || S > static_cast<unsigned>(kMaxSplit))
+        return cudaErrorInvalidValue;
+    if (L.smem > 48u * 1024u) {
+        cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             static_cast<int>(L.smem));
+        if (e != cudaSuccess)
+            return e;
+    }
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(L.grid.x * S, L.grid.y, L.grid.z);
+    cfg.blockDim = L.block;
+    cfg.dynamicSmemBytes = L.smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = S;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, L.p, L.vec_store);
+}
+
+template <int ZI, int XP, int UNR, int SOFT, int MODE>
+void add_split_variant(std::vector<VariantEntry>& v)
+{
+    v.push_back(VariantEntry{VariantKey{ZI, XP, UNR, kSrcShared, 0, kPrecFp32, SOFT, MODE, 1},
+                             &launch_split<ZI, XP, UNR, SOFT, MODE>, 0});
 }
 
 // Register the four atom-loop unrolls {1, 2, 4, 8} of one variant family.
@@ -443,5 +567,6 @@ void register_fwd_3d_precise(std::vector<VariantEntry>& v);
 void register_fwd_3d_soft(std::vector<VariantEntry>& v);
 void register_fwd_3d_soft_precise(std::vector<VariantEntry>& v);
 void register_fwd_2d(std::vector<VariantEntry>& v);
+void register_fwd_split(std::vector<VariantEntry>& v);
 
 }  // namespace coul

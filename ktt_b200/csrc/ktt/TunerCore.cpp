@@ -817,6 +817,7 @@ Nanoseconds TunerCore::LaunchDefinition(const KernelData& kernel, const KernelDe
     tune.atom_source = static_cast<int>(parameter("USE_CONSTANT_MEMORY", 0));
     tune.precision = static_cast<int>(parameter("PRECISION", 0));
     tune.rsqrt_soft = static_cast<int>(parameter("RSQRT_SOFT", 0));
+    tune.atom_split = static_cast<int>(parameter("ATOM_SPLIT", 0));
 
     const bool threeD = definition.globalSize.GetSizeZ() > 1;
     int rc = COUL_OK;

@@ -2,11 +2,13 @@
 
     python -m ktt_b200.run_slice2d [--repeat 50]
 
-Atoms x, y ~ U[0, 128), z ~ U[0, 32), q ~ U[-1, 1]; the slice at z = 16 A.  For each 2D tile shape:
-device time of the slice kernel (median of --repeat event-timed launches), pair rate, error against
-the FP64 oracle over the whole slice.  Then the whole call as a KTT user makes it (host atoms in,
-dz^2 slicing on the device, host slice out; wall clock, median) for the fastest shape, and the FP64
-oracle's own time on the host.  One JSON line per measurement.
+Atoms x, y ~ U[0, 128), z ~ U[0, 32), q ~ U[-1, 1]; the slice at z = 16 A.  For each compiled 2D
+tile shape: device time of the slice kernel (median of --repeat event-timed launches), pair rate,
+error against the FP64 oracle over the whole slice.  Shapes include the atom-split form (a cluster
+of 2, 4 or 8 CTAs per point tile, each streaming a share of the atoms) and 2/8 of the rsqrts on the
+FMA pipe.  Then the whole call as a KTT user makes it (host atoms in, dz^2 slicing on the device,
+host slice out; wall clock, median) for the fastest shape, and the FP64 oracle's own time on the
+host.  One JSON line per measurement.
 """
 from __future__ import annotations
 
@@ -16,8 +18,8 @@ import time
 
 import numpy as np
 
-SHAPES = [(bx, by, xp, yi) for (bx, by) in ((32, 4), (32, 2), (64, 2), (16, 8), (32, 8))
-          for xp in (1, 2, 4) for yi in (1, 2, 4)]
+SHAPES = [(bx, by, xp, yi, split, soft) for (bx, by) in ((32, 4), (32, 2), (64, 2), (16, 8), (32, 8))
+          for xp in (1, 2, 4) for yi in (1, 2, 4) for split in (0, 2, 4, 8) for soft in (0, 2)]
 
 
 def main() -> None:
@@ -43,11 +45,10 @@ def main() -> None:
     d_sliced = ctx.slice_atoms(atoms, case.z_slice)
     out = torch.empty((ny, nx), dtype=torch.float32, device="cuda")
     results = []
-    for bx, by, xp, yi in SHAPES:
-        tune = ktt_b200.Tune(block_x=bx, block_y=by, x_points=xp, z_iterations=yi)
-        try:
-            ctx.forward_2d(d_sliced, h, nx, ny, tune=tune, out=out)
-        except ktt_b200.CoulombError:
+    for bx, by, xp, yi, split, soft in SHAPES:
+        tune = ktt_b200.Tune(block_x=bx, block_y=by, x_points=xp, z_iterations=yi, atom_split=split,
+                             rsqrt_soft=soft)
+        if not ktt_b200.tune_supported_2d(tune):
             continue
         ms = []
         for _ in range(args.repeat):

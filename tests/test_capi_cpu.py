@@ -49,14 +49,31 @@ def test_tune_validation_without_device():
     t = T(block_x=0).c()
     assert lib.coul_tune_supported(ctypes.byref(t)) == ktt_b200.COUL_ERR_DEVICE_LIMITS
     assert b"block" in lib.coul_last_error()
+    # atom-split form: cluster sizes 2..8, FP32 shared-memory atoms only
+    split = dict(z_iterations=8, x_points=2, rsqrt_soft=2)
+    for s in (2, 3, 5, 8):
+        assert ktt_b200.tune_supported(T(atom_split=s, **split))
+    assert ktt_b200.tune_supported(T(atom_split=1, z_iterations=16, x_points=4))  # 1 = off
+    assert not ktt_b200.tune_supported(T(atom_split=9, **split))
+    assert not ktt_b200.tune_supported(T(atom_split=-1, **split))
+    assert not ktt_b200.tune_supported(T(atom_split=4, precision=ktt_b200.PREC_FP64_MERGE, **split))
+    assert not ktt_b200.tune_supported(T(atom_split=4, z_iterations=4, x_points=1,
+                                         atom_source=ktt_b200.ATOMS_CONSTANT))
+    assert ktt_b200.tune_supported_2d(T(z_iterations=2, x_points=1, atom_split=4))
+    assert ktt_b200.tune_supported_2d(T(z_iterations=4, x_points=4))
+    assert not ktt_b200.tune_supported_2d(T(z_iterations=8, x_points=2, atom_split=4))
 
 
 def test_variant_inventory():
     vs = ktt_b200.variants()
     assert len(vs) == ktt_b200.load_library().coul_variant_count()
     keys = {(t.z_iterations, t.x_points, t.unroll, t.atom_source, t.precision, t.rsqrt_soft, d2, soa)
-            for t, d2, soa in vs}
-    assert len(keys) == len(vs)  # no duplicates
+            for t, d2, soa in vs if t.atom_split == 0}
+    split_keys = {(t.z_iterations, t.x_points, t.unroll, t.rsqrt_soft, d2) for t, d2, soa in vs if t.atom_split}
+    assert len(keys) + len(split_keys) == len(vs)  # no duplicates
+    # the atom-split (cluster) form: FP32, float4 atoms through shared memory, 2D and 3D
+    assert all(t.precision == 0 and t.atom_source == 0 and not soa for t, _, soa in vs if t.atom_split)
+    assert any(d2 for _, _, _, _, d2 in split_keys) and any(not d2 for _, _, _, _, d2 in split_keys)
     # the KTT CUDA space of CoulombSum3d.cpp: Z_ITERATIONS x unroll x USE_SOA, all present for x_points 1
     for zi in (1, 2, 4, 8, 16, 32):
         for un in (1, 2, 4, 8):

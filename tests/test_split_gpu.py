@@ -1,0 +1,85 @@
+"""The atom-split (thread-block cluster) form of the forward kernel against the FP64 oracle and
+against the one-CTA-per-tile form: 3D maps and 2D slices, cluster sizes 2..8, ragged atom counts
+(fewer atoms than CTAs in a cluster included), accumulate semantics, run-to-run determinism."""
+import numpy as np
+import pytest
+
+import ktt_b200
+import oracle
+from ktt_b200 import errors, workloads
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+
+
+def _atoms(n, seed, box=20.0):
+    rng = np.random.default_rng(seed)
+    a = np.zeros((max(n, 0), 4), dtype=np.float32)
+    a[:, :3] = rng.uniform(0.0, box, (n, 3))
+    a[:, 3] = rng.uniform(-1.0, 1.0, n)
+    return a
+
+
+@pytest.mark.parametrize("n_atoms", [0, 1, 3, 7, 255, 257, 4000, 8195])
+@pytest.mark.parametrize("split", [2, 3, 4, 8])
+def test_split_3d_matches_oracle(ctx, n_atoms, split):
+    import torch
+    a = _atoms(n_atoms, seed=n_atoms + 31)
+    dims, h, origin = (37, 29, 19), 0.5, (-1.0, 0.5, 2.0)
+    tune = ktt_b200.Tune(block_x=32, block_y=4, z_iterations=8, x_points=2, rsqrt_soft=2, atom_split=split)
+    atoms = torch.from_numpy(a).cuda() if n_atoms else torch.zeros((0, 4), device="cuda")
+    out = torch.full((dims[2], dims[1], dims[0]), float("nan"), device="cuda")
+    ctx.forward_3d(atoms, dims, h, origin, tune=tune, out=out)
+    got = out.cpu().numpy()
+    if n_atoms == 0:
+        assert np.all(got == 0.0)
+        return
+    ref = oracle.grid3d(a, h, dims, origin)
+    assert errors.report(got, ref)["rel_norm"] <= TOL
+    plain = ctx.forward_3d(atoms, dims, h, origin, tune=ktt_b200.Tune(block_x=32, block_y=4, z_iterations=8,
+                                                                      x_points=2, rsqrt_soft=2))
+    assert float((out - plain).abs().max()) <= 2e-6 * max(float(plain.abs().max()), 1e-30)
+
+
+@pytest.mark.parametrize("shape", [(1, 1, 1), (2, 1, 1), (4, 1, 2), (2, 2, 2), (1, 2, 4)])
+@pytest.mark.parametrize("split", [2, 4, 8])
+def test_split_2d_slice_matches_oracle(ctx, shape, split):
+    import torch
+    zi, xp, un = shape
+    case = workloads.slice_2d(n_atoms=4000, n=256)
+    ref = oracle.slice2d(case.ktt_atoms(), case.spacing, case.nx, case.ny)
+    sliced = ctx.slice_atoms(torch.from_numpy(case.atoms).cuda(), case.z_slice)
+    tune = ktt_b200.Tune(block_x=32, block_y=4, z_iterations=zi, x_points=xp, unroll=un, atom_split=split)
+    got = ctx.forward_2d(sliced, case.spacing, case.nx, case.ny, tune=tune)
+    assert errors.report(got.cpu().numpy(), ref)["rel_norm"] <= TOL
+    again = ctx.forward_2d(sliced, case.spacing, case.nx, case.ny, tune=tune)
+    assert torch.equal(got, again)
+
+
+def test_split_2d_ragged_slice_and_accumulate(ctx):
+    import torch
+    a = _atoms(1234, seed=8)
+    nx, ny, h, zs = 101, 75, 0.5, 7.0
+    kat = a.copy()
+    kat[:, 2] = (np.float32(zs) - a[:, 2]) ** 2
+    ref = oracle.slice2d(kat, h, nx, ny)
+    sliced = ctx.slice_atoms(torch.from_numpy(a).cuda(), zs)
+    tune = ktt_b200.Tune(block_x=16, block_y=8, z_iterations=2, x_points=2, atom_split=3)
+    v = ctx.forward_2d(sliced, h, nx, ny, tune=tune)
+    assert errors.report(v.cpu().numpy(), ref)["rel_norm"] <= TOL
+    base = torch.linspace(-2, 2, nx * ny, device="cuda").reshape(ny, nx)
+    acc = base.clone()
+    ctx.forward_2d(sliced, h, nx, ny, tune=tune, out=acc, accumulate=True)
+    assert torch.equal(acc, base + v)
+
+
+def test_split_slab_equals_split_map(ctx):
+    import torch
+    a = _atoms(900, seed=12)
+    dims, h = (40, 33, 48), 0.5
+    tune = ktt_b200.Tune(block_x=32, block_y=4, z_iterations=8, x_points=1, rsqrt_soft=2, atom_split=4)
+    atoms = torch.from_numpy(a).cuda()
+    full = ctx.forward_3d(atoms, dims, h, tune=tune)
+    slab = ctx.forward_3d_slab(atoms, dims, h, 16, 40, tune=tune)
+    assert torch.equal(slab, full[16:40])
