@@ -1,0 +1,135 @@
+"""KTT's own CUDA kernels, compiled the way KTT compiles them, run on the same inputs as this
+library's kernels: the known-answer map against the golden output (KTT's 0.01 criterion) and
+against this library's map; a seeded uniform map over every configuration of KTT's CUDA space
+against this library's map and the FP64 oracle.
+
+With KTT_REF_SWEEP_OUT=<path> the last test also times KTT's whole 210-configuration space on the
+256^3 x 65,536-atom map and writes the device times to <path> (JSON)."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import ktt_b200
+import oracle
+import ref_kernels
+from ktt_b200 import errors, workloads
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not ref_kernels.available(),
+                                 reason="KTT's kernels are not built (make -C oracle refkernels)")]
+
+
+def _cols(a):
+    import torch
+    return [torch.from_numpy(np.ascontiguousarray(a[:, k])).cuda() for k in range(4)]
+
+
+@pytest.fixture(scope="module")
+def kat(golden_dir):
+    with open(os.path.join(golden_dir, "coulomb3d_kat.json")) as f:
+        return json.load(f)
+
+
+@pytest.mark.parametrize("cfg", [
+    {"WORK_GROUP_SIZE_X": 32, "WORK_GROUP_SIZE_Y": 2, "Z_ITERATIONS": 16, "INNER_UNROLL_FACTOR": 0, "USE_SOA": 0},
+    {"WORK_GROUP_SIZE_X": 16, "WORK_GROUP_SIZE_Y": 4, "Z_ITERATIONS": 32, "INNER_UNROLL_FACTOR": 8, "USE_SOA": 1},
+])
+def test_ktt_kernel_on_the_known_answer_map(ctx, kat, cfg):
+    import torch
+    cells, h = kat["cells"], kat["grid_spacing_f32"]
+    atoms = oracle.kat_atoms(64)
+    ta = torch.from_numpy(atoms).cuda()
+    ref_out = torch.zeros(cells ** 3, device="cuda")
+    ref_kernels.run_tuned(cfg, ta, _cols(atoms), 64, h, cells, ref_out)
+    ours = ctx.forward_3d(ta, (cells, cells, cells), h).reshape(-1)
+    torch.cuda.synchronize()
+    v = ref_out.cpu().numpy()
+    idx = np.asarray(kat["index"], dtype=np.int64)
+    golden = np.asarray(kat["bits"], dtype=np.uint32).view(np.float32)
+    assert np.max(np.abs(v[idx] - golden)) <= kat["validation_threshold"]
+    assert float((ref_out - ours).abs().max()) <= 1e-5 * float(ref_out.abs().max())
+
+
+def test_ktt_space_matches_this_library_and_fp64(ctx):
+    """All 42 compiled forms of KTT's space (two launch shapes each) on a 256^3 map of 2,048 seeded
+    atoms, and KTT's reference kernel, against this library's map (1e-5 normwise) and the FP64 oracle
+    on a seeded subset (1e-5)."""
+    import torch
+    w = workloads.uniform_map(n_atoms=2048)
+    g = w.dims[0]
+    ta = torch.from_numpy(w.atoms).cuda()
+    cols = _cols(w.atoms)
+    ours = ctx.forward_3d(ta, w.dims, w.spacing, tune=ktt_b200.Tune(z_iterations=8, x_points=2)).reshape(-1)
+    idx = workloads.subset_indices(g ** 3, 2e-4, seed=3)
+    ref64 = oracle.points3d(w.atoms, w.spacing, w.dims, idx)
+    scale = float(ours.abs().max())
+    seen = set()
+    failures = []
+    for cfg in ref_kernels.space():
+        key = (cfg["Z_ITERATIONS"], cfg["INNER_UNROLL_FACTOR"], cfg["USE_SOA"])
+        shape = (cfg["WORK_GROUP_SIZE_X"], cfg["WORK_GROUP_SIZE_Y"])
+        if (key, shape) in seen or shape not in ((32, 2), (16, 8)):
+            continue
+        seen.add((key, shape))
+        out = torch.zeros(g ** 3, device="cuda")
+        ref_kernels.run_tuned(cfg, ta, cols, w.atoms.shape[0], w.spacing, g, out)
+        torch.cuda.synchronize()
+        d = float((out - ours).abs().max()) / scale
+        e = errors.report(out.cpu().numpy()[idx], ref64)["rel_norm"]
+        if d > 1e-5 or e > 1e-5:
+            failures.append((cfg, d, e))
+    assert len(seen) == 84
+    out = torch.zeros(g ** 3, device="cuda")
+    ref_kernels.run_reference(ta, w.atoms.shape[0], w.spacing, g, out)
+    torch.cuda.synchronize()
+    assert float((out - ours).abs().max()) / scale <= 1e-5
+    assert not failures, failures[:5]
+
+
+@pytest.mark.skipif(not os.environ.get("KTT_REF_SWEEP_OUT"), reason="timing sweep is opt-in")
+def test_time_ktt_space_on_the_full_map(ctx):
+    """Device time of every configuration of KTT's CUDA space on the 256^3 x 65,536 map (one
+    warm-up, best of two timed launches each), and of this library's chosen configuration."""
+    import torch
+    w = workloads.uniform_map()
+    g = w.dims[0]
+    ta = torch.from_numpy(w.atoms).cuda()
+    cols = _cols(w.atoms)
+    out = torch.zeros(g ** 3, device="cuda")
+    pairs = float(g ** 3) * w.atoms.shape[0]
+    rows = []
+    for cfg in ref_kernels.space():
+        times = []
+        for rep in range(3):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            ref_kernels.run_tuned(cfg, ta, cols, w.atoms.shape[0], w.spacing, g, out)
+            b.record()
+            b.synchronize()
+            if rep:
+                times.append(a.elapsed_time(b))
+        rows.append({**cfg, "ms": min(times), "gpairs_per_s": pairs / (min(times) * 1e-3) / 1e9})
+    best = min(rows, key=lambda r: r["ms"])
+    ref = []
+    for rep in range(2):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        ref_kernels.run_reference(ta, w.atoms.shape[0], w.spacing, g, out)
+        b.record()
+        b.synchronize()
+        ref.append(a.elapsed_time(b))
+    tuned = ktt_b200.tuned("b200_map3d")
+    mine = []
+    for rep in range(3):
+        ctx.forward_3d(ta, w.dims, w.spacing, tune=tuned, out=out.reshape(g, g, g))
+        mine.append(ctx.elapsed_ms())
+    result = {"workload": "256^3 grid, h 0.5, 65,536 atoms U[0,128)^3 (seed 2)", "configurations": rows,
+              "best": best, "reference_kernel_ms": min(ref),
+              "this_library": {"tune": tuned.as_dict(), "ms": min(mine[1:]),
+                               "gpairs_per_s": pairs / (min(mine[1:]) * 1e-3) / 1e9},
+              "nvrtc_options": ref_kernels.manifest()["options"]}
+    with open(os.environ["KTT_REF_SWEEP_OUT"], "w") as f:
+        json.dump(result, f, indent=1)
+    assert best["ms"] > 0
