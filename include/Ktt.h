@@ -13,3 +13,4 @@
 #include <ktt/Searcher.h>
 #include <ktt/StopCondition.h>
 #include <ktt/Tuner.h>
+#include <ktt/TuningLoader.h>

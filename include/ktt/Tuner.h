@@ -78,6 +78,12 @@ public:
         const DimensionVector& globalSize, const DimensionVector& localSize, const std::vector<std::string>& typeNames = {});
     KernelDefinitionId AddKernelDefinitionFromFile(const std::string& name, const std::string& filePath,
         const DimensionVector& globalSize, const DimensionVector& localSize, const std::vector<std::string>& typeNames = {});
+    // Without sizes: global and local size (1, 1, 1), to be set by thread modifiers (KTT's JSON
+    // tuning scripts define their kernels this way).
+    KernelDefinitionId AddKernelDefinition(const std::string& name, const std::string& source,
+        const std::vector<std::string>& typeNames = {});
+    KernelDefinitionId AddKernelDefinitionFromFile(const std::string& name, const std::string& filePath,
+        const std::vector<std::string>& typeNames = {});
     KernelDefinitionId GetKernelDefinitionId(const std::string& name, const std::vector<std::string>& typeNames = {}) const;
     void RemoveKernelDefinition(const KernelDefinitionId id);
     void SetArguments(const KernelDefinitionId id, const std::vector<ArgumentId>& argumentIds);
@@ -123,6 +129,17 @@ public:
     void AddConstraint(const KernelId id, const std::vector<std::string>& parameters, ConstraintFunction function);
     void AddGenericConstraint(const KernelId id, const std::vector<std::string>& parameters, GenericConstraintFunction function);
 
+    // Script forms.  KTT evaluates these strings with embedded Python; here the Python expression
+    // subset of KTT's scripts (arithmetic, comparisons, and/or/not, conditional expressions, lists,
+    // comprehensions, min/max/range/...) is parsed and evaluated natively.  A values script yields
+    // a list; a modifier script sees every tuning parameter by name and the incoming size as
+    // "defaultSize"; a constraint script sees the named parameters.
+    void AddScriptParameter(const KernelId id, const std::string& name, const ParameterValueType valueType,
+        const std::string& valueScript, const std::string& group = "");
+    void AddScriptThreadModifier(const KernelId id, const std::vector<KernelDefinitionId>& definitionIds, const ModifierType type,
+        const ModifierDimension dimension, const std::string& script);
+    void AddScriptConstraint(const KernelId id, const std::vector<std::string>& parameters, const std::string& script);
+
     // ---- arguments -------------------------------------------------------------------------
     template <typename T>
     ArgumentId AddArgumentVector(const std::vector<T>& data, const ArgumentAccessType accessType, const ArgumentId& customId = "")
@@ -163,6 +180,18 @@ public:
             &data, sizeof(T), customId);
     }
 
+    // Vector argument read from a raw binary file, or generated by a script evaluated once per
+    // element index (bound to "i") and converted to dataType.
+    ArgumentId AddArgumentVectorFromFile(const std::string& filePath, const ArgumentDataType dataType, const size_t elementSize,
+        const ArgumentAccessType accessType, const ArgumentMemoryLocation memoryLocation = ArgumentMemoryLocation::Device,
+        const ArgumentManagementType managementType = ArgumentManagementType::Framework, const ArgumentId& customId = "");
+    ArgumentId AddArgumentVectorFromGenerator(const std::string& generatorFunction, const ArgumentDataType dataType,
+        const size_t bufferSize, const size_t elementSize, const ArgumentAccessType accessType,
+        const ArgumentMemoryLocation memoryLocation = ArgumentMemoryLocation::Device,
+        const ArgumentManagementType managementType = ArgumentManagementType::Framework, const ArgumentId& customId = "");
+    // Writes the argument's current data (from the device once it has been used there) to a raw file.
+    void SaveArgumentVector(const ArgumentId& id, const std::string& filePath);
+
     void RemoveArgument(const ArgumentId& id);
     void SetReadOnlyArgumentCache(const bool flag);
 
@@ -183,8 +212,15 @@ public:
     KernelResult TuneIteration(const KernelId id, const std::vector<BufferOutputDescriptor>& output,
         const bool recomputeReference = false);
     std::vector<KernelResult> SimulateTuning(const KernelId id, const std::vector<KernelResult>& results,
-        const uint64_t iterations = 0);
+        std::unique_ptr<StopCondition> stopCondition = nullptr);
+    // The same, stopping after `iterations` replayed configurations (0 = until the space is exhausted).
+    std::vector<KernelResult> SimulateTuning(const KernelId id, const std::vector<KernelResult>& results,
+        const uint64_t iterations);
     void SetSearcher(const KernelId id, std::unique_ptr<Searcher> searcher);
+    // KTT's profile-based searcher needs CUPTI counters and a trained model loaded through embedded
+    // Python; neither is part of this library, so this logs an error and leaves the searcher unchanged.
+    void SetProfileBasedSearcher(const KernelId id, const std::string& modelPath, const bool useBuiltinModule = true,
+        const uint32_t batchSize = 5, const uint32_t neighborSize = 100, const uint32_t randomSize = 10);
     void InitializeConfigurationData(const KernelId id);
     void ClearConfigurationData(const KernelId id);
     uint64_t GetConfigurationsCount(const KernelId id) const;

@@ -24,6 +24,7 @@ INCLUDE = os.path.join(REPO, "include")
 BUILD = os.path.join(HERE, "_build")
 LIB_CUDA = os.path.join(HERE, "libcoulktt.so")
 LIB_TUNER = os.path.join(HERE, "libktt_b200.so")
+LAUNCHER = os.path.join(HERE, "ktt_tuning_launcher")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler",
@@ -108,6 +109,13 @@ def build(verbose: bool = False, workers: int | None = None) -> list[str]:
             _run([cxx, "-shared", "-o", LIB_TUNER] + cpp_objs +
                  ["-L", HERE, "-lcoulktt", "-Wl,-rpath,$ORIGIN", "-pthread"])
         out.append(LIB_TUNER)
+        # KTT's TuningLauncher counterpart: runs a JSON tuning script
+        launcher_src = os.path.join(CSRC, "launcher", "ktt_tuning_launcher.cpp")
+        if (not os.path.exists(LAUNCHER) or os.path.getmtime(LIB_TUNER) > os.path.getmtime(LAUNCHER)
+                or _stale(LAUNCHER, launcher_src, newest)):
+            _run([cxx] + CXX_FLAGS + [launcher_src, "-o", LAUNCHER, "-L", HERE, "-lktt_b200", "-lcoulktt",
+                                      "-Wl,-rpath,$ORIGIN", "-pthread"])
+        out.append(LAUNCHER)
     return out
 
 

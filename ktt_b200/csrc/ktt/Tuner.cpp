@@ -4,11 +4,15 @@
 // turned into the invalid return values of KTT 2.1.0 (Source/Tuner.cpp:40-150): InvalidKernelId,
 // InvalidKernelDefinitionId, InvalidArgumentId, an empty configuration, or a KernelResult whose
 // status says what went wrong.
+#include <algorithm>
+#include <cstring>
 #include <fstream>
 #include <iterator>
+#include <memory>
 #include <sstream>
 
 #include "Logger.h"
+#include "Script.h"
 #include "TunerCore.h"
 
 namespace ktt
@@ -108,6 +112,18 @@ KernelDefinitionId Tuner::AddKernelDefinitionFromFile(const std::string& name, c
     }, InvalidKernelDefinitionId);
 }
 
+KernelDefinitionId Tuner::AddKernelDefinition(const std::string& name, const std::string& source,
+    const std::vector<std::string>& typeNames)
+{
+    return AddKernelDefinition(name, source, DimensionVector(), DimensionVector(), typeNames);
+}
+
+KernelDefinitionId Tuner::AddKernelDefinitionFromFile(const std::string& name, const std::string& filePath,
+    const std::vector<std::string>& typeNames)
+{
+    return AddKernelDefinitionFromFile(name, filePath, DimensionVector(), DimensionVector(), typeNames);
+}
+
 KernelDefinitionId Tuner::GetKernelDefinitionId(const std::string& name, const std::vector<std::string>& typeNames) const
 {
     return m_Core->GetDefinitionId(name, typeNames);
@@ -189,6 +205,291 @@ void Tuner::AddConstraint(const KernelId id, const std::vector<std::string>& par
 void Tuner::AddGenericConstraint(const KernelId id, const std::vector<std::string>& parameters, GenericConstraintFunction function)
 {
     GuardedVoid([&] { m_Core->AddConstraint(id, parameters, function, false); });
+}
+
+// ---- script forms (Source/Tuner.h:233-336 of KTT; evaluated by Script.cpp) ----------------------
+
+namespace
+{
+
+script::Value ScriptValue(const ParameterValue& v, const std::string& name)
+{
+    if (const auto* p = std::get_if<uint64_t>(&v)) return script::Value::Int(static_cast<int64_t>(*p));
+    if (const auto* p = std::get_if<int64_t>(&v)) return script::Value::Int(*p);
+    if (const auto* p = std::get_if<double>(&v)) return script::Value::Float(*p);
+    if (const auto* p = std::get_if<bool>(&v)) return script::Value::Bool(*p);
+    throw std::runtime_error("string parameter " + name + " cannot be used in a script");
+}
+
+ParameterValue ParameterFromScript(const script::Value& v, const ParameterValueType type, const std::string& name)
+{
+    switch (type)
+    {
+    case ParameterValueType::UnsignedInt:
+        if (v.kind == script::Value::Kind::Float || v.AsInt() < 0)
+        {
+            throw std::runtime_error("value " + v.Repr() + " of parameter " + name + " is not an unsigned integer");
+        }
+        return static_cast<uint64_t>(v.AsInt());
+    case ParameterValueType::Int:
+        if (v.kind == script::Value::Kind::Float)
+        {
+            throw std::runtime_error("value " + v.Repr() + " of parameter " + name + " is not an integer");
+        }
+        return v.AsInt();
+    case ParameterValueType::Double: return v.AsDouble();
+    case ParameterValueType::Bool: return v.Truthy();
+    case ParameterValueType::String: break;
+    }
+
+    throw std::runtime_error("string parameters cannot be produced by a values script (parameter " + name + ")");
+}
+
+template <typename T>
+void AppendBytes(std::vector<uint8_t>& out, const T value)
+{
+    const auto* p = reinterpret_cast<const uint8_t*>(&value);
+    out.insert(out.end(), p, p + sizeof(T));
+}
+
+size_t DataTypeSize(const ArgumentDataType type)
+{
+    switch (type)
+    {
+    case ArgumentDataType::Char:
+    case ArgumentDataType::UnsignedChar: return 1;
+    case ArgumentDataType::Short:
+    case ArgumentDataType::UnsignedShort:
+    case ArgumentDataType::Half: return 2;
+    case ArgumentDataType::Int:
+    case ArgumentDataType::UnsignedInt:
+    case ArgumentDataType::Float: return 4;
+    case ArgumentDataType::Long:
+    case ArgumentDataType::UnsignedLong:
+    case ArgumentDataType::Double: return 8;
+    case ArgumentDataType::Custom: return 0;
+    }
+
+    return 0;
+}
+
+} // namespace
+
+void Tuner::AddScriptParameter(const KernelId id, const std::string& name, const ParameterValueType valueType,
+    const std::string& valueScript, const std::string& group)
+{
+    GuardedVoid([&]
+    {
+        const script::Expression expression(valueScript);
+        const script::Value list = expression.Evaluate(script::Environment());
+
+        if (list.kind != script::Value::Kind::List || list.list.empty())
+        {
+            throw std::runtime_error("the values script of parameter " + name + " must yield a non-empty list");
+        }
+
+        std::vector<ParameterValue> values;
+
+        for (const auto& v : list.list)
+        {
+            values.push_back(ParameterFromScript(v, valueType, name));
+        }
+
+        m_Core->AddParameter(id, name, values, group);
+    });
+}
+
+void Tuner::AddScriptThreadModifier(const KernelId id, const std::vector<KernelDefinitionId>& definitionIds,
+    const ModifierType type, const ModifierDimension dimension, const std::string& script)
+{
+    GuardedVoid([&]
+    {
+        auto expression = std::make_shared<script::Expression>(script);
+        std::vector<std::string> names;
+
+        for (const auto& free : expression->FreeNames())
+        {
+            if (free == "defaultSize")
+            {
+                continue;
+            }
+
+            const auto& parameters = m_Core->Kernel(id).parameters;
+            const bool known = std::any_of(parameters.cbegin(), parameters.cend(),
+                [&](const KernelParameterInfo& p) { return p.name == free; });
+
+            if (!known)
+            {
+                throw std::runtime_error("thread modifier script '" + script + "' reads " + free
+                    + ", which is not a tuning parameter of the kernel");
+            }
+
+            names.push_back(free);
+        }
+
+        ModifierData data;
+        data.type = type;
+        data.dimension = dimension;
+        data.definitions = definitionIds;
+        data.parameters = names;
+        data.function = [expression, names](const uint64_t defaultSize, const std::vector<uint64_t>& values)
+        {
+            script::Environment env;
+            env.Set("defaultSize", script::Value::Int(static_cast<int64_t>(defaultSize)));
+
+            for (size_t k = 0; k < names.size(); ++k)
+            {
+                env.Set(names[k], script::Value::Int(static_cast<int64_t>(values[k])));
+            }
+
+            const int64_t size = expression->Evaluate(env).AsInt();
+
+            if (size < 0)
+            {
+                throw std::runtime_error("thread modifier script '" + expression->Source() + "' gave a negative size");
+            }
+
+            return static_cast<uint64_t>(size);
+        };
+        m_Core->AddModifier(id, data);
+    });
+}
+
+void Tuner::AddScriptConstraint(const KernelId id, const std::vector<std::string>& parameters, const std::string& script)
+{
+    GuardedVoid([&]
+    {
+        auto expression = std::make_shared<script::Expression>(script);
+        m_Core->AddConstraint(id, parameters, [expression, parameters](const std::vector<const ParameterValue*>& values)
+        {
+            script::Environment env;
+
+            for (size_t k = 0; k < parameters.size(); ++k)
+            {
+                env.Set(parameters[k], ScriptValue(*values[k], parameters[k]));
+            }
+
+            return expression->Evaluate(env).Truthy();
+        }, false);
+    });
+}
+
+ArgumentId Tuner::AddArgumentVectorFromFile(const std::string& filePath, const ArgumentDataType dataType, const size_t elementSize,
+    const ArgumentAccessType accessType, [[maybe_unused]] const ArgumentMemoryLocation memoryLocation,
+    [[maybe_unused]] const ArgumentManagementType managementType, const ArgumentId& customId)
+{
+    std::vector<uint8_t> data;
+
+    try
+    {
+        std::ifstream file(filePath, std::ios::binary);
+
+        if (!file)
+        {
+            throw std::runtime_error("Unable to open argument data file " + filePath);
+        }
+
+        data.assign(std::istreambuf_iterator<char>(file), std::istreambuf_iterator<char>());
+
+        if (elementSize == 0 || data.size() % elementSize != 0)
+        {
+            throw std::runtime_error("File " + filePath + " holds " + std::to_string(data.size())
+                + " bytes, not a whole number of " + std::to_string(elementSize) + "-byte elements");
+        }
+    }
+    catch (const std::exception& e)
+    {
+        log::Error(e.what());
+        return InvalidArgumentId;
+    }
+
+    return AddArgumentWithOwnedData(elementSize, dataType, ArgumentMemoryType::Vector, accessType, data.data(), data.size(),
+        customId);
+}
+
+ArgumentId Tuner::AddArgumentVectorFromGenerator(const std::string& generatorFunction, const ArgumentDataType dataType,
+    const size_t bufferSize, const size_t elementSize, const ArgumentAccessType accessType,
+    [[maybe_unused]] const ArgumentMemoryLocation memoryLocation, [[maybe_unused]] const ArgumentManagementType managementType,
+    const ArgumentId& customId)
+{
+    std::vector<uint8_t> data;
+
+    try
+    {
+        if (elementSize == 0 || DataTypeSize(dataType) != elementSize || bufferSize % elementSize != 0)
+        {
+            throw std::runtime_error("Generated argument: element size " + std::to_string(elementSize)
+                + " does not match its data type, or the buffer size " + std::to_string(bufferSize)
+                + " is not a whole number of elements");
+        }
+
+        const script::Expression expression(generatorFunction);
+        const size_t count = bufferSize / elementSize;
+        data.reserve(bufferSize);
+        script::Environment env;
+
+        for (size_t i = 0; i < count; ++i)
+        {
+            env.Set("i", script::Value::Int(static_cast<int64_t>(i)));
+            const script::Value v = expression.Evaluate(env);
+
+            switch (dataType)
+            {
+            case ArgumentDataType::Float: AppendBytes(data, static_cast<float>(v.AsDouble())); break;
+            case ArgumentDataType::Double: AppendBytes(data, v.AsDouble()); break;
+            case ArgumentDataType::Char: AppendBytes(data, static_cast<int8_t>(v.AsInt())); break;
+            case ArgumentDataType::UnsignedChar: AppendBytes(data, static_cast<uint8_t>(v.AsInt())); break;
+            case ArgumentDataType::Short: AppendBytes(data, static_cast<int16_t>(v.AsInt())); break;
+            case ArgumentDataType::UnsignedShort: AppendBytes(data, static_cast<uint16_t>(v.AsInt())); break;
+            case ArgumentDataType::Int: AppendBytes(data, static_cast<int32_t>(v.AsInt())); break;
+            case ArgumentDataType::UnsignedInt: AppendBytes(data, static_cast<uint32_t>(v.AsInt())); break;
+            case ArgumentDataType::Long: AppendBytes(data, static_cast<int64_t>(v.AsInt())); break;
+            case ArgumentDataType::UnsignedLong: AppendBytes(data, static_cast<uint64_t>(v.AsInt())); break;
+            default: throw std::runtime_error("Generated arguments of this data type are not supported");
+            }
+        }
+    }
+    catch (const std::exception& e)
+    {
+        log::Error(e.what());
+        return InvalidArgumentId;
+    }
+
+    return AddArgumentWithOwnedData(elementSize, dataType, ArgumentMemoryType::Vector, accessType, data.data(), data.size(),
+        customId);
+}
+
+void Tuner::SaveArgumentVector(const ArgumentId& id, const std::string& filePath)
+{
+    GuardedVoid([&]
+    {
+        ArgumentData& argument = m_Core->Argument(id);
+
+        if (argument.memoryType != ArgumentMemoryType::Vector)
+        {
+            throw std::runtime_error("Argument " + id + " is not a vector");
+        }
+
+        std::vector<uint8_t> bytes(argument.bytes);
+
+        if (argument.ownership == ArgumentOwnership::User || argument.deviceCurrent)
+        {
+            m_Core->DownloadArgument(argument, bytes.data(), bytes.size());
+        }
+        else
+        {
+            std::memcpy(bytes.data(), argument.HostData(), bytes.size());
+        }
+
+        std::ofstream file(filePath, std::ios::binary);
+
+        if (!file)
+        {
+            throw std::runtime_error("Unable to write " + filePath);
+        }
+
+        file.write(reinterpret_cast<const char*>(bytes.data()), static_cast<std::streamsize>(bytes.size()));
+    });
 }
 
 ArgumentId Tuner::AddArgumentWithOwnedData(const size_t elementSize, const ArgumentDataType dataType,
@@ -336,12 +637,26 @@ KernelResult Tuner::TuneIteration(const KernelId id, const std::vector<BufferOut
 
 std::vector<KernelResult> Tuner::SimulateTuning(const KernelId id, const std::vector<KernelResult>& results, const uint64_t iterations)
 {
-    return Guarded([&] { return m_Core->SimulateTuning(id, results, iterations); }, std::vector<KernelResult>{});
+    return Guarded([&] { return m_Core->SimulateTuning(id, results, iterations, nullptr); }, std::vector<KernelResult>{});
+}
+
+std::vector<KernelResult> Tuner::SimulateTuning(const KernelId id, const std::vector<KernelResult>& results,
+    std::unique_ptr<StopCondition> stopCondition)
+{
+    return Guarded([&] { return m_Core->SimulateTuning(id, results, 0, stopCondition.get()); }, std::vector<KernelResult>{});
 }
 
 void Tuner::SetSearcher(const KernelId id, std::unique_ptr<Searcher> searcher)
 {
     GuardedVoid([&] { m_Core->SetSearcher(id, std::move(searcher)); });
+}
+
+void Tuner::SetProfileBasedSearcher([[maybe_unused]] const KernelId id, const std::string& modelPath,
+    [[maybe_unused]] const bool useBuiltinModule, [[maybe_unused]] const uint32_t batchSize,
+    [[maybe_unused]] const uint32_t neighborSize, [[maybe_unused]] const uint32_t randomSize)
+{
+    log::Error("The profile-based searcher (model " + modelPath + ") needs CUPTI counters and a Python-loaded model, "
+        "which this library does not provide; the kernel keeps its current searcher");
 }
 
 void Tuner::InitializeConfigurationData(const KernelId id) { GuardedVoid([&] { (void)m_Core->Space(id); }); }

@@ -722,7 +722,7 @@ DimensionVector TunerCore::ModifiedSize(const KernelData& kernel, const KernelDe
 }
 
 Nanoseconds TunerCore::LaunchDefinition(const KernelData& kernel, const KernelDefinitionId id,
-    const KernelConfiguration& configuration, [[maybe_unused]] const DimensionVector& global, const DimensionVector& local)
+    const KernelConfiguration& configuration, const DimensionVector& global, const DimensionVector& local)
 {
     (void)kernel;
     const DefinitionData& definition = Definition(id);
@@ -819,7 +819,9 @@ Nanoseconds TunerCore::LaunchDefinition(const KernelData& kernel, const KernelDe
     tune.rsqrt_soft = static_cast<int>(parameter("RSQRT_SOFT", 0));
     tune.atom_split = static_cast<int>(parameter("ATOM_SPLIT", 0));
 
-    const bool threeD = definition.globalSize.GetSizeZ() > 1;
+    // a 3D launch: the definition's global size, or (for definitions sized by modifier scripts) the
+    // launch's, spans more than one z plane
+    const bool threeD = definition.globalSize.GetSizeZ() > 1 || global.GetSizeZ() > 1;
     int rc = COUL_OK;
 
     if (definition.name == "directCoulombSum" && args.size() == 9 && threeD)
@@ -1309,10 +1311,10 @@ KernelResult TunerCore::TuneIteration(const KernelId id, const std::vector<Buffe
 }
 
 std::vector<KernelResult> TunerCore::SimulateTuning(const KernelId id, const std::vector<KernelResult>& recorded,
-    const uint64_t iterations)
+    const uint64_t iterations, StopCondition* stop)
 {
     // Replays recorded results through the searcher without running anything
-    // (Source/TuningRunner/TuningRunner.cpp:131-201).
+    // (Source/TuningRunner/TuningRunner.cpp:131-201); a stop condition sees the recorded results.
     KernelData& kernel = Kernel(id);
     ClearSpace(id);
     ConfigurationSpace& space = Space(id);
@@ -1325,7 +1327,13 @@ std::vector<KernelResult> TunerCore::SimulateTuning(const KernelId id, const std
     kernel.searcher->Initialize(space);
     std::vector<KernelResult> results;
 
-    while (!space.IsExhausted() && (iterations == 0 || results.size() < iterations))
+    if (stop != nullptr)
+    {
+        stop->Initialize(space.GetConfigurationsCount());
+    }
+
+    while (!space.IsExhausted() && (iterations == 0 || results.size() < iterations)
+        && (stop == nullptr || !stop->IsFulfilled()))
     {
         const KernelConfiguration configuration = kernel.searcher->GetCurrentConfiguration();
         auto it = std::find_if(recorded.cbegin(), recorded.cend(),
@@ -1346,6 +1354,17 @@ std::vector<KernelResult> TunerCore::SimulateTuning(const KernelId id, const std
         }
 
         results.push_back(result);
+
+        if (stop != nullptr)
+        {
+            stop->Update(result);
+
+            if (stop->IsFulfilled())
+            {
+                log::Info(stop->GetStatusString());
+                break;
+            }
+        }
 
         if (space.IsExhausted() || !kernel.searcher->CalculateNextConfiguration(result))
         {

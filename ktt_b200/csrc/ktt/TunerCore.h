@@ -132,7 +132,8 @@ public:
         const KernelRunMode mode);
     std::vector<KernelResult> Tune(const KernelId id, std::unique_ptr<StopCondition> stop);
     KernelResult TuneIteration(const KernelId id, const std::vector<BufferOutputDescriptor>& output, const bool recompute);
-    std::vector<KernelResult> SimulateTuning(const KernelId id, const std::vector<KernelResult>& results, const uint64_t iterations);
+    std::vector<KernelResult> SimulateTuning(const KernelId id, const std::vector<KernelResult>& results, const uint64_t iterations,
+        StopCondition* stop);
     void SetSearcher(const KernelId id, std::unique_ptr<Searcher> searcher);
     ConfigurationSpace& Space(const KernelId id);
     void ClearSpace(const KernelId id);

@@ -23,6 +23,12 @@ It writes, next to this script:
   in simulated tuning without a GPU.
 * ``ktt_prefix.json`` -- the configuration -> ``#define`` prefix expectation of
   ``Tests/KernelManagerTests.cpp:57-81``.
+* ``ktt_scripts/`` -- KTT's two JSON tuning scripts for this path, parsed and
+  written back unchanged in content: ``Examples/JSON/CoulombSum3d.json`` (the
+  known-answer run: generated atoms, validated against ``Coulomb3d.bin`` at 0.01)
+  and ``Examples/CoulombSum3d/CoulombSum3dCudaScript.json`` (simulated tuning
+  over the recorded 2080 Ti results), with ``manifest.json`` naming each
+  source file and its sha256.  The tuning-script loader's tests run them.
 """
 from __future__ import annotations
 
@@ -117,6 +123,23 @@ def prefix(ktt_root: str) -> None:
         json.dump(out, f, indent=1)
 
 
+def scripts(ktt_root: str) -> None:
+    out_dir = os.path.join(HERE, "ktt_scripts")
+    os.makedirs(out_dir, exist_ok=True)
+    manifest = {}
+    for rel in ("Examples/JSON/CoulombSum3d.json", "Examples/CoulombSum3d/CoulombSum3dCudaScript.json"):
+        raw = open(os.path.join(ktt_root, rel), "rb").read()
+        doc = json.loads(raw)
+        name = os.path.basename(rel)
+        with open(os.path.join(out_dir, name), "w") as f:
+            json.dump(doc, f, indent=1)
+            f.write("\n")
+        manifest[name] = {"source": rel + " (KTT 2.1.0)", "sha256": hashlib.sha256(raw).hexdigest()}
+    with open(os.path.join(out_dir, "manifest.json"), "w") as f:
+        json.dump(manifest, f, indent=1)
+        f.write("\n")
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--ktt-root", default="/root/reference")
@@ -124,6 +147,7 @@ def main() -> None:
     kat(args.ktt_root)
     space_2080(args.ktt_root)
     prefix(args.ktt_root)
+    scripts(args.ktt_root)
 
 
 if __name__ == "__main__":
