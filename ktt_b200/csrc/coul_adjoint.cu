@@ -65,20 +65,34 @@ __global__ void __launch_bounds__(kAdjThreads) adjoint_kernel(const AdjParams p)
     const int64_t rows = static_cast<int64_t>(p.ny) * p.nz;
     const int64_t r_begin = static_cast<int64_t>(blockIdx.y) * p.rows_per_chunk;
     const int64_t r_end = r_begin + p.rows_per_chunk < rows ? r_begin + p.rows_per_chunk : rows;
+    // Atoms in lane pairs (k = 2m, 2m + 1): the per-pair FP32 work runs as packed FFMA2 / FMUL2 /
+    // FADD2 instructions, two atoms per instruction, halving the issue slots the FMA pipe needs.
+    constexpr int P = A / 2;
+    static_assert(A % 2 == 0, "atoms per thread come in lane pairs");
+    float2 nax[P];
+#pragma unroll
+    for (int m = 0; m < P; ++m)
+        nax[m] = make_float2(-ax[2 * m], -ax[2 * m + 1]);
+
     for (int64_t row = r_begin; row < r_end; ++row) {
         const int y = static_cast<int>(row % p.ny);
         const int z = static_cast<int>(row / p.ny);
         const float gy = fmaf(static_cast<float>(y), p.h, p.oy);
         const float gz = fmaf(static_cast<float>(z), p.h, p.oz);
-        float dy[A], dz[A], dyz2[A], sq[A], sx[A], s3[A];
+        float dy[A], dz[A];
+        float2 dyz2[P], sq[P], sx[P], s3[P];
 #pragma unroll
         for (int k = 0; k < A; ++k) {
             dy[k] = gy - ay[k];
             dz[k] = gz - az[k];
-            dyz2[k] = fmaf(dy[k], dy[k], dz[k] * dz[k]);
-            sq[k] = 0.0f;
-            sx[k] = 0.0f;
-            s3[k] = 0.0f;
+        }
+#pragma unroll
+        for (int m = 0; m < P; ++m) {
+            dyz2[m] = make_float2(fmaf(dy[2 * m], dy[2 * m], dz[2 * m] * dz[2 * m]),
+                                  fmaf(dy[2 * m + 1], dy[2 * m + 1], dz[2 * m + 1] * dz[2 * m + 1]));
+            sq[m] = make_float2(0.0f, 0.0f);
+            sx[m] = make_float2(0.0f, 0.0f);
+            s3[m] = make_float2(0.0f, 0.0f);
         }
         const float* grow = p.grad_map + row * static_cast<int64_t>(p.nx);
         for (int x0 = 0; x0 < p.nx; x0 += kAdjSegment) {
@@ -87,28 +101,36 @@ __global__ void __launch_bounds__(kAdjThreads) adjoint_kernel(const AdjParams p)
             for (int i = tid; i < len; i += kAdjThreads)
                 s_g[i] = grow[x0 + i];
             __syncthreads();
+#pragma unroll 2
             for (int i = 0; i < len; ++i) {
-                const float g = s_g[i];
-                const float gx = fmaf(static_cast<float>(x0 + i), p.h, p.ox);
+                const float2 g = splat(s_g[i]);
+                const float2 gx = splat(fmaf(static_cast<float>(x0 + i), p.h, p.ox));
 #pragma unroll
-                for (int k = 0; k < A; ++k) {
-                    const float dx = gx - ax[k];
-                    const float r2 = fmaf(dx, dx, dyz2[k]);
-                    const float inv = rsqrt_mufu(r2);
-                    const float t = g * inv;
-                    sq[k] += t;
-                    const float t3 = t * inv * inv;
-                    sx[k] = fmaf(t3, dx, sx[k]);
-                    s3[k] += t3;
+                for (int m = 0; m < P; ++m) {
+                    const float2 dx = __fadd2_rn(gx, nax[m]);
+                    const float2 r2 = __ffma2_rn(dx, dx, dyz2[m]);
+                    const float2 inv = make_float2(rsqrt_mufu(r2.x), rsqrt_mufu(r2.y));
+                    const float2 t = __fmul2_rn(g, inv);
+                    sq[m] = __fadd2_rn(sq[m], t);
+                    const float2 t3 = __fmul2_rn(t, __fmul2_rn(inv, inv));
+                    sx[m] = __ffma2_rn(t3, dx, sx[m]);
+                    s3[m] = __fadd2_rn(s3[m], t3);
                 }
             }
         }
 #pragma unroll
-        for (int k = 0; k < A; ++k) {
-            acc[k][0] += static_cast<double>(sq[k]);
-            acc[k][1] += static_cast<double>(sx[k]);
-            acc[k][2] += static_cast<double>(dy[k]) * static_cast<double>(s3[k]);
-            acc[k][3] += static_cast<double>(dz[k]) * static_cast<double>(s3[k]);
+        for (int m = 0; m < P; ++m) {
+#pragma unroll
+            for (int l = 0; l < 2; ++l) {
+                const int k = 2 * m + l;
+                const float vq = l ? sq[m].y : sq[m].x;
+                const float vx = l ? sx[m].y : sx[m].x;
+                const float v3 = l ? s3[m].y : s3[m].x;
+                acc[k][0] += static_cast<double>(vq);
+                acc[k][1] += static_cast<double>(vx);
+                acc[k][2] += static_cast<double>(dy[k]) * static_cast<double>(v3);
+                acc[k][3] += static_cast<double>(dz[k]) * static_cast<double>(v3);
+            }
         }
     }
 
