@@ -116,6 +116,24 @@ def build(verbose: bool = False, workers: int | None = None) -> list[str]:
             _run([cxx] + CXX_FLAGS + [launcher_src, "-o", LAUNCHER, "-L", HERE, "-lktt_b200", "-lcoulktt",
                                       "-Wl,-rpath,$ORIGIN", "-pthread"])
         out.append(LAUNCHER)
+        # the Python module of the ktt:: surface, under KTT's module name (pyktt)
+        try:
+            import sysconfig
+
+            import pybind11
+            pyktt = os.path.join(HERE, "pyktt" + sysconfig.get_config_var("EXT_SUFFIX"))
+            pyktt_src = os.path.join(CSRC, "python", "pyktt.cpp")
+            if (not os.path.exists(pyktt) or os.path.getmtime(LIB_TUNER) > os.path.getmtime(pyktt)
+                    or _stale(pyktt, pyktt_src, newest)):
+                if verbose:
+                    print("[ktt_b200.build] compiling the pyktt module", file=sys.stderr)
+                _run([cxx] + CXX_FLAGS + ["-shared", "-fvisibility=hidden", "-I", sysconfig.get_paths()["include"],
+                                          "-I", pybind11.get_include(), pyktt_src, "-o", pyktt, "-L", HERE,
+                                          "-lktt_b200", "-lcoulktt", "-Wl,-rpath,$ORIGIN"])
+            out.append(pyktt)
+        except ImportError:
+            if verbose:
+                print("[ktt_b200.build] pybind11 not importable: pyktt module not built", file=sys.stderr)
     return out
 
 

@@ -1,0 +1,69 @@
+"""A KTT-style Python host program for CoulombSum3d through pyktt on the B200: the kernel
+definition, arguments, KTT's tuning parameters, thread modifiers and constraints
+(Examples/CoulombSum3d/CoulombSum3d.cpp:67-237, written against KTT's Python API), a reference
+computation in Python (the FP64 oracle) and KTT's SideBySide validation, a random-search Tune, then
+Run of the best configuration with the output downloaded into a NumPy array."""
+import numpy as np
+import pytest
+
+import oracle
+from ktt_b200 import errors
+from ktt_b200 import pyktt as ktt
+
+pytestmark = pytest.mark.gpu
+
+
+def test_coulomb3d_python_host_program():
+    grid, n, h = 128, 1024, 0.5
+    rng = np.random.default_rng(21)
+    atoms = np.empty((n, 4), dtype=np.float32)
+    atoms[:, :3] = rng.uniform(0.0, grid * h, (n, 3))
+    atoms[:, 3] = rng.uniform(-1.0, 1.0, n)
+    reference = oracle.grid3d(atoms, h, (grid, grid, grid)).astype(np.float32).reshape(-1)
+
+    ktt.Tuner.SetLoggingLevel(ktt.LoggingLevel.Warning)
+    tuner = ktt.Tuner(0, 0, ktt.ComputeApi.CUDA)
+    tuner.SetGlobalSizeType(ktt.GlobalSizeType.CUDA)
+    tuner.SetCompilerOptions("-use_fast_math")
+    d = tuner.AddKernelDefinitionFromFile("directCoulombSum", "CoulombSum3d.cu", ktt.DimensionVector(grid, grid, grid),
+                                          ktt.DimensionVector())
+    k = tuner.CreateSimpleKernel("CoulombSum", d)
+    ro = ktt.ArgumentAccessType.ReadOnly
+    args = [tuner.AddArgumentVectorFloat(atoms.reshape(-1), ro)]
+    args += [tuner.AddArgumentVectorFloat(np.ascontiguousarray(atoms[:, c]), ro) for c in range(4)]
+    args += [tuner.AddArgumentScalarInt(n), tuner.AddArgumentScalarFloat(h), tuner.AddArgumentScalarInt(grid)]
+    grid_id = tuner.AddArgumentVectorFloat(np.zeros(grid ** 3, dtype=np.float32), ktt.ArgumentAccessType.WriteOnly)
+    args.append(grid_id)
+    tuner.SetArguments(d, args)
+
+    tuner.AddParameter(k, "WORK_GROUP_SIZE_X", [16, 32])
+    tuner.AddParameter(k, "WORK_GROUP_SIZE_Y", [1, 2, 4, 8])
+    tuner.AddParameter(k, "WORK_GROUP_SIZE_Z", [1])
+    tuner.AddParameter(k, "Z_ITERATIONS", [1, 2, 4, 8, 16, 32])
+    tuner.AddParameter(k, "INNER_UNROLL_FACTOR", [0, 1, 2, 4, 8, 16, 32])
+    tuner.AddParameter(k, "USE_CONSTANT_MEMORY", [0])
+    tuner.AddParameter(k, "USE_SOA", [0, 1])
+    tuner.AddParameter(k, "VECTOR_SIZE", [1])
+    for dim, name in ((ktt.ModifierDimension.X, "WORK_GROUP_SIZE_X"), (ktt.ModifierDimension.Y, "WORK_GROUP_SIZE_Y")):
+        tuner.AddThreadModifier(k, [d], ktt.ModifierType.Local, dim, name, ktt.ModifierAction.Multiply)
+        tuner.AddThreadModifier(k, [d], ktt.ModifierType.Global, dim, name, ktt.ModifierAction.DivideCeil)
+    tuner.AddThreadModifier(k, [d], ktt.ModifierType.Global, ktt.ModifierDimension.Z, "Z_ITERATIONS",
+                            ktt.ModifierAction.DivideCeil)
+    tuner.AddConstraint(k, ["INNER_UNROLL_FACTOR", "Z_ITERATIONS"], lambda v: v[0] < v[1])
+    tuner.AddConstraint(k, ["WORK_GROUP_SIZE_X", "WORK_GROUP_SIZE_Y"], lambda v: v[0] * v[1] >= 64)
+
+    def compute_reference(buffer):
+        np.frombuffer(buffer, dtype=np.float32)[:] = reference
+
+    tuner.SetReferenceComputation(grid_id, grid ** 3 * 4, compute_reference)
+    tuner.SetValidationMethod(ktt.ValidationMethod.SideBySideComparison, 0.01)
+    tuner.SetSearcher(k, ktt.RandomSearcher())
+    results = tuner.Tune(k, ktt.ConfigurationCount(12))
+    assert len(results) == 12
+    assert all(r.GetStatus() == ktt.ResultStatus.Ok for r in results), [str(r.GetStatus()) for r in results]
+
+    best = tuner.GetBestConfiguration(k)
+    out = np.zeros(grid ** 3, dtype=np.float32)
+    result = tuner.Run(k, best, [ktt.BufferOutputDescriptor(grid_id, out)])
+    assert result.GetStatus() == ktt.ResultStatus.Ok
+    assert errors.report(out, reference)["rel_norm"] <= 1e-5
