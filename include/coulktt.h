@@ -197,7 +197,8 @@ COUL_API int coul_forward_3d_reference(coul_ctx* ctx, const float* d_atoms, int6
 COUL_API int coul_forward_2d(coul_ctx* ctx, const float* d_atoms_xy_dz2_q, int64_t n_atoms, float spacing, int nx,
                              int ny, const coul_tune* tune, int accumulate, float* d_out);
 /* Gather four separate atom arrays (KTT's USE_SOA layout: atomInfoX/Y/Z/W) into float4 (x, y, z, q),
-   on the device; d_out must hold n_atoms float4 and be 16-byte aligned. */
+   on the device; d_out must hold n_atoms float4 and be 16-byte aligned.  d_q may be NULL: the
+   fourth component is then 0 (three-component arrays such as N-body velocities). */
 COUL_API int coul_pack_atoms(coul_ctx* ctx, const float* d_x, const float* d_y, const float* d_z, const float* d_q,
                              int64_t n_atoms, float* d_out);
 /* Convert (x, y, z, q) atoms into the 2D convention (x, y, (z_slice - z)^2, q) on the device. */
@@ -224,6 +225,30 @@ COUL_API int coul_forward_3d_host(coul_ctx* ctx, const float* h_atoms, int64_t n
  */
 COUL_API int coul_adjoint_3d(coul_ctx* ctx, const float* d_atoms, int64_t n_atoms, const coul_grid* grid,
                              const float* d_grad_map, float* d_grad_q, float* d_grad_xyz);
+
+/* ---- N-body: the sibling pair sum of KTT's Nbody example ---------------------------------- */
+/* Tuning fields (the KTT parameter each one covers in brackets, Examples/Nbody/Nbody.cpp:140-209). */
+typedef struct coul_nbody_tune {
+    int block_x;           /* threads per block, a multiple of 32 up to 512      [WORK_GROUP_SIZE_X] */
+    int bodies_per_thread; /* bodies i per thread in registers: 1, 2, 4 or 8     [OUTER_UNROLL_FACTOR] */
+    int unroll;            /* unroll of the loop over bodies j: 1, 2 or 4        [INNER_UNROLL_FACTOR1] */
+    int j_split;           /* 0 / 1: one CTA per tile of bodies i; 2..8: a thread-block cluster of that
+                              many CTAs shares the tile, each taking a share of the bodies j, partial
+                              accelerations reduced over distributed shared memory  [WORK_GROUP_SIZE_Y] */
+} coul_nbody_tune;
+COUL_API int coul_nbody_tune_default(coul_nbody_tune* tune);
+COUL_API int coul_nbody_tune_supported(const coul_nbody_tune* tune);
+/*
+ * One step of KTT's nbody_kernel (Examples/Nbody/Nbody.cu:260-410; reference NbodyReference.cu:36-75):
+ * for every body i, a_i = sum_j m_j d_ij / (|d_ij|^2 + softening_sqr)^(3/2) with d_ij = p_j - p_i,
+ * then p_i' = p_i + dt v_i + damping dt^2 a_i and v_i' = v_i + dt a_i.  d_pos_mass holds n float4
+ * (x, y, z, mass), d_vel n float4 (x, y, z, unused); the outputs (16-byte aligned, not aliasing the
+ * inputs) get (x', y', z', mass) and (vx', vy', vz', 0).  Any n >= 0 (KTT's kernel needs n to be a
+ * multiple of its tile).  Asynchronous on the context's stream; timed by coul_elapsed_ms.
+ */
+COUL_API int coul_nbody_step(coul_ctx* ctx, const float* d_pos_mass, const float* d_vel, int64_t n, float dt,
+                             float damping, float softening_sqr, const coul_nbody_tune* tune, float* d_pos_mass_new,
+                             float* d_vel_new);
 
 /* ---- batched: many molecules in one persistent launch ------------------------------ */
 /*

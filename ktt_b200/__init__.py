@@ -344,6 +344,44 @@ class CoulombContext:
         return out
 
 
+@dataclass
+class NbodyTune:
+    """N-body step configuration (coul_nbody_tune; KTT parameter in brackets): block_x
+    [WORK_GROUP_SIZE_X], bodies_per_thread [OUTER_UNROLL_FACTOR], unroll [INNER_UNROLL_FACTOR1],
+    j_split (cluster of CTAs sharing a tile of bodies, splitting the bodies j) [WORK_GROUP_SIZE_Y]."""
+    block_x: int = 128
+    bodies_per_thread: int = 4
+    unroll: int = 2
+    j_split: int = 0
+
+    def c(self):
+        from ._signatures import NbodyTuneC
+        return NbodyTuneC(self.block_x, self.bodies_per_thread, self.unroll, self.j_split)
+
+
+def nbody_tune_supported(tune: NbodyTune) -> bool:
+    return load_library().coul_nbody_tune_supported(ctypes.byref(tune.c())) == COUL_OK
+
+
+def nbody_step(ctx: "CoulombContext", pos_mass, vel, dt: float, damping: float, softening_sqr: float,
+               tune: NbodyTune | None = None, out_pos=None, out_vel=None):
+    """One step of KTT's N-body example (coul_nbody_step): pos_mass and vel are (n, 4) float32 CUDA
+    tensors; returns (pos_mass', vel')."""
+    import torch
+    CoulombContext._check_atoms(pos_mass)
+    CoulombContext._check_atoms(vel)
+    n = pos_mass.shape[0]
+    if vel.shape[0] != n:
+        raise CoulombError(COUL_ERR_INVALID_ARGUMENT, "pos_mass and vel must hold the same number of bodies")
+    out_pos = torch.empty_like(pos_mass) if out_pos is None else out_pos
+    out_vel = torch.empty_like(vel) if out_vel is None else out_vel
+    ctx._bind_stream()
+    t = (tune or NbodyTune()).c()
+    _check(ctx._lib.coul_nbody_step(ctx.handle, _ptr(pos_mass), _ptr(vel), n, float(dt), float(damping),
+                                    float(softening_sqr), ctypes.byref(t), _ptr(out_pos), _ptr(out_vel)))
+    return out_pos, out_vel
+
+
 def adjoint_3d(ctx: "CoulombContext", atoms, dims, spacing, grad_map, origin=None):
     """dL/dr and dL/dq for G = dL/dV on the map: returns an (n, 4) tensor (dx, dy, dz, dq)."""
     import torch

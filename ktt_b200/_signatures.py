@@ -6,6 +6,11 @@ class Molecule(ctypes.Structure):
     pass
 
 
+class NbodyTuneC(ctypes.Structure):
+    _fields_ = [("block_x", ctypes.c_int), ("bodies_per_thread", ctypes.c_int), ("unroll", ctypes.c_int),
+                ("j_split", ctypes.c_int)]
+
+
 def register(lib) -> None:
     from . import _Grid, _Tune
 
@@ -19,6 +24,10 @@ def register(lib) -> None:
         "coul_batch_info": [vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ci), ctypes.POINTER(ctypes.c_double)],
         "coul_pack_atoms": [vp, vp, vp, vp, vp, ctypes.c_int64, vp],
         "coul_adjoint_3d": [vp, vp, ctypes.c_int64, ctypes.POINTER(_Grid), vp, vp, vp],
+        "coul_nbody_tune_default": [ctypes.POINTER(NbodyTuneC)],
+        "coul_nbody_tune_supported": [ctypes.POINTER(NbodyTuneC)],
+        "coul_nbody_step": [vp, vp, vp, ctypes.c_int64, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                            ctypes.POINTER(NbodyTuneC), vp, vp],
         "coul_buffer_alloc": [vp, ctypes.c_size_t, ctypes.POINTER(vp)],
         "coul_buffer_free": [vp, vp],
         "coul_buffer_upload": [vp, vp, vp, ctypes.c_size_t],

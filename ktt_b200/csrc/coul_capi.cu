@@ -92,7 +92,7 @@ __global__ void pack_atoms_kernel(const float* __restrict__ x, const float* __re
 {
     const int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (j < n)
-        out[j] = make_float4(x[j], y[j], z[j], q[j]);
+        out[j] = make_float4(x[j], y[j], z[j], q != nullptr ? q[j] : 0.0f);
 }
 
 // Self-test of the bounded-wait machinery: one CTA arms an mbarrier for one arrival and waits on
@@ -584,7 +584,7 @@ COUL_API int coul_pack_atoms(coul_ctx* ctx, const float* d_x, const float* d_y, 
 {
     if (ctx == nullptr)
         return set_error(COUL_ERR_INVALID_ARGUMENT, "ctx is NULL");
-    if (n_atoms < 0 || (n_atoms > 0 && (!d_x || !d_y || !d_z || !d_q || !d_out || !aligned16(d_out))))
+    if (n_atoms < 0 || (n_atoms > 0 && (!d_x || !d_y || !d_z || !d_out || !aligned16(d_out))))
         return set_error(COUL_ERR_INVALID_ARGUMENT, "bad atom arrays");
     if (n_atoms == 0)
         return COUL_OK;

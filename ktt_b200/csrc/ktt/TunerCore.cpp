@@ -780,16 +780,9 @@ Nanoseconds TunerCore::LaunchDefinition(const KernelData& kernel, const KernelDe
         }
     };
 
-    auto packedAtoms = [&](const size_t first, const int64_t n) -> const float*
+    // device scratch of at least `bytes` (kept across launches, grown on demand)
+    auto scratch = [&](const size_t bytes) -> float*
     {
-        // KTT's USE_SOA layouts carry the same atoms in four arrays; gather them into float4 on the device.
-        if (parameter("USE_SOA", 0) == 0)
-        {
-            return vector(first);
-        }
-
-        const size_t bytes = static_cast<size_t>(std::max<int64_t>(n, 1)) * 16;
-
         if (m_ScratchBytes < bytes)
         {
             if (m_ScratchDevice != nullptr)
@@ -803,10 +796,22 @@ Nanoseconds TunerCore::LaunchDefinition(const KernelData& kernel, const KernelDe
             m_ScratchBytes = bytes;
         }
 
+        return static_cast<float*>(m_ScratchDevice);
+    };
+
+    auto packedAtoms = [&](const size_t first, const int64_t n) -> const float*
+    {
+        // KTT's USE_SOA layouts carry the same atoms in four arrays; gather them into float4 on the device.
+        if (parameter("USE_SOA", 0) == 0)
+        {
+            return vector(first);
+        }
+
+        float* packed = scratch(static_cast<size_t>(std::max<int64_t>(n, 1)) * 16);
         CheckCoul(coul_pack_atoms(ctx, vector(first + 1), vector(first + 2), vector(first + 3), vector(first + 4), n,
-                      static_cast<float*>(m_ScratchDevice)),
+                      packed),
             "pack of four-array atoms");
-        return static_cast<const float*>(m_ScratchDevice);
+        return packed;
     };
 
     coul_tune tune;
@@ -880,6 +885,50 @@ Nanoseconds TunerCore::LaunchDefinition(const KernelData& kernel, const KernelDe
         rc = coul_forward_2d(ctx, vector(0), static_cast<int64_t>(scalar(1)), static_cast<float>(scalar(2)),
             static_cast<int>(definition.globalSize.GetSizeX()), static_cast<int>(definition.globalSize.GetSizeY()), &reference, 0,
             vector(3));
+    }
+    else if (definition.name == "nbody_kernel" && args.size() == 15)
+    {
+        // Examples/Nbody/Nbody.cu:260-275: (timeDelta, oldBodyInfo, oldPosX, oldPosY, oldPosZ, mass, newBodyInfo,
+        // oldVel, oldVelX, oldVelY, oldVelZ, newVel, damping, softeningSqr, n).  WORK_GROUP_SIZE_X -> block size,
+        // OUTER_UNROLL_FACTOR -> bodies per thread, INNER_UNROLL_FACTOR1 -> j-loop unroll, WORK_GROUP_SIZE_Y -> CTAs
+        // per cluster splitting the j range; USE_SOA reads the separate arrays (gathered into float4 here);
+        // LOCAL_MEM, VECTOR_TYPE and INNER_UNROLL_FACTOR2 have no counterpart (bodies j always come through
+        // the TMA-staged shared-memory ring, pairs of bodies i always share packed FP32x2 instructions).
+        const int64_t n = static_cast<int64_t>(scalar(14));
+        coul_nbody_tune nb;
+        coul_nbody_tune_default(&nb);
+        nb.block_x = static_cast<int>(parameter("WORK_GROUP_SIZE_X", static_cast<int64_t>(local.GetSizeX())));
+        nb.bodies_per_thread = static_cast<int>(parameter("OUTER_UNROLL_FACTOR", 1));
+        const int64_t u = parameter("INNER_UNROLL_FACTOR1", 0);
+        nb.unroll = u <= 1 ? 1 : (u < 4 ? 2 : 4);
+        const int64_t wy = parameter("WORK_GROUP_SIZE_Y", 1);
+        nb.j_split = wy >= 2 ? static_cast<int>(wy) : 0;
+        const float* pos = vector(1);
+        const float* vel = vector(7);
+
+        if (parameter("USE_SOA", 0) == 1)
+        {
+            float* packed = scratch(static_cast<size_t>(std::max<int64_t>(n, 1)) * 32);
+            float* packedVel = packed + std::max<int64_t>(n, 1) * 4;
+            CheckCoul(coul_pack_atoms(ctx, vector(2), vector(3), vector(4), vector(5), n, packed), "pack of positions");
+            CheckCoul(coul_pack_atoms(ctx, vector(8), vector(9), vector(10), nullptr, n, packedVel), "pack of velocities");
+            pos = packed;
+            vel = packedVel;
+        }
+
+        rc = coul_nbody_step(ctx, pos, vel, n, static_cast<float>(scalar(0)), static_cast<float>(scalar(12)),
+            static_cast<float>(scalar(13)), &nb, vector(6), vector(11));
+    }
+    else if (definition.name == "nbody_kernel_reference" && args.size() == 7)
+    {
+        // Examples/Nbody/NbodyReference.cu:36-44: (dt, pos_old, pos_new, oldVel, newVel, damping, softeningSqr); the
+        // body count is the launch's global size
+        const int64_t n = static_cast<int64_t>(global.GetSizeX() * (GetGlobalSizeType() == GlobalSizeType::CUDA
+            ? local.GetSizeX() : 1));
+        coul_nbody_tune nb;
+        coul_nbody_tune_default(&nb);
+        rc = coul_nbody_step(ctx, vector(1), vector(3), n, static_cast<float>(scalar(0)), static_cast<float>(scalar(5)),
+            static_cast<float>(scalar(6)), &nb, vector(2), vector(4));
     }
     else
     {

@@ -12,7 +12,8 @@ reference computation: ``Examples/CoulombSum3d/CoulombSum3dReference.cu:11-26``,
 into ``liboracle.so``.  Pinning: the FP32 restatement reproduces the output of
 the reference's own generator (compiled from its source by ``make -C oracle
 ref``) bit for bit; the sampled golden vectors of that output are committed in
-``tests/golden/coulomb3d_kat.json``.
+``tests/golden/coulomb3d_kat.json``.  ``nbody_oracle.c`` restates the N-body step of KTT's Nbody
+example (``Examples/Nbody/NbodyReference.cu:36-75``) in FP64.
 """
 from __future__ import annotations
 
@@ -59,7 +60,10 @@ def _load():
     lib.oracle_kat_atoms.argtypes = [ctypes.c_int, _f32p]
     lib.oracle_kat_fp32.argtypes = [_f32p, ctypes.c_int, ctypes.c_float, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                     _f32p]
-    for name in ("oracle_grid3d", "oracle_points3d", "oracle_slice2d", "oracle_adjoint3d", "oracle_loss_perturbed"):
+    lib.oracle_nbody_step.argtypes = [_f32p, _f32p, i64, ctypes.c_float, ctypes.c_float, ctypes.c_float, vp, i64,
+                                      _f64p, _f64p, _f64p]
+    for name in ("oracle_grid3d", "oracle_points3d", "oracle_slice2d", "oracle_adjoint3d", "oracle_loss_perturbed",
+                 "oracle_nbody_step"):
         getattr(lib, name).restype = ctypes.c_int
     _lib = lib
     return lib
@@ -192,3 +196,26 @@ def kat_fp32(atoms, gs: float = 0.49, cells: int = 256, z0: int = 0, z1: int | N
     out = np.empty((z1 - z0) * cells * cells, dtype=np.float32)
     _load().oracle_kat_fp32(a, a.shape[0], np.float32(gs), int(cells), int(z0), z1, out)
     return out.reshape(z1 - z0, cells, cells)
+
+
+def nbody_step(pos_mass, vel, dt: float, damping: float, softening_sqr: float, idx=None):
+    """FP64 N-body step for all bodies or the bodies idx: returns (pos', vel', acc) with shapes
+    (k, 4), (k, 4), (k, 3); the j sum always runs over all bodies."""
+    lib = _load()
+    p = np.ascontiguousarray(np.asarray(pos_mass, dtype=np.float32).reshape(-1, 4))
+    v = np.ascontiguousarray(np.asarray(vel, dtype=np.float32).reshape(-1, 4))
+    n = p.shape[0]
+    if idx is None:
+        sel, ptr, k = None, None, n
+    else:
+        sel = np.ascontiguousarray(np.asarray(idx, dtype=np.int64).reshape(-1))
+        ptr, k = sel.ctypes.data_as(ctypes.c_void_p), sel.shape[0]
+    pos_out = np.empty((k, 4))
+    vel_out = np.empty((k, 4))
+    acc = np.empty((k, 3))
+    rc = lib.oracle_nbody_step(p.reshape(-1), v.reshape(-1), n, np.float32(dt), np.float32(damping),
+                               np.float32(softening_sqr), ptr, k, pos_out.reshape(-1), vel_out.reshape(-1),
+                               acc.reshape(-1))
+    del sel
+    _check(rc, "oracle_nbody_step")
+    return pos_out, vel_out, acc
