@@ -49,6 +49,8 @@ def _function(fname: str, kernel: str):
     if fname not in _modules:
         mod = _check(cu.cuModuleLoad(os.path.join(KDIR, fname).encode()))
         _modules[fname] = mod
+    # kernels that are not extern "C" are looked up by the lowered name recorded at build time
+    kernel = manifest()["kernels"].get(fname, {}).get("function", kernel)
     return _check(cu.cuModuleGetFunction(_modules[fname], kernel.encode()))
 
 
@@ -84,3 +86,50 @@ def run_reference(atoms, n_atoms: int, spacing: float, grid: int, out, stream=No
 def manifest() -> dict:
     with open(os.path.join(KDIR, "manifest.json")) as f:
         return json.load(f)
+
+
+# ---- KTT's N-body example (Examples/Nbody) ----
+
+def nbody_configs():
+    """The compiled sample of the tuned N-body kernel's space (manifest entries), as dicts."""
+    return [dict(v) for k, v in manifest()["kernels"].items() if k.startswith("nbody_") and "reference" not in v]
+
+
+def _nbody_name(cfg):
+    keys = ("WORK_GROUP_SIZE_X", "WORK_GROUP_SIZE_Y", "OUTER_UNROLL_FACTOR", "INNER_UNROLL_FACTOR1",
+            "INNER_UNROLL_FACTOR2", "USE_SOA", "LOCAL_MEM", "USE_CONSTANT_MEMORY", "VECTOR_TYPE")
+    return "nbody_" + "_".join(str(cfg[k]) for k in keys) + ".cubin"
+
+
+def run_nbody_tuned(cfg, dt, pos4, posx, posy, posz, mass, new_pos4, vel4, velx, vely, velz, new_vel4, damping,
+                    eps2, n, stream=None):
+    """One launch of KTT's nbody_kernel (Examples/Nbody/Nbody.cu:260-275) with the example's launch
+    geometry (Examples/Nbody/Nbody.cpp:126-160, OpenCL global size n x 1): grid n / (OUTER_UNROLL_FACTOR *
+    WORK_GROUP_SIZE_X), block (WORK_GROUP_SIZE_X, WORK_GROUP_SIZE_Y).  n must be a multiple of
+    WORK_GROUP_SIZE_X * OUTER_UNROLL_FACTOR and of WORK_GROUP_SIZE_X * VECTOR_TYPE."""
+    import torch
+    from cuda.bindings import driver as cu
+    wx, wy, ouf, vt = cfg["WORK_GROUP_SIZE_X"], cfg["WORK_GROUP_SIZE_Y"], cfg["OUTER_UNROLL_FACTOR"], cfg["VECTOR_TYPE"]
+    if n % (wx * ouf) or n % (wx * vt):
+        raise ValueError("body count not divisible by the configuration's tile")
+    fn = _function(_nbody_name(cfg), "nbody_kernel")
+    s = stream or torch.cuda.current_stream()
+    ptrs = [pos4, posx, posy, posz, mass, new_pos4, vel4, velx, vely, velz, new_vel4]
+    args = ((float(dt), *(t.data_ptr() for t in ptrs), float(damping), float(eps2), int(n)),
+            (ctypes.c_float,) + (ctypes.c_void_p,) * 11 + (ctypes.c_float, ctypes.c_float, ctypes.c_int))
+    _check(cu.cuLaunchKernel(fn, n // (wx * ouf), 1, 1, wx, wy, 1, 0, cu.CUstream(s.cuda_stream), args, 0))
+
+
+def run_nbody_reference(dt, pos4, new_pos4, vel4, new_vel4, damping, eps2, n, stream=None):
+    """One launch of nbody_kernel_reference (Examples/Nbody/NbodyReference.cu:36-75) with the example's
+    64-thread blocks; n must be a multiple of 64."""
+    import torch
+    from cuda.bindings import driver as cu
+    if n % 64:
+        raise ValueError("the reference N-body kernel needs a multiple of 64 bodies")
+    fn = _function("nbody_reference.cubin", "nbody_kernel_reference")
+    s = stream or torch.cuda.current_stream()
+    args = ((float(dt), pos4.data_ptr(), new_pos4.data_ptr(), vel4.data_ptr(), new_vel4.data_ptr(), float(damping),
+             float(eps2)),
+            (ctypes.c_float,) + (ctypes.c_void_p,) * 4 + (ctypes.c_float, ctypes.c_float))
+    _check(cu.cuLaunchKernel(fn, n // 64, 1, 1, 64, 1, 1, 0, cu.CUstream(s.cuda_stream), args, 0))

@@ -136,3 +136,84 @@ def test_time_ktt_space_on_the_full_map(ctx):
     with open(os.environ["KTT_REF_SWEEP_OUT"], "w") as f:
         json.dump(result, f, indent=1)
     assert best["ms"] > 0
+
+
+# ---- KTT's N-body example ----
+
+def _nbody_inputs(n, seed=11):
+    import torch
+    rng = np.random.default_rng(seed)
+    pos = rng.uniform(0.0, 20.0, (n, 4)).astype(np.float32)
+    vel = rng.uniform(0.0, 20.0, (n, 4)).astype(np.float32)
+    vel[:, 3] = 0.0
+    t = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in
+         dict(pos=pos, vel=vel, px=pos[:, 0], py=pos[:, 1], pz=pos[:, 2], m=pos[:, 3], vx=vel[:, 0], vy=vel[:, 1],
+              vz=vel[:, 2]).items()}
+    return pos, vel, t
+
+
+def _run_ktt_nbody(cfg, t, n, new_pos, new_vel):
+    ref_kernels.run_nbody_tuned(cfg, 0.001, t["pos"], t["px"], t["py"], t["pz"], t["m"], new_pos, t["vel"], t["vx"],
+                                t["vy"], t["vz"], new_vel, 0.5, 0.01, n)
+
+
+def test_ktt_nbody_kernels_match_this_library(ctx):
+    """KTT's N-body reference kernel and 24 seeded configurations of its tuned kernel on 8,192 bodies,
+    against this library's step (positions and velocities within 1e-5 of their magnitude)."""
+    import torch
+    n = 8192
+    pos, vel, t = _nbody_inputs(n)
+    ours_p, ours_v = ktt_b200.nbody_step(ctx, t["pos"], t["vel"], 0.001, 0.5, 0.01)
+    torch.cuda.synchronize()
+    sp, sv = float(ours_p.abs().max()), float(ours_v.abs().max())
+    new_p, new_v = torch.empty_like(t["pos"]), torch.empty_like(t["vel"])
+    ref_kernels.run_nbody_reference(0.001, t["pos"], new_p, t["vel"], new_v, 0.5, 0.01, n)
+    torch.cuda.synchronize()
+    assert float((new_p - ours_p).abs().max()) <= 1e-5 * sp
+    assert float((new_v - ours_v).abs().max()) <= 1e-5 * sv
+    configs = ref_kernels.nbody_configs()
+    rng = np.random.default_rng(7)
+    bad = []
+    for k in rng.choice(len(configs), 24, replace=False):
+        cfg = configs[int(k)]
+        new_p.zero_()
+        new_v.zero_()
+        _run_ktt_nbody(cfg, t, n, new_p, new_v)
+        torch.cuda.synchronize()
+        dp = float((new_p - ours_p).abs().max()) / sp
+        dv = float((new_v[:, :3] - ours_v[:, :3]).abs().max()) / sv
+        if dp > 1e-5 or dv > 1e-5:
+            bad.append((cfg, dp, dv))
+    assert not bad, bad[:3]
+
+
+@pytest.mark.skipif(not os.environ.get("KTT_REF_NBODY_SWEEP_OUT"), reason="timing sweep is opt-in")
+def test_time_ktt_nbody_space():
+    """Device time of the compiled sample of KTT's tuned N-body kernel space and of its reference
+    kernel on the example's 131,072 bodies (one warm-up, best of two timed launches each)."""
+    import torch
+    n = 128 * 1024
+    _, _, t = _nbody_inputs(n)
+    new_p, new_v = torch.empty_like(t["pos"]), torch.empty_like(t["vel"])
+
+    def timed(fn):
+        times = []
+        for rep in range(3):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            b.synchronize()
+            if rep:
+                times.append(a.elapsed_time(b))
+        return min(times)
+
+    rows = []
+    for cfg in ref_kernels.nbody_configs():
+        ms = timed(lambda: _run_ktt_nbody(cfg, t, n, new_p, new_v))
+        rows.append({**{k: v for k, v in cfg.items() if k != "function"}, "ms": ms,
+                     "ginteractions_per_s": n * n / (ms * 1e-3) / 1e9})
+    ref_ms = timed(lambda: ref_kernels.run_nbody_reference(0.001, t["pos"], new_p, t["vel"], new_v, 0.5, 0.01, n))
+    with open(os.environ["KTT_REF_NBODY_SWEEP_OUT"], "w") as f:
+        json.dump({"n": n, "configurations": rows, "best": min(rows, key=lambda r: r["ms"]),
+                   "reference_kernel_ms": ref_ms}, f, indent=1)
