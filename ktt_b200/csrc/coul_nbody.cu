@@ -7,12 +7,14 @@
 // The pair is the Coulomb pair with a softening term and a vector accumulator: one MUFU rsqrt and
 // 12 FP32 operations (3 differences, 3 FMAs for r^2 + eps^2, 1/r^2, m/r, m/r^3, 3 FMAs into a).
 // The FP32 pipe bounds it (F / 12 pairs/s), so all rsqrts stay on MUFU and the FP32 work runs as
-// packed FFMA2/FMUL2/FADD2 on two bodies i per instruction.
+// packed FFMA2/FMUL2/FADD2 on two bodies j per instruction.
 //
-// Layout: each thread owns `BP` bodies i (strided by the block size so loads and stores coalesce),
-// held in registers as BP/2 lane pairs; the bodies j stream through the CTA's TMA ring of 256-body
-// float4 stages (the forward kernel's ring: one elected thread issues cp.async.bulk, mbarrier
-// expect-tx, bounded waits) and are read as shared-memory broadcasts.  With j_split = S >= 2 a
+// Layout: each thread owns `BP` bodies i (strided by the block size so loads and stores coalesce) in
+// registers; the bodies j stream through the CTA's TMA ring of 256-body float4 stages (the forward
+// kernel's ring: one elected thread issues cp.async.bulk, mbarrier expect-tx, bounded waits), each
+// stage is transposed once into x/y/z/m arrays, and every thread reads the bodies (j, j + 1) as
+// 8-byte shared-memory broadcasts that meet a body i, held as a splat pair, in one packed
+// instruction -- so no per-pair register moves are needed to form the packed operands.  With j_split = S >= 2 a
 // thread-block cluster of S CTAs shares one tile of bodies i, each CTA taking 1/S of the bodies j,
 // and rank 0 adds the partial accelerations from the peers' shared memory in rank order before it
 // integrates and stores (for body counts too small to fill 148 SMs one tile per CTA).
@@ -38,15 +40,22 @@ struct NbodyParams {
 
 constexpr int kNbodyMaxThreads = 512;
 constexpr int kNbodyMaxSplit = 8;
+// dynamic shared memory: the TMA ring, its barriers, the transposed stage, the split's partial sums
+constexpr int kNbodySoaOffset = kStages * kTileAtoms * 16 + 16;
+constexpr int kNbodyRedOffset = kNbodySoaOffset + kTileAtoms * 16;
+static_assert(kStages * 8 <= 16 && kNbodySoaOffset % 16 == 0, "ring barriers fit before the transposed stage");
+
+// the widest register blocks (8 bodies i, each with three splat positions and three pair accumulators)
+// need more than the 128 registers a 512-thread block leaves per thread
+constexpr int nbody_max_threads(int bp) { return bp >= 8 ? 256 : kNbodyMaxThreads; }
 
 template <int BP, int UNR, bool SPLIT>
-__global__ void __launch_bounds__(kNbodyMaxThreads) nbody_kernel(const NbodyParams p)
+__global__ void __launch_bounds__(nbody_max_threads(BP), 1) nbody_kernel(const NbodyParams p)
 {
-    static_assert(BP == 1 || BP % 2 == 0, "bodies per thread: 1 or lane pairs");
-    constexpr int P = (BP + 1) / 2;  // with BP == 1 the second lane of the pair is idle (never stored)
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    unsigned char* tiles = smem_raw;
+    unsigned char* tiles = smem_raw;  // TMA ring of float4 (x, y, z, m) stages
     uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + kStages * kTileAtoms * 16);
+    float* soa = reinterpret_cast<float*>(smem_raw + kNbodySoaOffset);  // x[256] y[256] z[256] m[256]
     const int tid = threadIdx.x;
     const int nthreads = blockDim.x;
 
@@ -58,24 +67,19 @@ __global__ void __launch_bounds__(kNbodyMaxThreads) nbody_kernel(const NbodyPara
         tile = static_cast<int>(blockIdx.x / S);
     }
 
-    // bodies i of this thread: tile * (nthreads * BP) + tid + k * nthreads
+    // bodies i of this thread: tile * (nthreads * BP) + tid + k * nthreads, each held as a splat pair
+    // (-x_i, -x_i) that meets the bodies (j, j + 1) in one packed instruction; the accumulators keep
+    // the even-j and odd-j partial sums in their two lanes
     const int64_t ibase = static_cast<int64_t>(tile) * nthreads * BP + tid;
-    float2 nx[P], ny[P], nz[P], ax[P], ay[P], az[P];
+    float2 nx[BP], ny[BP], nz[BP], ax[BP], ay[BP], az[BP];
 #pragma unroll
-    for (int m = 0; m < P; ++m) {
-        float c[2][3];
-#pragma unroll
-        for (int l = 0; l < 2; ++l) {
-            const int64_t i = ibase + static_cast<int64_t>(2 * m + l) * nthreads;
-            const float4 b = (2 * m + l < BP && i < p.n) ? p.pos[i] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            c[l][0] = -b.x;
-            c[l][1] = -b.y;
-            c[l][2] = -b.z;
-        }
-        nx[m] = make_float2(c[0][0], c[1][0]);
-        ny[m] = make_float2(c[0][1], c[1][1]);
-        nz[m] = make_float2(c[0][2], c[1][2]);
-        ax[m] = ay[m] = az[m] = make_float2(0.0f, 0.0f);
+    for (int k = 0; k < BP; ++k) {
+        const int64_t i = ibase + static_cast<int64_t>(k) * nthreads;
+        const float4 b = i < p.n ? p.pos[i] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        nx[k] = splat(-b.x);
+        ny[k] = splat(-b.y);
+        nz[k] = splat(-b.z);
+        ax[k] = ay[k] = az[k] = make_float2(0.0f, 0.0f);
     }
     const float2 eps2 = splat(p.eps2);
 
@@ -114,13 +118,6 @@ __global__ void __launch_bounds__(kNbodyMaxThreads) nbody_kernel(const NbodyPara
         const int buf = static_cast<int>(s % kStages);
         const uint32_t parity = static_cast<uint32_t>((s / kStages) & 1);
         const bool arrived = mbar_wait_bounded(&full[buf], parity);
-        const int cnt = stage_count(s);
-        float4* tile4 = reinterpret_cast<float4*>(tiles + buf * kTileAtoms * 16);
-        if (arrived && cnt < kTileAtoms) {
-            // ragged last stage: far-away massless bodies, so the unrolled loop needs no bound
-            for (int j = cnt + tid; j < kTileAtoms; j += nthreads)
-                tile4[j] = make_float4(kPadCoord, kPadCoord, kPadCoord, 0.0f);
-        }
         if (__syncthreads_or(arrived ? 0 : 1)) {
             if (tid == 0) {
                 report_status(p.status, kStatusTimeout);
@@ -130,52 +127,70 @@ __global__ void __launch_bounds__(kNbodyMaxThreads) nbody_kernel(const NbodyPara
             ok = false;
             break;
         }
-#pragma unroll UNR
-        for (int j = 0; j < kTileAtoms; ++j) {
-            const float4 b = tile4[j];
-            const float2 bx = splat(b.x), by = splat(b.y), bz = splat(b.z), bm = splat(b.w);
-#pragma unroll
-            for (int m = 0; m < P; ++m) {
-                const float2 dx = __fadd2_rn(bx, nx[m]);
-                const float2 dy = __fadd2_rn(by, ny[m]);
-                const float2 dz = __fadd2_rn(bz, nz[m]);
-                const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, eps2)));
-                const float2 inv = make_float2(rsqrt_mufu(r2.x), rsqrt_mufu(r2.y));
-                const float2 f = __fmul2_rn(__fmul2_rn(bm, inv), __fmul2_rn(inv, inv));
-                ax[m] = __ffma2_rn(dx, f, ax[m]);
-                ay[m] = __ffma2_rn(dy, f, ay[m]);
-                az[m] = __ffma2_rn(dz, f, az[m]);
-            }
+        // Transpose the stage into four arrays (so a pair of bodies j is one 8-byte broadcast load);
+        // the ragged last stage is padded with far-away massless bodies, so the loop needs no bound.
+        const int cnt = stage_count(s);
+        const float4* tile4 = reinterpret_cast<const float4*>(tiles + buf * kTileAtoms * 16);
+        for (int j = tid; j < kTileAtoms; j += nthreads) {
+            const float4 b = j < cnt ? tile4[j] : make_float4(kPadCoord, kPadCoord, kPadCoord, 0.0f);
+            soa[0 * kTileAtoms + j] = b.x;
+            soa[1 * kTileAtoms + j] = b.y;
+            soa[2 * kTileAtoms + j] = b.z;
+            soa[3 * kTileAtoms + j] = b.w;
         }
+        // the TMA stage is free again: order the reads before its refill, which overlaps the math
         fence_proxy_async_smem();
         __syncthreads();
         if (tid == 0 && s + kStages < nst)
             issue(s + kStages);
+        const float2* sx = reinterpret_cast<const float2*>(soa);
+        const float2* sy = reinterpret_cast<const float2*>(soa + kTileAtoms);
+        const float2* sz = reinterpret_cast<const float2*>(soa + 2 * kTileAtoms);
+        const float2* sm = reinterpret_cast<const float2*>(soa + 3 * kTileAtoms);
+#pragma unroll UNR
+        for (int j = 0; j < kTileAtoms / 2; ++j) {
+            const float2 bx = sx[j], by = sy[j], bz = sz[j], bm = sm[j];
+#pragma unroll
+            for (int k = 0; k < BP; ++k) {
+                const float2 dx = __fadd2_rn(bx, nx[k]);
+                const float2 dy = __fadd2_rn(by, ny[k]);
+                const float2 dz = __fadd2_rn(bz, nz[k]);
+                const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, eps2)));
+                const float2 inv = make_float2(rsqrt_mufu(r2.x), rsqrt_mufu(r2.y));
+                const float2 f = __fmul2_rn(__fmul2_rn(bm, inv), __fmul2_rn(inv, inv));
+                ax[k] = __ffma2_rn(dx, f, ax[k]);
+                ay[k] = __ffma2_rn(dy, f, ay[k]);
+                az[k] = __ffma2_rn(dz, f, az[k]);
+            }
+        }
+        __syncthreads();  // the four arrays are rewritten by the next stage
+    }
+
+    float a[BP][3];
+#pragma unroll
+    for (int k = 0; k < BP; ++k) {
+        a[k][0] = ax[k].x + ax[k].y;
+        a[k][1] = ay[k].x + ay[k].y;
+        a[k][2] = az[k].x + az[k].y;
     }
 
     if constexpr (SPLIT) {
         // partial accelerations of the cluster, added by rank 0 in rank order
-        float* red = reinterpret_cast<float*>(smem_raw + kStages * kTileAtoms * 16 + kStages * 8);
+        float* red = reinterpret_cast<float*>(smem_raw + kNbodyRedOffset);
 #pragma unroll
-        for (int m = 0; m < P; ++m) {
-            red[(6 * m + 0) * nthreads + tid] = ax[m].x;
-            red[(6 * m + 1) * nthreads + tid] = ax[m].y;
-            red[(6 * m + 2) * nthreads + tid] = ay[m].x;
-            red[(6 * m + 3) * nthreads + tid] = ay[m].y;
-            red[(6 * m + 4) * nthreads + tid] = az[m].x;
-            red[(6 * m + 5) * nthreads + tid] = az[m].y;
-        }
+        for (int k = 0; k < BP; ++k)
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+                red[(3 * k + c) * nthreads + tid] = a[k][c];
         cluster_sync();
         if (rank == 0) {
             for (uint32_t peer = 1; peer < S; ++peer) {
                 const uint32_t base = cluster_map(red, peer);
 #pragma unroll
-                for (int m = 0; m < P; ++m) {
-                    auto at = [&](int c) { return ld_cluster_f32(base + 4u * static_cast<uint32_t>((6 * m + c) * nthreads + tid)); };
-                    ax[m] = __fadd2_rn(ax[m], make_float2(at(0), at(1)));
-                    ay[m] = __fadd2_rn(ay[m], make_float2(at(2), at(3)));
-                    az[m] = __fadd2_rn(az[m], make_float2(at(4), at(5)));
-                }
+                for (int k = 0; k < BP; ++k)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c)
+                        a[k][c] += ld_cluster_f32(base + 4u * static_cast<uint32_t>((3 * k + c) * nthreads + tid));
             }
         }
         cluster_sync();  // the peers' shared memory stays valid until rank 0 has read it
@@ -188,21 +203,15 @@ __global__ void __launch_bounds__(kNbodyMaxThreads) nbody_kernel(const NbodyPara
     const float dt = p.dt;
     const float half = p.damping * dt * dt;
 #pragma unroll
-    for (int m = 0; m < P; ++m) {
-#pragma unroll
-        for (int l = 0; l < 2; ++l) {
-            const int64_t i = ibase + static_cast<int64_t>(2 * m + l) * nthreads;
-            if (2 * m + l >= BP || i >= p.n)
-                continue;
-            const float4 b = p.pos[i];
-            const float4 v = p.vel[i];
-            const float a0 = l ? ax[m].y : ax[m].x;
-            const float a1 = l ? ay[m].y : ay[m].x;
-            const float a2 = l ? az[m].y : az[m].x;
-            p.pos_new[i] = make_float4(fmaf(half, a0, fmaf(dt, v.x, b.x)), fmaf(half, a1, fmaf(dt, v.y, b.y)),
-                                       fmaf(half, a2, fmaf(dt, v.z, b.z)), b.w);
-            p.vel_new[i] = make_float4(fmaf(dt, a0, v.x), fmaf(dt, a1, v.y), fmaf(dt, a2, v.z), 0.0f);
-        }
+    for (int k = 0; k < BP; ++k) {
+        const int64_t i = ibase + static_cast<int64_t>(k) * nthreads;
+        if (i >= p.n)
+            continue;
+        const float4 b = p.pos[i];
+        const float4 v = p.vel[i];
+        p.pos_new[i] = make_float4(fmaf(half, a[k][0], fmaf(dt, v.x, b.x)), fmaf(half, a[k][1], fmaf(dt, v.y, b.y)),
+                                   fmaf(half, a[k][2], fmaf(dt, v.z, b.z)), b.w);
+        p.vel_new[i] = make_float4(fmaf(dt, a[k][0], v.x), fmaf(dt, a[k][1], v.y), fmaf(dt, a[k][2], v.z), 0.0f);
     }
 }
 
@@ -275,6 +284,8 @@ int find_nbody(const coul_nbody_tune* t, const NbodyVariant** out)
                                                      std::to_string(kNbodyMaxThreads));
     if (t->j_split < 0 || t->j_split > kNbodyMaxSplit)
         return set_error(COUL_ERR_INVALID_ARGUMENT, "j_split must be in 0.." + std::to_string(kNbodyMaxSplit));
+    if (t->block_x > nbody_max_threads(t->bodies_per_thread))
+        return set_error(COUL_ERR_DEVICE_LIMITS, "8 bodies per thread allow at most 256 threads per block");
     const int unroll = t->unroll <= 1 ? 1 : t->unroll;
     const bool split = t->j_split >= 2;
     for (const auto& e : nbody_variants()) {
@@ -344,9 +355,9 @@ COUL_API int coul_nbody_step(coul_ctx* ctx, const float* d_pos_mass, const float
     const int split = tune->j_split >= 2 ? tune->j_split : 1;
     if (tiles * split > 2147483647LL)
         return set_error(COUL_ERR_DEVICE_LIMITS, "too many bodies for one launch");
-    size_t smem = static_cast<size_t>(kStages) * kTileAtoms * 16 + kStages * 8;
+    size_t smem = kNbodyRedOffset;
     if (split > 1)
-        smem += static_cast<size_t>(tune->block_x) * 6 * ((tune->bodies_per_thread + 1) / 2) * sizeof(float);
+        smem += static_cast<size_t>(tune->block_x) * 3 * tune->bodies_per_thread * sizeof(float);
     if ((rc = ctx_begin_timing(ctx)))
         return rc;
     cudaError_t e = v->launch(p, dim3(static_cast<unsigned>(tiles)), dim3(static_cast<unsigned>(tune->block_x)), smem, split,

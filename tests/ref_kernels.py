@@ -90,6 +90,9 @@ def manifest() -> dict:
 
 # ---- KTT's N-body example (Examples/Nbody) ----
 
+class DeviceLimitsExceeded(Exception):
+    """The configuration cannot be launched on this device (KTT's ResultStatus::DeviceLimitsExceeded)."""
+
 def nbody_configs():
     """The compiled sample of the tuned N-body kernel's space (manifest entries), as dicts."""
     return [dict(v) for k, v in manifest()["kernels"].items() if k.startswith("nbody_") and "reference" not in v]
@@ -113,6 +116,11 @@ def run_nbody_tuned(cfg, dt, pos4, posx, posy, posz, mass, new_pos4, vel4, velx,
     if n % (wx * ouf) or n % (wx * vt):
         raise ValueError("body count not divisible by the configuration's tile")
     fn = _function(_nbody_name(cfg), "nbody_kernel")
+    # a block beyond what the compiled kernel's registers allow is KTT's DeviceLimitsExceeded: refuse it
+    # before launching rather than let the launch fail
+    limit = _check(cu.cuFuncGetAttribute(cu.CUfunction_attribute.CU_FUNC_ATTRIBUTE_MAX_THREADS_PER_BLOCK, fn))
+    if wx * wy > limit:
+        raise DeviceLimitsExceeded(f"{wx * wy} threads per block, the kernel allows {limit}")
     s = stream or torch.cuda.current_stream()
     ptrs = [pos4, posx, posy, posz, mass, new_pos4, vel4, velx, vely, velz, new_vel4]
     args = ((float(dt), *(t.data_ptr() for t in ptrs), float(damping), float(eps2), int(n)),
