@@ -282,8 +282,10 @@ int find_nbody(const coul_nbody_tune* t, const NbodyVariant** out)
     if (t->block_x < 32 || t->block_x > kNbodyMaxThreads || t->block_x % 32 != 0)
         return set_error(COUL_ERR_DEVICE_LIMITS, "N-body block size must be a multiple of 32 in 32.." +
                                                      std::to_string(kNbodyMaxThreads));
-    if (t->j_split < 0 || t->j_split > kNbodyMaxSplit)
-        return set_error(COUL_ERR_INVALID_ARGUMENT, "j_split must be in 0.." + std::to_string(kNbodyMaxSplit));
+    if (t->j_split < 0)
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "j_split must not be negative");
+    if (t->j_split > kNbodyMaxSplit)  // beyond the portable cluster size: no compiled form
+        return set_error(COUL_ERR_UNSUPPORTED, "j_split above " + std::to_string(kNbodyMaxSplit) + " is not supported");
     if (t->block_x > nbody_max_threads(t->bodies_per_thread))
         return set_error(COUL_ERR_DEVICE_LIMITS, "8 bodies per thread allow at most 256 threads per block");
     const int unroll = t->unroll <= 1 ? 1 : t->unroll;

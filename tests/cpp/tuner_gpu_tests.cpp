@@ -466,6 +466,114 @@ void TestUserDeviceBuffers()
     coul_ctx_destroy(ctx);
 }
 
+// KTT's Nbody example (Examples/Nbody/Nbody.cpp:62-240) on 16,384 bodies: its parameters, thread
+// modifiers, constraints and argument lists, the tuned kernel validated against the reference
+// kernel (SideBySide 0.001) over a random sample of the space; configurations with no compiled
+// counterpart end as CompilationFailed / DeviceLimitsExceeded, the rest must validate.
+void TestNbodyExample()
+{
+    const int n = 16 * 1024;
+    std::mt19937 engine(42);
+    std::uniform_real_distribution<float> dist(0.0f, 20.0f);
+    std::vector<float> info(4 * n), px(n), py(n), pz(n), mass(n), newInfo(4 * n, 0.0f);
+    std::vector<float> vel(4 * n), vx(n), vy(n), vz(n), newVel(4 * n, 0.0f);
+
+    for (int i = 0; i < n; ++i)
+    {
+        px[i] = dist(engine);
+        py[i] = dist(engine);
+        pz[i] = dist(engine);
+        mass[i] = dist(engine);
+        vx[i] = dist(engine);
+        vy[i] = dist(engine);
+        vz[i] = dist(engine);
+        info[4 * i] = px[i];
+        info[4 * i + 1] = py[i];
+        info[4 * i + 2] = pz[i];
+        info[4 * i + 3] = mass[i];
+        vel[4 * i] = vx[i];
+        vel[4 * i + 1] = vy[i];
+        vel[4 * i + 2] = vz[i];
+        vel[4 * i + 3] = 0.0f;
+    }
+
+    ktt::Tuner tuner(0, 0, ktt::ComputeApi::CUDA);
+    tuner.SetGlobalSizeType(ktt::GlobalSizeType::OpenCL);
+    tuner.SetCompilerOptions("-use_fast_math");
+    const auto definition = tuner.AddKernelDefinitionFromFile("nbody_kernel", "Nbody.cu", ktt::DimensionVector(n, 1),
+        ktt::DimensionVector(1, 1));
+    const auto referenceDefinition = tuner.AddKernelDefinitionFromFile("nbody_kernel_reference", "NbodyReference.cu",
+        ktt::DimensionVector(n, 1), ktt::DimensionVector(64));
+    const auto kernel = tuner.CreateSimpleKernel("Nbody", definition);
+    const auto referenceKernel = tuner.CreateSimpleKernel("NbodyReference", referenceDefinition);
+
+    tuner.AddParameter(kernel, "WORK_GROUP_SIZE_X", std::vector<uint64_t>{16, 32, 64, 128, 256, 512});
+    tuner.AddThreadModifier(kernel, {definition}, ktt::ModifierType::Local, ktt::ModifierDimension::X, "WORK_GROUP_SIZE_X",
+        ktt::ModifierAction::Multiply);
+    tuner.AddParameter(kernel, "WORK_GROUP_SIZE_Y", std::vector<uint64_t>{1, 2, 4, 8, 16});
+    tuner.AddThreadModifier(kernel, {definition}, ktt::ModifierType::Local, ktt::ModifierDimension::Y, "WORK_GROUP_SIZE_Y",
+        ktt::ModifierAction::Multiply);
+    tuner.AddThreadModifier(kernel, {definition}, ktt::ModifierType::Global, ktt::ModifierDimension::Y, "WORK_GROUP_SIZE_Y",
+        ktt::ModifierAction::Multiply);
+    tuner.AddParameter(kernel, "OUTER_UNROLL_FACTOR", std::vector<uint64_t>{1, 2, 4, 8});
+    tuner.AddThreadModifier(kernel, {definition}, ktt::ModifierType::Global, ktt::ModifierDimension::X, "OUTER_UNROLL_FACTOR",
+        ktt::ModifierAction::Divide);
+    tuner.AddParameter(kernel, "INNER_UNROLL_FACTOR1", std::vector<uint64_t>{0, 1, 2, 4, 8, 16, 32});
+    tuner.AddParameter(kernel, "INNER_UNROLL_FACTOR2", std::vector<uint64_t>{0, 1, 2, 4, 8, 16, 32});
+    tuner.AddParameter(kernel, "USE_SOA", std::vector<uint64_t>{0, 1});
+    tuner.AddParameter(kernel, "LOCAL_MEM", std::vector<uint64_t>{0, 1});
+    tuner.AddParameter(kernel, "USE_CONSTANT_MEMORY", std::vector<uint64_t>{0});
+    tuner.AddParameter(kernel, "VECTOR_TYPE", std::vector<uint64_t>{1, 2, 4});
+
+    const auto infoId = tuner.AddArgumentVector(info, ktt::ArgumentAccessType::ReadOnly);
+    const auto pxId = tuner.AddArgumentVector(px, ktt::ArgumentAccessType::ReadOnly);
+    const auto pyId = tuner.AddArgumentVector(py, ktt::ArgumentAccessType::ReadOnly);
+    const auto pzId = tuner.AddArgumentVector(pz, ktt::ArgumentAccessType::ReadOnly);
+    const auto massId = tuner.AddArgumentVector(mass, ktt::ArgumentAccessType::ReadOnly);
+    const auto newInfoId = tuner.AddArgumentVector(newInfo, ktt::ArgumentAccessType::WriteOnly);
+    const auto velId = tuner.AddArgumentVector(vel, ktt::ArgumentAccessType::ReadOnly);
+    const auto vxId = tuner.AddArgumentVector(vx, ktt::ArgumentAccessType::ReadOnly);
+    const auto vyId = tuner.AddArgumentVector(vy, ktt::ArgumentAccessType::ReadOnly);
+    const auto vzId = tuner.AddArgumentVector(vz, ktt::ArgumentAccessType::ReadOnly);
+    const auto newVelId = tuner.AddArgumentVector(newVel, ktt::ArgumentAccessType::WriteOnly);
+    const auto dtId = tuner.AddArgumentScalar(0.001f);
+    const auto dampingId = tuner.AddArgumentScalar(0.5f);
+    const auto epsId = tuner.AddArgumentScalar(0.1f * 0.1f);
+    const auto nId = tuner.AddArgumentScalar(n);
+
+    tuner.AddConstraint(kernel, {"INNER_UNROLL_FACTOR2", "OUTER_UNROLL_FACTOR"},
+        [](const std::vector<uint64_t>& v) { return v.at(0) <= v.at(1); });
+    tuner.AddConstraint(kernel, {"INNER_UNROLL_FACTOR1", "INNER_UNROLL_FACTOR2"},
+        [](const std::vector<uint64_t>& v) { return v.at(0) * v.at(1) <= 256; });
+    tuner.AddConstraint(kernel, {"VECTOR_TYPE", "USE_SOA"},
+        [](const std::vector<uint64_t>& v) { return (v.at(0) == 1 && v.at(1) == 0) || v.at(1) == 1; });
+    tuner.AddConstraint(kernel, {"WORK_GROUP_SIZE_X", "WORK_GROUP_SIZE_Y"},
+        [](const std::vector<uint64_t>& v) { return v.at(0) * v.at(1) >= 64 && v.at(0) * v.at(1) <= 1024; });
+
+    tuner.SetArguments(definition, {dtId, infoId, pxId, pyId, pzId, massId, newInfoId, velId, vxId, vyId, vzId, newVelId,
+        dampingId, epsId, nId});
+    tuner.SetArguments(referenceDefinition, {dtId, infoId, newInfoId, velId, newVelId, dampingId, epsId});
+    tuner.SetValidationMethod(ktt::ValidationMethod::SideBySideComparison, 0.001);
+    tuner.SetReferenceKernel(newVelId, referenceKernel, ktt::KernelConfiguration());
+    tuner.SetReferenceKernel(newInfoId, referenceKernel, ktt::KernelConfiguration());
+    tuner.SetSearcher(kernel, std::make_unique<ktt::RandomSearcher>());
+
+    const auto results = tuner.Tune(kernel, std::make_unique<ktt::ConfigurationCount>(40));
+    CHECK(results.size() == 40);
+    int ok = 0;
+
+    for (const auto& r : results)
+    {
+        const auto s = r.GetStatus();
+        CHECK(s == ktt::ResultStatus::Ok || s == ktt::ResultStatus::CompilationFailed
+            || s == ktt::ResultStatus::DeviceLimitsExceeded);
+        ok += s == ktt::ResultStatus::Ok ? 1 : 0;
+    }
+
+    CHECK(ok >= 10);
+    std::cout << "nbody: " << ok << " of " << results.size() << " configurations validated" << std::endl;
+}
+
 } // namespace
 
 int main(int argc, char** argv)
@@ -484,6 +592,7 @@ int main(int argc, char** argv)
         {"coulomb2d_random", TestCoulomb2dRandomSearch},
         {"iterative_launcher", TestIterativeLauncher},
         {"user_buffers", TestUserDeviceBuffers},
+        {"nbody_example", TestNbodyExample},
     };
     const auto it = tests.find(argv[1]);
 

@@ -24,7 +24,7 @@ def gpu_tests_binary(tmp_path_factory):
 
 
 @pytest.mark.parametrize("name", ["coulomb3d_tune", "coulomb3d_reference_computation", "coulomb2d_random",
-                                  "iterative_launcher", "user_buffers"])
+                                  "iterative_launcher", "user_buffers", "nbody_example"])
 def test_tuner_gpu(gpu_tests_binary, workdir, name):  # noqa: F811
     r = subprocess.run([gpu_tests_binary, name, workdir], capture_output=True, text=True, timeout=900)
     assert r.returncode == 0, r.stdout[-4000:] + r.stderr[-4000:]
