@@ -1,6 +1,6 @@
 """Measure the N-body step (coul_nbody_step) over its configuration space.
 
-    python -m ktt_b200.run_nbody [--n 131072] [--repeat 5]
+    python -m ktt_b200.run_nbody [--n 131072] [--repeat 5] [--only BX,BP,UN,JS]
 
 Bodies as in KTT's Nbody example (positions, masses, velocities uniform in [0, 20); dt 0.001,
 damping 0.5, softening 0.1^2; 131,072 bodies by default, Examples/Nbody/Nbody.cpp:62-118).  For every
@@ -23,7 +23,10 @@ def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--n", type=int, default=128 * 1024)
     ap.add_argument("--repeat", type=int, default=5)
+    ap.add_argument("--only", default="", metavar="BX,BP,UN,JS",
+                    help="run one configuration (block_x, bodies_per_thread, unroll, j_split), e.g. for a profiler")
     args = ap.parse_args()
+    configs = [tuple(int(v) for v in args.only.split(","))] if args.only else CONFIGS
 
     import torch
 
@@ -40,7 +43,7 @@ def main() -> None:
     bound = ffma_rate / 12.0
     interactions = float(args.n) * args.n
     rows = []
-    for bx, bp, un, js in CONFIGS:
+    for bx, bp, un, js in configs:
         tune = ktt_b200.NbodyTune(block_x=bx, bodies_per_thread=bp, unroll=un, j_split=js)
         if not ktt_b200.nbody_tune_supported(tune):
             continue
