@@ -274,6 +274,9 @@ enum {
     COUL_BATCH_SEPARATE = 2    /* baseline: one plain forward launch per molecule */
 };
 
+/* Whether a persistent batched variant is compiled for this tile shape (the batch's counterpart of
+   coul_tune_supported). */
+COUL_API int coul_batch_tune_supported(const coul_tune* tune);
 /* tune selects the tile shape (z_iterations, x_points, unroll, precision, rsqrt_soft, block). */
 COUL_API int coul_batch_create(coul_ctx* ctx, const coul_molecule* molecules, int n_molecules, const coul_tune* tune,
                                coul_batch** batch);

@@ -116,6 +116,7 @@ def load_library():
         "coul_elapsed_ms": [vp, ctypes.POINTER(ctypes.c_double)],
         "coul_tune_supported": [T],
         "coul_tune_supported_2d": [T],
+        "coul_batch_tune_supported": [T],
         "coul_variant_count": [],
         "coul_variant_get": [ci, T, ctypes.POINTER(ci), ctypes.POINTER(ci)],
         "coul_forward_3d": [vp, vp, i64, G, T, ci, vp],
@@ -175,6 +176,11 @@ def variants() -> list[tuple[Tune, bool, bool]]:
 def tune_supported(tune: Tune) -> bool:
     lib = load_library()
     return lib.coul_tune_supported(ctypes.byref(tune.c())) == COUL_OK
+
+
+def batch_tune_supported(tune: Tune) -> bool:
+    """Whether the persistent batched kernel has a compiled variant for this tile shape."""
+    return load_library().coul_batch_tune_supported(ctypes.byref(tune.c())) == COUL_OK
 
 
 def tune_supported_2d(tune: Tune) -> bool:

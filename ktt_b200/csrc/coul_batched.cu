@@ -102,6 +102,21 @@ static cudaError_t launch_batched(coul_batch* b, cudaStream_t stream, int accumu
 
 extern "C" {
 
+COUL_API int coul_batch_tune_supported(const coul_tune* tune)
+{
+    if (tune == nullptr)
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "tune is NULL");
+    const int threads = tune->block_x * tune->block_y;
+    if (tune->block_x < 1 || tune->block_y < 1 || threads > kMaxThreads)
+        return set_error(COUL_ERR_DEVICE_LIMITS, "block shape outside 1..256 threads");
+    const int unroll = tune->unroll <= 1 ? 1 : tune->unroll;
+    for (const auto& v : batch_variants())
+        if (v.zi == tune->z_iterations && v.xp == tune->x_points && v.unroll == unroll && v.prec == tune->precision &&
+            v.soft == tune->rsqrt_soft && tune->atom_source == COUL_ATOMS_SHARED_TMA)
+            return COUL_OK;
+    return set_error(COUL_ERR_UNSUPPORTED, "no compiled persistent variant for this tile shape");
+}
+
 COUL_API int coul_batch_create(coul_ctx* ctx, const coul_molecule* molecules, int n_molecules, const coul_tune* tune,
                                coul_batch** out)
 {

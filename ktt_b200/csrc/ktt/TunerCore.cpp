@@ -265,6 +265,11 @@ TunerCore::~TunerCore()
             coul_buffer_free(m_Context, m_ScratchDevice);
         }
 
+        for (auto& [key, batch] : m_Batches)
+        {
+            coul_batch_destroy(batch);
+        }
+
         coul_ctx_destroy(m_Context);
     }
 }
@@ -885,6 +890,60 @@ Nanoseconds TunerCore::LaunchDefinition(const KernelData& kernel, const KernelDe
         rc = coul_forward_2d(ctx, vector(0), static_cast<int64_t>(scalar(1)), static_cast<float>(scalar(2)),
             static_cast<int>(definition.globalSize.GetSizeX()), static_cast<int>(definition.globalSize.GetSizeY()), &reference, 0,
             vector(3));
+    }
+    else if (definition.name == "coulombBatch" && args.size() == 6)
+    {
+        // This library's batched map as a tunable kernel (no KTT counterpart; KTT launches one kernel per
+        // problem): (atoms: float4 of all molecules concatenated, atomOffsets: int64[m + 1] in atoms,
+        // grids: float[7 m] = nx, ny, nz, spacing, origin x/y/z, maps: float of all maps concatenated (output),
+        // mapOffsets: int64[m + 1] in floats, moleculeCount: int).  The tile configuration comes from the same
+        // parameters as directCoulombSum; one persistent launch, replayed from a CUDA graph, computes all maps.
+        const int m = static_cast<int>(scalar(5));
+        const ArgumentData& atomOffsets = Argument(args.at(1));
+        const ArgumentData& grids = Argument(args.at(2));
+        const ArgumentData& mapOffsets = Argument(args.at(4));
+
+        if (m < 1 || atomOffsets.bytes < static_cast<size_t>(m + 1) * 8 || mapOffsets.bytes < static_cast<size_t>(m + 1) * 8
+            || grids.bytes < static_cast<size_t>(m) * 7 * 4 || atomOffsets.dataType != ArgumentDataType::Long
+            || mapOffsets.dataType != ArgumentDataType::Long || grids.dataType != ArgumentDataType::Float)
+        {
+            throw RunFailure(ResultStatus::ComputationFailed, "coulombBatch: offsets must be int64[m + 1], grids float[7 m]");
+        }
+
+        const auto* ao = static_cast<const int64_t*>(atomOffsets.HostData());
+        const auto* mo = static_cast<const int64_t*>(mapOffsets.HostData());
+        const auto* gr = static_cast<const float*>(grids.HostData());
+        float* atoms = vector(0);
+        float* maps = vector(3);
+        tune.z_iterations = static_cast<int>(parameter("Z_ITERATIONS", 8));
+        tune.x_points = static_cast<int>(parameter("X_POINTS", parameter("VECTOR_SIZE", 1)));
+        tune.atom_source = COUL_ATOMS_SHARED_TMA;
+        std::ostringstream key;
+        key << static_cast<const void*>(atoms) << '/' << static_cast<const void*>(maps) << '/' << m << '/' << tune.block_x << ','
+            << tune.block_y << ',' << tune.z_iterations << ',' << tune.x_points << ',' << tune.unroll << ',' << tune.precision
+            << ',' << tune.rsqrt_soft;
+        auto it = m_Batches.find(key.str());
+
+        if (it == m_Batches.end())
+        {
+            std::vector<coul_molecule> molecules(static_cast<size_t>(m));
+
+            for (int i = 0; i < m; ++i)
+            {
+                coul_molecule& mol = molecules[static_cast<size_t>(i)];
+                mol.d_atoms = atoms + ao[i] * 4;
+                mol.n_atoms = ao[i + 1] - ao[i];
+                mol.grid = coul_grid{static_cast<int>(gr[7 * i]), static_cast<int>(gr[7 * i + 1]), static_cast<int>(gr[7 * i + 2]),
+                    gr[7 * i + 3], {gr[7 * i + 4], gr[7 * i + 5], gr[7 * i + 6]}};
+                mol.d_out = maps + mo[i];
+            }
+
+            coul_batch* batch = nullptr;
+            CheckCoul(coul_batch_create(ctx, molecules.data(), m, &tune, &batch), "coulombBatch set-up");
+            it = m_Batches.emplace(key.str(), batch).first;
+        }
+
+        rc = coul_batch_run(ctx, it->second, COUL_BATCH_GRAPH, 0);
     }
     else if (definition.name == "nbody_kernel" && args.size() == 15)
     {

@@ -187,6 +187,8 @@ private:
     std::map<ArgumentId, ValidationData> m_Validation;
     void* m_ScratchDevice = nullptr;  // float4 atoms gathered from KTT's four-array layout
     size_t m_ScratchBytes = 0;
+    // persistent batches of the coulombBatch definition, one per (arguments, tile configuration)
+    std::map<std::string, coul_batch*> m_Batches;
 
     void ResetWritableArguments(const KernelData& kernel);
     bool ValidateOutputs(const KernelData& kernel, const KernelConfiguration& configuration, KernelResult& result);
