@@ -1,7 +1,7 @@
 """Measure the batched persistent path on the uneven-molecule batch.
 
     python -m ktt_b200.run_batch [--molecules 512] [--repeat 3] [--margin 8] [--set field=value ...]
-    python -m ktt_b200.run_batch --autotune [--save ktt_b200/tuned/b200_batch.json]
+    python -m ktt_b200.run_batch --autotune-ktt-form [--save ktt_b200/tuned/b200_batch.json]
 
 512 molecules with atom counts log-uniform in [200, 20000] (seeded), atoms uniform in a cube of side
 (n / 0.1)^(1/3) A, grids = bounding box + `margin` A on every side at 0.5 A.  Prints one JSON line
@@ -10,41 +10,20 @@ the same kernel form per molecule, and one synchronous launch per molecule of KT
 (atoms in __constant__ memory, all rsqrts on MUFU, FP32; what a KTT user's per-molecule Tuner::Run
 loop launches).
 
---autotune searches the batched kernel's tile space (the compiled batch variants x CTA shapes) on
-the batch itself, exhaustively or on a seeded random sample of --budget configurations, each timed
-as a graph replay; the KTT-form baseline's (z_iterations, x_points, CTA shape) is searched the
-same way, so both arms run at their best tile shape.
+The batched kernel's tile comes from `python -m ktt_b200.autotune batch` (KTT's searchers over the
+tuner's coulombBatch definition), stored under "batched"; --autotune-ktt-form searches the KTT-form
+baseline's (z_iterations, x_points, CTA shape) exhaustively on the batch and stores it under
+"ktt_form", so both arms run at their best tile shape.
 """
 from __future__ import annotations
 
 import argparse
 import json
 import os
-import random
 
-# compiled batch variants: (z_iterations, x_points, unroll, precision, rsqrt_soft)
-BATCH_FORMS = [(8, 2, 2, 0, 2), (8, 2, 1, 0, 2), (8, 2, 2, 0, 0), (8, 2, 1, 0, 0), (4, 2, 1, 0, 2),
-               (4, 4, 1, 0, 2), (8, 4, 1, 0, 2), (16, 1, 1, 0, 2), (16, 2, 1, 0, 2), (8, 1, 2, 0, 2),
-               (8, 1, 1, 0, 2), (8, 1, 2, 0, 0), (4, 1, 2, 0, 2)]
-CTA_SHAPES = [(8, 16), (16, 8), (32, 4), (8, 8), (16, 16), (4, 32), (8, 32), (32, 8)]
 KTT_FORMS = [(zi, xp) for zi in (4, 8, 16) for xp in (1, 2, 4)]
 KTT_CTA_SHAPES = [(32, 4), (16, 8), (32, 8), (64, 4)]
 DEFAULT_TUNED = os.path.join(os.path.dirname(__file__), "tuned", "b200_batch.json")
-
-
-def _tune(ktt_b200, zi, xp, un, prec, soft, bx, by):
-    return ktt_b200.Tune(block_x=bx, block_y=by, z_iterations=zi, x_points=xp, unroll=un,
-                         precision=prec, rsqrt_soft=soft)
-
-
-def _time_graph(ctx, batch, ktt_b200, repeat):
-    batch.run(ktt_b200.BATCH_GRAPH)
-    ctx.synchronize()
-    ms = []
-    for _ in range(repeat):
-        batch.run(ktt_b200.BATCH_GRAPH)
-        ms.append(ctx.elapsed_ms())
-    return min(ms)
 
 
 def _time_ktt_form(ctx, inputs, outs, tune, repeat):
@@ -66,21 +45,6 @@ def _time_ktt_form(ctx, inputs, outs, tune, repeat):
     return best
 
 
-def autotune(ctx, inputs, ktt_b200, budget, seed, repeat=1):
-    space = [f + s for f in BATCH_FORMS for s in CTA_SHAPES if s[0] * s[1] <= 256]
-    if budget and budget < len(space):
-        space = random.Random(seed).sample(space, budget)
-    trials = []
-    for cfg in space:
-        tune = _tune(ktt_b200, *cfg)
-        batch = ktt_b200.Batch(ctx, inputs, tune)
-        ms = _time_graph(ctx, batch, ktt_b200, repeat)
-        trials.append({"tune": tune.as_dict(), "ms": ms, "gpairs_per_s": batch.total_pairs / (ms * 1e-3) / 1e9})
-        batch.close()
-        print(json.dumps({"trial": trials[-1]}), flush=True)
-    return min(trials, key=lambda t: t["ms"]), len(space)
-
-
 def autotune_ktt_form(ctx, inputs, outs, ktt_b200, pairs):
     trials = []
     for zi, xp in KTT_FORMS:
@@ -100,9 +64,8 @@ def main() -> None:
     ap.add_argument("--seed", type=int, default=4)
     ap.add_argument("--margin", type=float, default=8.0, help="A of margin on every side of the bounding box")
     ap.add_argument("--set", action="append", default=[], metavar="FIELD=VALUE")
-    ap.add_argument("--autotune", action="store_true")
-    ap.add_argument("--budget", type=int, default=0, help="random sample size for --autotune (0 = all)")
-    ap.add_argument("--save", default="", help="write the autotuned configurations to this JSON file")
+    ap.add_argument("--autotune-ktt-form", action="store_true")
+    ap.add_argument("--save", default="", help="write the tuned configurations, with the new ktt_form, to this file")
     ap.add_argument("--tuned", default=DEFAULT_TUNED, help="tuned configurations to start from")
     args = ap.parse_args()
 
@@ -122,12 +85,10 @@ def main() -> None:
         with open(args.tuned) as f:
             tuned = json.load(f)
     out = {"molecules": len(mols), "margin_per_side": args.margin}
-    if args.autotune:
-        best, searched = autotune(ctx, inputs, ktt_b200, args.budget, args.seed)
+    if args.autotune_ktt_form:
         ktt_best = autotune_ktt_form(ctx, inputs, outs, ktt_b200, pairs)
-        tuned = {"batched": best["tune"], "ktt_form": ktt_best["tune"],
-                 "searched": searched, "workload": f"{len(mols)} molecules, seed {args.seed}, margin {args.margin}"}
-        out["autotune"] = {"configurations": searched, "best": best, "ktt_form_best": ktt_best}
+        tuned["ktt_form"] = ktt_best["tune"]
+        out["ktt_form_best"] = ktt_best
         if args.save:
             with open(args.save, "w") as f:
                 json.dump(tuned, f, indent=1)
