@@ -13,4 +13,5 @@
 #include <ktt/Searcher.h>
 #include <ktt/StopCondition.h>
 #include <ktt/Tuner.h>
+#include <ktt/ProfileBasedSearcher.h>
 #include <ktt/TuningLoader.h>

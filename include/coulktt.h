@@ -322,6 +322,38 @@ COUL_API int coul_batch_run_static(void* stream, const coul_molecule* molecules,
  */
 COUL_API int coul_measure_pipe_rates(coul_ctx* ctx, double* rsqrt_per_s, double* ffma_per_s);
 
+/* ---- hardware counters ----------------------------------------------------------- */
+/*
+ * Counter collection around the context's launches with CUPTI's range profiler (user range,
+ * user replay), loaded at run time from libcupti.  Replaces KTT's CUPTI metric interface
+ * (Source/ComputeEngine/Cuda/Cupti/CuptiMetricInterface.cpp:21-120: metric configuration,
+ * counter-data image, unsupported metrics dropped with a warning; CuptiInstance.cpp / CuptiPass:
+ * one pass per kernel run, repeated until every pass is collected).  Usage:
+ *
+ *   coul_profiler_create(ctx, names, n, valid, &p, &passes)   names the metrics (Perfworks names)
+ *   do {                                               the caller reruns the same launches once per
+ *       coul_profiler_begin_pass(p);                   pass; they must do the same work each time
+ *       ... launches on the context's stream ...
+ *       coul_profiler_end_pass(p, &done);
+ *   } while (!done);
+ *   coul_profiler_read(p, values);                     one double per metric, in the given order
+ *   coul_profiler_destroy(p);
+ *
+ * Metrics the device does not offer are dropped (valid[i] = 0, optional array of n entries) and
+ * read back as NaN; if none is left, create fails with COUL_ERR_INVALID_ARGUMENT.  Clocks and other
+ * device settings are left as they are.  One profiler per process at a time.  Without libcupti
+ * create returns COUL_ERR_UNSUPPORTED.  coul_profiler_supported answers the same question without
+ * a GPU for a named chip ("GB100" for B200).
+ */
+typedef struct coul_profiler coul_profiler;
+COUL_API int coul_profiler_supported(const char* chip, const char* const* metrics, int n_metrics, int* valid);
+COUL_API int coul_profiler_create(coul_ctx* ctx, const char* const* metrics, int n_metrics, int* valid,
+                                  coul_profiler** out, int* passes);
+COUL_API int coul_profiler_begin_pass(coul_profiler* profiler);
+COUL_API int coul_profiler_end_pass(coul_profiler* profiler, int* all_passes_done);
+COUL_API int coul_profiler_read(coul_profiler* profiler, double* values);
+COUL_API int coul_profiler_destroy(coul_profiler* profiler);
+
 /* ---- failure detection ------------------------------------------------------ */
 /*
  * Runs one CTA that waits on an mbarrier with the given budget (at most 2 s).  With arrive != 0

@@ -25,6 +25,14 @@ public:
     virtual ComputeActionId RunKernelAsync(const KernelDefinitionId id, const QueueId queue, const DimensionVector& globalSize,
         const DimensionVector& localSize) = 0;
     virtual void WaitForComputeAction(const ComputeActionId id) = 0;
+    // Profiled launches (Source/Api/ComputeInterface.h:82-119).  Here the counter passes replay the
+    // launcher's whole execution before its timed run (Tuner::SetProfiling), so these run the
+    // definition like RunKernel and no profiling runs ever remain.
+    virtual void RunKernelWithProfiling(const KernelDefinitionId id) = 0;
+    virtual void RunKernelWithProfiling(const KernelDefinitionId id, const DimensionVector& globalSize,
+        const DimensionVector& localSize) = 0;
+    virtual uint64_t GetRemainingProfilingRuns(const KernelDefinitionId id) const = 0;
+    virtual uint64_t GetRemainingProfilingRuns() const = 0;
 
     virtual QueueId GetDefaultQueue() const = 0;
     virtual std::vector<QueueId> GetAllQueues() const = 0;

@@ -2,11 +2,13 @@
 //
 // Interfaces of KTT 2.1.0 Source/Api/Output/ComputationResult.h, KernelCompilationData.h,
 // KernelResult.h (durations and overheads, TotalDuration = kernel durations + extra duration:
-// Source/Api/Output/KernelResult.cpp:108-242) and BufferOutputDescriptor.h.
+// Source/Api/Output/KernelResult.cpp:108-242), KernelProfilingCounter.h, KernelProfilingData.h,
+// ProfilingCounterType.h and BufferOutputDescriptor.h.
 #pragma once
 
 #include <memory>
 #include <string>
+#include <variant>
 #include <vector>
 
 #include <ktt/Configuration.h>
@@ -27,6 +29,65 @@ public:
     uint64_t m_RegistersCount;
 };
 
+enum class ProfilingCounterType
+{
+    Int,
+    UnsignedInt,
+    Double,
+    Percent,
+    Throughput,
+    UtilizationLevel
+};
+
+// One hardware counter of a profiled run (CUPTI metrics arrive as Double).
+class KTT_API KernelProfilingCounter
+{
+public:
+    KernelProfilingCounter();
+    explicit KernelProfilingCounter(const std::string& name, const ProfilingCounterType type, const int64_t value);
+    explicit KernelProfilingCounter(const std::string& name, const ProfilingCounterType type, const uint64_t value);
+    explicit KernelProfilingCounter(const std::string& name, const ProfilingCounterType type, const double value);
+
+    const std::string& GetName() const;
+    ProfilingCounterType GetType() const;
+    int64_t GetValueInt() const;
+    uint64_t GetValueUint() const;
+    double GetValueDouble() const;
+
+    bool operator==(const KernelProfilingCounter& other) const;
+    bool operator!=(const KernelProfilingCounter& other) const;
+    bool operator<(const KernelProfilingCounter& other) const;
+
+private:
+    std::string m_Name;
+    ProfilingCounterType m_Type;
+    std::variant<int64_t, uint64_t, double> m_Value;
+};
+
+// The counters of one profiled computation; while passes remain it holds their count instead
+// (valid once it has no remaining runs).
+class KTT_API KernelProfilingData
+{
+public:
+    KernelProfilingData();
+    explicit KernelProfilingData(const uint64_t remainingRuns);
+    explicit KernelProfilingData(const std::vector<KernelProfilingCounter>& counters);
+
+    bool IsValid() const;
+    bool HasCounter(const std::string& name) const;
+    const KernelProfilingCounter& GetCounter(const std::string& name) const;
+    const std::vector<KernelProfilingCounter>& GetCounters() const;
+    void SetCounters(const std::vector<KernelProfilingCounter>& counters);
+    void AddCounter(const KernelProfilingCounter& counter);
+    bool HasRemainingProfilingRuns() const;
+    uint64_t GetRemainingProfilingRuns() const;
+    void DecreaseRemainingProfilingRuns();
+
+private:
+    std::vector<KernelProfilingCounter> m_Counters;
+    uint64_t m_RemainingRuns;
+};
+
 class KTT_API ComputationResult
 {
 public:
@@ -39,6 +100,7 @@ public:
         const Nanoseconds compilationOverhead = 0);
     void SetSizeData(const DimensionVector& globalSize, const DimensionVector& localSize);
     void SetCompilationData(std::unique_ptr<KernelCompilationData> data);
+    void SetProfilingData(std::unique_ptr<KernelProfilingData> data);
 
     const std::string& GetKernelFunction() const;
     const DimensionVector& GetGlobalSize() const;
@@ -49,6 +111,7 @@ public:
     bool HasCompilationData() const;
     const KernelCompilationData& GetCompilationData() const;
     bool HasProfilingData() const;
+    const KernelProfilingData& GetProfilingData() const;
     bool HasRemainingProfilingRuns() const;
     bool HasPowerData() const;
 
@@ -60,6 +123,7 @@ private:
     Nanoseconds m_Overhead;
     Nanoseconds m_CompilationOverhead;
     std::unique_ptr<KernelCompilationData> m_CompilationData;
+    std::unique_ptr<KernelProfilingData> m_ProfilingData;
 };
 
 class KTT_API KernelResult

@@ -197,8 +197,14 @@ public:
 
     // ---- running and validation ------------------------------------------------------------
     KernelResult Run(const KernelId id, const KernelConfiguration& configuration, const std::vector<BufferOutputDescriptor>& output);
+    // Profiled runs collect hardware counters with CUPTI's range profiler: before the timed run the
+    // kernel's whole execution (its launcher, or each definition) is replayed once per counter pass,
+    // each time from reset arguments, and the counters are attached to the first ComputationResult.
     void SetProfiling(const bool flag);
     bool GetProfiling();
+    // Counters to collect (names of CUPTI's metrics; ones the device does not offer are dropped with
+    // a warning); by default KTT's list plus the XU-pipe instruction count.
+    void SetProfilingCounters(const std::vector<std::string>& counters);
     void SetValidationMethod(const ValidationMethod method, const double toleranceThreshold);
     void SetValidationMode(const ValidationMode mode);
     void SetValidationRange(const ArgumentId& id, const size_t range);
@@ -217,8 +223,9 @@ public:
     std::vector<KernelResult> SimulateTuning(const KernelId id, const std::vector<KernelResult>& results,
         const uint64_t iterations);
     void SetSearcher(const KernelId id, std::unique_ptr<Searcher> searcher);
-    // KTT's profile-based searcher needs CUPTI counters and a trained model loaded through embedded
-    // Python; neither is part of this library, so this logs an error and leaves the searcher unchanged.
+    // KTT's profile-based searcher (ProfileBasedSearcher.h) with the counter model at modelPath (the
+    // JSON forest of ktt_b200/profile_model.py; for a KTT model path "X.sav", "X.sav.json").
+    // useBuiltinModule has no effect: the searcher is native code.
     void SetProfileBasedSearcher(const KernelId id, const std::string& modelPath, const bool useBuiltinModule = true,
         const uint32_t batchSize = 5, const uint32_t neighborSize = 100, const uint32_t randomSize = 10);
     void InitializeConfigurationData(const KernelId id);

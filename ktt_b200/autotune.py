@@ -3,6 +3,8 @@
     python -m ktt_b200.autotune map3d [--searcher mcmc|random|deterministic] [--budget 60] [--save]
     python -m ktt_b200.autotune batch [--searcher mcmc|random|deterministic] [--budget 40] [--save]
     python -m ktt_b200.autotune map3d --dry-run          # the configuration space only (no GPU)
+    python -m ktt_b200.autotune map3d --profile --results space.json ...   # record counters of every run
+    python -m ktt_b200.autotune map3d --searcher profile --model model.json # KTT's profile-based searcher
 
 The kernel is registered with the ktt:: tuner exactly as a KTT host program registers
 directCoulombSum (Examples/CoulombSum3d/CoulombSum3d.cpp:100-237) -- definition, arguments, tuning
@@ -71,8 +73,31 @@ def _add_space(ktt, tuner, kernel, definition, space, supported):
     tuner.AddConstraint(kernel, names, lambda v: supported(_tune_from(v, names)))
 
 
-def _searcher(ktt, name):
+SEARCHERS = ["mcmc", "random", "deterministic", "profile"]
+
+
+def _searcher(ktt, name, tuner=None, model="", seed=None):
+    if name == "profile":
+        # KTT's profile-based searcher (native, include/ktt/ProfileBasedSearcher.h) with a counter model
+        # trained by ktt_b200.profile_model from results recorded with --profile
+        if not model:
+            raise ValueError("the profile-based searcher needs --model (see ktt_b200/profile_model.py)")
+        return ktt.ProfileBasedSearcher(tuner, ktt.CounterModel.Load(model), 5, 100, 10,
+                                        seed if seed is not None else int.from_bytes(os.urandom(8), "little"))
     return {"mcmc": ktt.McmcSearcher, "random": ktt.RandomSearcher, "deterministic": ktt.DeterministicSearcher}[name]()
+
+
+def _run(ktt, tuner, kernel, searcher, budget, profile, results_path, model, seed):
+    """The search itself: searcher, optional counters on every run, optional KTT-format results file."""
+    tuner.SetSearcher(kernel, _searcher(ktt, searcher, tuner, model, seed))
+    if profile:
+        tuner.SetProfiling(True)
+    results = tuner.Tune(kernel, ktt.ConfigurationCount(budget))
+    tuner.SetProfiling(False)
+    if results_path:
+        base = results_path[:-5] if results_path.endswith(".json") else results_path
+        tuner.SaveResults(results, base, ktt.OutputFormat.JSON)
+    return results
 
 
 def _summary(results, work):
@@ -81,6 +106,7 @@ def _summary(results, work):
         cfg = {p.GetName(): int(p.GetValueString()) for p in r.GetConfiguration().GetPairs()}
         ns = r.GetTotalDuration()
         trials.append({"config": cfg, "status": str(r.GetStatus()).split(".")[-1],
+                       "profiled": bool(r.GetResults()) and r.GetResults()[0].HasProfilingData(),
                        "ms": ns * 1e-6 if r.IsValid() else None,
                        "gpairs_per_s": work / (ns * 1e-9) / 1e9 if r.IsValid() and ns > 0 else None})
     valid = [t for t in trials if t["gpairs_per_s"] is not None]
@@ -91,7 +117,8 @@ def _summary(results, work):
 
 
 def tune_map3d(grid: int = 256, atoms: int = 65536, searcher: str = "mcmc", budget: int = 60,
-               dry_run: bool = False) -> dict:
+               dry_run: bool = False, profile: bool = False, results_path: str = "", model: str = "",
+               seed: int | None = None) -> dict:
     """Searches the single-map tile space on the uniform workload (grid^3 points at 0.5 A, `atoms` atoms
     uniform in the cube the grid spans).  dry_run: only build the space and report its size."""
     import ktt_b200
@@ -128,8 +155,7 @@ def tune_map3d(grid: int = 256, atoms: int = 65536, searcher: str = "mcmc", budg
     tuner.SetReferenceComputation(grid_id, g ** 3 * 4, compute_reference)
     threshold = 1e-5 * float(np.abs(ref).max())
     tuner.SetValidationMethod(ktt.ValidationMethod.SideBySideComparison, threshold)
-    tuner.SetSearcher(kernel, _searcher(ktt, searcher))
-    results = tuner.Tune(kernel, ktt.ConfigurationCount(budget))
+    results = _run(ktt, tuner, kernel, searcher, budget, profile, results_path, model, seed)
     best, trials = _summary(results, float(g) ** 3 * n)
     out = {
         "workload": f"{g}^3 grid, h={h} A, {n} atoms uniform in the {g * h:g} A cube",
@@ -145,7 +171,8 @@ def tune_map3d(grid: int = 256, atoms: int = 65536, searcher: str = "mcmc", budg
 
 
 def tune_batch(molecules: int = 512, seed: int = 4, searcher: str = "mcmc", budget: int = 40,
-               dry_run: bool = False) -> dict:
+               dry_run: bool = False, profile: bool = False, results_path: str = "", model: str = "",
+               search_seed: int | None = None) -> dict:
     """Searches the batched-map tile space (the coulombBatch definition) on the uneven molecule batch
     (`molecules` molecules of 200-20000 atoms, log-uniform, from `seed`)."""
     import torch
@@ -192,8 +219,7 @@ def tune_batch(molecules: int = 512, seed: int = 4, searcher: str = "mcmc", budg
 
     tuner.SetReferenceComputation(maps_id, ref.size * 4, compute_reference)
     tuner.SetValidationMethod(ktt.ValidationMethod.SideBySideComparison, 1e-5 * float(np.abs(ref).max()))
-    tuner.SetSearcher(kernel, _searcher(ktt, searcher))
-    results = tuner.Tune(kernel, ktt.ConfigurationCount(budget))
+    results = _run(ktt, tuner, kernel, searcher, budget, profile, results_path, model, search_seed)
     pairs = float(sum(m.pairs for m in mols))
     best, trials = _summary(results, pairs)
     return {
@@ -209,7 +235,11 @@ def tune_batch(molecules: int = 512, seed: int = 4, searcher: str = "mcmc", budg
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("target", choices=["map3d", "batch"])
-    ap.add_argument("--searcher", choices=["mcmc", "random", "deterministic"], default="mcmc")
+    ap.add_argument("--searcher", choices=SEARCHERS, default="mcmc")
+    ap.add_argument("--model", default="", help="counter model of the profile-based searcher")
+    ap.add_argument("--search-seed", type=int, default=None, help="seed of the profile-based searcher")
+    ap.add_argument("--profile", action="store_true", help="collect hardware counters on every run")
+    ap.add_argument("--results", default="", help="also write the tuner's results (KTT JSON) to this file")
     ap.add_argument("--budget", type=int, default=0, help="configurations to test (default 60 map3d, 40 batch)")
     ap.add_argument("--atoms", type=int, default=65536)
     ap.add_argument("--grid", type=int, default=256)
@@ -224,9 +254,11 @@ def main() -> None:
     from ktt_b200 import pyktt as ktt
     ktt.Tuner.SetLoggingLevel(ktt.LoggingLevel.Warning)
     if args.target == "map3d":
-        result = tune_map3d(args.grid, args.atoms, args.searcher, args.budget, args.dry_run)
+        result = tune_map3d(args.grid, args.atoms, args.searcher, args.budget, args.dry_run, args.profile,
+                            args.results, args.model, args.search_seed)
     else:
-        result = tune_batch(args.molecules, args.seed, args.searcher, args.budget, args.dry_run)
+        result = tune_batch(args.molecules, args.seed, args.searcher, args.budget, args.dry_run, args.profile,
+                            args.results, args.model, args.search_seed)
     print(json.dumps({k: v for k, v in result.items() if k != "trials"}))
     path = args.out or (os.path.join(TUNED, "b200_map3d.json" if args.target == "map3d" else "b200_batch.json")
                         if args.save else "")

@@ -85,6 +85,76 @@ const char* StatusName(const ResultStatus status)
     return "ComputationFailed";
 }
 
+// ProfilingCounterType names of Source/Output/JsonConverters.h:56-64
+const char* CounterTypeName(const ProfilingCounterType type)
+{
+    switch (type)
+    {
+    case ProfilingCounterType::Int: return "Int";
+    case ProfilingCounterType::UnsignedInt: return "UnsignedInt";
+    case ProfilingCounterType::Double: return "Double";
+    case ProfilingCounterType::Percent: return "Percent";
+    case ProfilingCounterType::Throughput: return "Throughput";
+    case ProfilingCounterType::UtilizationLevel: return "UtilizationLevel";
+    }
+
+    return "Double";
+}
+
+// Value written by the counter's type (Source/Output/JsonConverters.cpp:141-166); floating-point
+// values with all 17 significant digits, so that a counter reads back bit for bit, NaN as null
+std::string CounterValueJson(const KernelProfilingCounter& counter)
+{
+    switch (counter.GetType())
+    {
+    case ProfilingCounterType::Int: return std::to_string(counter.GetValueInt());
+    case ProfilingCounterType::UnsignedInt:
+    case ProfilingCounterType::Throughput:
+    case ProfilingCounterType::UtilizationLevel: return std::to_string(counter.GetValueUint());
+    default:
+    {
+        const double v = counter.GetValueDouble();
+
+        if (!std::isfinite(v))
+        {
+            return "null";
+        }
+
+        std::ostringstream text;
+        text << std::setprecision(17) << v;
+        return text.str();
+    }
+    }
+}
+
+KernelProfilingCounter CounterFromJson(const Json& j)
+{
+    const std::string name = j.StringOr("Name", "");
+    const std::string typeName = j.StringOr("Type", "Double");
+    const Json* value = j.Find("Value");
+    const double number = value == nullptr || value->kind == Json::Kind::Null
+        ? std::nan("") : (value->integral ? static_cast<double>(value->integer) : value->number);
+
+    if (typeName == "Int")
+    {
+        return KernelProfilingCounter(name, ProfilingCounterType::Int,
+            static_cast<int64_t>(value && value->integral ? value->integer : std::llround(number)));
+    }
+
+    for (const auto type : {ProfilingCounterType::UnsignedInt, ProfilingCounterType::Throughput,
+             ProfilingCounterType::UtilizationLevel})
+    {
+        if (typeName == CounterTypeName(type))
+        {
+            return KernelProfilingCounter(name, type,
+                static_cast<uint64_t>(value && value->integral ? value->integer : std::llround(number)));
+        }
+    }
+
+    return KernelProfilingCounter(name, typeName == "Percent" ? ProfilingCounterType::Percent : ProfilingCounterType::Double,
+        number);
+}
+
 ResultStatus StatusFromName(const std::string& name)
 {
     if (name == "Ok") return ResultStatus::Ok;
@@ -212,7 +282,24 @@ void Tuner::SaveResults(const std::vector<KernelResult>& results, const std::str
                         << ", \"Y\": " << g.GetSizeY() << ", \"Z\": " << g.GetSizeZ() << "}, \"KernelFunction\": \""
                         << Escape(cr.GetKernelFunction()) << "\", \"LocalSize\": {\"X\": " << l.GetSizeX()
                         << ", \"Y\": " << l.GetSizeY() << ", \"Z\": " << l.GetSizeZ() << "}, \"Overhead\": "
-                        << t(cr.GetOverhead()) << "}";
+                        << t(cr.GetOverhead());
+
+                    if (cr.HasProfilingData())
+                    {
+                        const KernelProfilingData& data = cr.GetProfilingData();
+                        out << ", \"ProfilingData\": {\"Counters\": [";
+
+                        for (size_t k = 0; k < data.GetCounters().size(); ++k)
+                        {
+                            const KernelProfilingCounter& counter = data.GetCounters()[k];
+                            out << (k ? ", " : "") << "{\"Name\": \"" << Escape(counter.GetName()) << "\", \"Type\": \""
+                                << CounterTypeName(counter.GetType()) << "\", \"Value\": " << CounterValueJson(counter) << "}";
+                        }
+
+                        out << "], \"RemainingProfilingRuns\": " << data.GetRemainingProfilingRuns() << "}";
+                    }
+
+                    out << "}";
                 }
 
                 out << "\n      ],\n      \"Configuration\": [";
@@ -387,6 +474,30 @@ std::vector<KernelResult> Tuner::LoadResults(const std::string& filePath, const 
                                  : DimensionVector();
                     };
                     cr.SetSizeData(size("GlobalSize"), size("LocalSize"));
+
+                    if (const Json* profiling = c.Find("ProfilingData"))
+                    {
+                        const uint64_t remaining = static_cast<uint64_t>(profiling->NumberOr("RemainingProfilingRuns", 0.0));
+                        auto data = std::make_unique<KernelProfilingData>(remaining);
+
+                        if (remaining == 0)
+                        {
+                            std::vector<KernelProfilingCounter> counters;
+
+                            if (const Json* list = profiling->Find("Counters"))
+                            {
+                                for (const auto& k : list->items)
+                                {
+                                    counters.push_back(CounterFromJson(k));
+                                }
+                            }
+
+                            data->SetCounters(counters);
+                        }
+
+                        cr.SetProfilingData(std::move(data));
+                    }
+
                     computations.push_back(cr);
                 }
             }

@@ -3,10 +3,111 @@
 // Duration bookkeeping as in KTT 2.1.0 Source/Api/Output/KernelResult.cpp:108-242: the kernel
 // duration of a result is the sum of its computations' durations, the total duration adds the
 // extra duration, the total overhead sums every overhead, and a result is valid when its status is Ok.
+#include <algorithm>
+#include <stdexcept>
+
 #include <ktt/Results.h>
 
 namespace ktt
 {
+
+// ---- profiling counters (Source/Api/Output/KernelProfilingCounter.cpp, KernelProfilingData.cpp) ----
+
+KernelProfilingCounter::KernelProfilingCounter() : m_Type(ProfilingCounterType::Double), m_Value(0.0) {}
+
+KernelProfilingCounter::KernelProfilingCounter(const std::string& name, const ProfilingCounterType type, const int64_t value) :
+    m_Name(name), m_Type(type), m_Value(value)
+{}
+
+KernelProfilingCounter::KernelProfilingCounter(const std::string& name, const ProfilingCounterType type, const uint64_t value) :
+    m_Name(name), m_Type(type), m_Value(value)
+{}
+
+KernelProfilingCounter::KernelProfilingCounter(const std::string& name, const ProfilingCounterType type, const double value) :
+    m_Name(name), m_Type(type), m_Value(value)
+{}
+
+const std::string& KernelProfilingCounter::GetName() const { return m_Name; }
+ProfilingCounterType KernelProfilingCounter::GetType() const { return m_Type; }
+
+int64_t KernelProfilingCounter::GetValueInt() const
+{
+    if (!std::holds_alternative<int64_t>(m_Value))
+    {
+        throw std::runtime_error("Profiling counter " + m_Name + " does not hold a signed integer value");
+    }
+
+    return std::get<int64_t>(m_Value);
+}
+
+uint64_t KernelProfilingCounter::GetValueUint() const
+{
+    if (!std::holds_alternative<uint64_t>(m_Value))
+    {
+        throw std::runtime_error("Profiling counter " + m_Name + " does not hold an unsigned integer value");
+    }
+
+    return std::get<uint64_t>(m_Value);
+}
+
+double KernelProfilingCounter::GetValueDouble() const
+{
+    if (!std::holds_alternative<double>(m_Value))
+    {
+        throw std::runtime_error("Profiling counter " + m_Name + " does not hold a floating-point value");
+    }
+
+    return std::get<double>(m_Value);
+}
+
+bool KernelProfilingCounter::operator==(const KernelProfilingCounter& other) const { return m_Name == other.m_Name; }
+bool KernelProfilingCounter::operator!=(const KernelProfilingCounter& other) const { return !(*this == other); }
+bool KernelProfilingCounter::operator<(const KernelProfilingCounter& other) const { return m_Name < other.m_Name; }
+
+KernelProfilingData::KernelProfilingData() : m_RemainingRuns(0) {}
+KernelProfilingData::KernelProfilingData(const uint64_t remainingRuns) : m_RemainingRuns(remainingRuns) {}
+KernelProfilingData::KernelProfilingData(const std::vector<KernelProfilingCounter>& counters) :
+    m_Counters(counters), m_RemainingRuns(0)
+{}
+
+bool KernelProfilingData::IsValid() const { return m_RemainingRuns == 0; }
+
+bool KernelProfilingData::HasCounter(const std::string& name) const
+{
+    return std::any_of(m_Counters.cbegin(), m_Counters.cend(), [&name](const auto& c) { return c.GetName() == name; });
+}
+
+const KernelProfilingCounter& KernelProfilingData::GetCounter(const std::string& name) const
+{
+    const auto it = std::find_if(m_Counters.cbegin(), m_Counters.cend(), [&name](const auto& c) { return c.GetName() == name; });
+
+    if (it == m_Counters.cend())
+    {
+        throw std::runtime_error("Profiling counter with name " + name + " was not found");
+    }
+
+    return *it;
+}
+
+const std::vector<KernelProfilingCounter>& KernelProfilingData::GetCounters() const { return m_Counters; }
+
+void KernelProfilingData::SetCounters(const std::vector<KernelProfilingCounter>& counters)
+{
+    m_Counters = counters;
+    m_RemainingRuns = 0;
+}
+
+void KernelProfilingData::AddCounter(const KernelProfilingCounter& counter) { m_Counters.push_back(counter); }
+bool KernelProfilingData::HasRemainingProfilingRuns() const { return m_RemainingRuns > 0; }
+uint64_t KernelProfilingData::GetRemainingProfilingRuns() const { return m_RemainingRuns; }
+
+void KernelProfilingData::DecreaseRemainingProfilingRuns()
+{
+    if (m_RemainingRuns > 0)
+    {
+        --m_RemainingRuns;
+    }
+}
 
 KernelCompilationData::KernelCompilationData() :
     m_MaxWorkGroupSize(0), m_LocalMemorySize(0), m_PrivateMemorySize(0), m_ConstantMemorySize(0), m_RegistersCount(0)
@@ -26,6 +127,11 @@ ComputationResult::ComputationResult(const ComputationResult& other) :
     {
         m_CompilationData = std::make_unique<KernelCompilationData>(*other.m_CompilationData);
     }
+
+    if (other.m_ProfilingData)
+    {
+        m_ProfilingData = std::make_unique<KernelProfilingData>(*other.m_ProfilingData);
+    }
 }
 
 ComputationResult& ComputationResult::operator=(const ComputationResult& other)
@@ -40,6 +146,7 @@ ComputationResult& ComputationResult::operator=(const ComputationResult& other)
         m_CompilationOverhead = other.m_CompilationOverhead;
         m_CompilationData = other.m_CompilationData ? std::make_unique<KernelCompilationData>(*other.m_CompilationData)
                                                     : nullptr;
+        m_ProfilingData = other.m_ProfilingData ? std::make_unique<KernelProfilingData>(*other.m_ProfilingData) : nullptr;
     }
 
     return *this;
@@ -60,6 +167,7 @@ void ComputationResult::SetSizeData(const DimensionVector& globalSize, const Dim
 }
 
 void ComputationResult::SetCompilationData(std::unique_ptr<KernelCompilationData> data) { m_CompilationData = std::move(data); }
+void ComputationResult::SetProfilingData(std::unique_ptr<KernelProfilingData> data) { m_ProfilingData = std::move(data); }
 const std::string& ComputationResult::GetKernelFunction() const { return m_KernelFunction; }
 const DimensionVector& ComputationResult::GetGlobalSize() const { return m_GlobalSize; }
 const DimensionVector& ComputationResult::GetLocalSize() const { return m_LocalSize; }
@@ -74,8 +182,22 @@ const KernelCompilationData& ComputationResult::GetCompilationData() const
     return m_CompilationData ? *m_CompilationData : empty;
 }
 
-bool ComputationResult::HasProfilingData() const { return false; }
-bool ComputationResult::HasRemainingProfilingRuns() const { return false; }
+bool ComputationResult::HasProfilingData() const { return m_ProfilingData != nullptr; }
+
+const KernelProfilingData& ComputationResult::GetProfilingData() const
+{
+    if (!m_ProfilingData)
+    {
+        throw std::runtime_error("Computation result of " + m_KernelFunction + " has no profiling data");
+    }
+
+    return *m_ProfilingData;
+}
+
+bool ComputationResult::HasRemainingProfilingRuns() const
+{
+    return m_ProfilingData != nullptr && m_ProfilingData->HasRemainingProfilingRuns();
+}
 bool ComputationResult::HasPowerData() const { return false; }
 
 // ---- KernelResult ---------------------------------------------------------------------------
@@ -169,7 +291,10 @@ Nanoseconds KernelResult::GetTotalOverhead() const
 }
 
 bool KernelResult::IsValid() const { return m_Status == ResultStatus::Ok; }
-bool KernelResult::HasRemainingProfilingRuns() const { return false; }
+bool KernelResult::HasRemainingProfilingRuns() const
+{
+    return std::any_of(m_Results.cbegin(), m_Results.cend(), [](const auto& r) { return r.HasRemainingProfilingRuns(); });
+}
 
 // ---- BufferOutputDescriptor -----------------------------------------------------------------
 

@@ -11,6 +11,8 @@
 #include <memory>
 #include <sstream>
 
+#include <ktt/ProfileBasedSearcher.h>
+
 #include "Logger.h"
 #include "Script.h"
 #include "TunerCore.h"
@@ -554,16 +556,11 @@ KernelResult Tuner::Run(const KernelId id, const KernelConfiguration& configurat
         [&] { KernelResult r("", configuration); r.SetStatus(ResultStatus::ComputationFailed); return r; }());
 }
 
-void Tuner::SetProfiling(const bool flag)
-{
-    // Hardware counters are collected with Nsight Compute on this path; KTT's in-process CUPTI
-    // replay is not provided, so profiling requests only record the flag.
-    if (flag)
-    {
-        log::Warning("In-process profiling counters are not collected; use Nsight Compute on the launched kernels");
-    }
+void Tuner::SetProfiling(const bool flag) { m_Core->SetProfiling(flag); }
 
-    m_Core->SetProfiling(flag);
+void Tuner::SetProfilingCounters(const std::vector<std::string>& counters)
+{
+    GuardedVoid([&] { m_Core->SetProfilingCounters(counters); });
 }
 
 bool Tuner::GetProfiling() { return m_Core->GetProfiling(); }
@@ -651,12 +648,39 @@ void Tuner::SetSearcher(const KernelId id, std::unique_ptr<Searcher> searcher)
     GuardedVoid([&] { m_Core->SetSearcher(id, std::move(searcher)); });
 }
 
-void Tuner::SetProfileBasedSearcher([[maybe_unused]] const KernelId id, const std::string& modelPath,
-    [[maybe_unused]] const bool useBuiltinModule, [[maybe_unused]] const uint32_t batchSize,
-    [[maybe_unused]] const uint32_t neighborSize, [[maybe_unused]] const uint32_t randomSize)
+void Tuner::SetProfileBasedSearcher(const KernelId id, const std::string& modelPath,
+    [[maybe_unused]] const bool useBuiltinModule, const uint32_t batchSize, const uint32_t neighborSize,
+    const uint32_t randomSize)
 {
-    log::Error("The profile-based searcher (model " + modelPath + ") needs CUPTI counters and a Python-loaded model, "
-        "which this library does not provide; the kernel keeps its current searcher");
+    // Source/Tuner.cpp:591-615 imports the Python searcher module and a pickled model; here the
+    // searcher is native and the model is the JSON forest written by ktt_b200/profile_model.py, read
+    // from modelPath or, for a KTT model path such as "X.sav", from "X.sav.json".
+    GuardedVoid([&]
+    {
+        CounterModel model;
+        std::string error;
+
+        for (const auto& path : {modelPath, modelPath + ".json"})
+        {
+            try
+            {
+                model = CounterModel::Load(path);
+                break;
+            }
+            catch (const std::exception& e)
+            {
+                error += std::string(error.empty() ? "" : "; ") + e.what();
+            }
+        }
+
+        if (model.IsEmpty())
+        {
+            throw std::runtime_error("No counter model for the profile-based searcher (" + error
+                + "); pickled scikit-learn models are not loaded, convert them with ktt_b200/profile_model.py");
+        }
+
+        m_Core->SetSearcher(id, std::make_unique<ProfileBasedSearcher>(*this, model, batchSize, neighborSize, randomSize));
+    });
 }
 
 void Tuner::InitializeConfigurationData(const KernelId id) { GuardedVoid([&] { (void)m_Core->Space(id); }); }

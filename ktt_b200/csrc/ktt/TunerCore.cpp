@@ -70,6 +70,16 @@ public:
     }
 
     void RunKernel(const KernelDefinitionId id) override { RunKernel(id, GetCurrentGlobalSize(id), GetCurrentLocalSize(id)); }
+    void RunKernelWithProfiling(const KernelDefinitionId id) override { RunKernel(id); }
+
+    void RunKernelWithProfiling(const KernelDefinitionId id, const DimensionVector& globalSize,
+        const DimensionVector& localSize) override
+    {
+        RunKernel(id, globalSize, localSize);
+    }
+
+    uint64_t GetRemainingProfilingRuns([[maybe_unused]] const KernelDefinitionId id) const override { return 0; }
+    uint64_t GetRemainingProfilingRuns() const override { return 0; }
 
     void RunKernel(const KernelDefinitionId id, const DimensionVector& globalSize, const DimensionVector& localSize) override
     {
@@ -81,7 +91,7 @@ public:
         if (it == m_Results.end())
         {
             ComputationResult result(m_Core.Definition(id).name);
-            result.SetSizeData(globalSize, localSize);
+            result.SetSizeData(m_Core.GridSize(globalSize, localSize), localSize);
             result.SetDurationData(duration, wall > duration ? wall - duration : 0);
             m_Results.emplace(id, result);
             m_Order.push_back(id);
@@ -1183,6 +1193,145 @@ bool TunerCore::ValidateOutputs(const KernelData& kernel, const KernelConfigurat
 
 // -- running --
 
+DimensionVector TunerCore::GridSize(const DimensionVector& global, const DimensionVector& local) const
+{
+    // results record the launch grid in blocks whatever the global size type (KTT divides an
+    // OpenCL-style global size by the local size before the launch: CudaKernel.cpp:107-137)
+    if (m_GlobalSizeType != GlobalSizeType::OpenCL)
+    {
+        return global;
+    }
+
+    auto blocks = [](const size_t g, const size_t l) { return l == 0 ? g : (g + l - 1) / l; };
+    return DimensionVector(blocks(global.GetSizeX(), local.GetSizeX()), blocks(global.GetSizeY(), local.GetSizeY()),
+        blocks(global.GetSizeZ(), local.GetSizeZ()));
+}
+
+const std::vector<std::string>& TunerCore::DefaultProfilingCounters()
+{
+    // KTT's default metric list (Source/ComputeEngine/Cuda/Cupti/CuptiMetricInterface.cpp:621-660),
+    // the counters its profile-based searcher reads, plus the XU-pipe instruction count that the
+    // searcher's B200 analysis adds for the MUFU-bound kernels of this path
+    static const std::vector<std::string> counters{
+        "dram__throughput.avg.pct_of_peak_sustained_elapsed",
+        "dram__sectors_read.sum",
+        "dram__sectors_write.sum",
+        "lts__t_sectors.avg.pct_of_peak_sustained_elapsed",
+        "lts__t_sectors_op_read.sum",
+        "lts__t_sectors_op_write.sum",
+        "l1tex__t_requests_pipe_lsu_mem_global_op_ld.avg.pct_of_peak_sustained_active",
+        "l1tex__t_requests_pipe_lsu_mem_global_op_ld.sum",
+        "l1tex__data_pipe_lsu_wavefronts_mem_shared.avg.pct_of_peak_sustained_elapsed",
+        "l1tex__data_pipe_lsu_wavefronts_mem_shared_op_ld.sum",
+        "l1tex__data_pipe_lsu_wavefronts_mem_shared_op_st.sum",
+        "l1tex__t_sectors_pipe_lsu_mem_local_op_ld.sum",
+        "l1tex__t_sectors_pipe_lsu_mem_local_op_st.sum",
+        "sm__warps_active.avg.pct_of_peak_sustained_active",
+        "smsp__cycles_active.avg.pct_of_peak_sustained_elapsed",
+        "smsp__sass_thread_inst_executed_op_fp16_pred_on.sum",
+        "smsp__sass_thread_inst_executed_op_fp32_pred_on.sum",
+        "smsp__sass_thread_inst_executed_op_fp64_pred_on.sum",
+        "smsp__sass_thread_inst_executed_op_integer_pred_on.sum",
+        "smsp__sass_thread_inst_executed_op_control_pred_on.sum",
+        "smsp__sass_thread_inst_executed_op_memory_pred_on.sum",
+        "smsp__sass_thread_inst_executed_op_misc_pred_on.sum",
+        "smsp__sass_thread_inst_executed_op_conversion_pred_on.sum",
+        "smsp__inst_executed.sum",
+        "smsp__inst_executed_pipe_fp16.sum",
+        "smsp__pipe_fma_cycles_active.avg.pct_of_peak_sustained_active",
+        "smsp__inst_executed_pipe_fp64.avg.pct_of_peak_sustained_active",
+        "smsp__inst_executed_pipe_xu.avg.pct_of_peak_sustained_active",
+        "smsp__inst_executed_pipe_lsu.avg.pct_of_peak_sustained_active",
+        "smsp__inst_executed_pipe_tex.avg.pct_of_peak_sustained_active",
+        "smsp__issue_active.avg.pct_of_peak_sustained_active",
+        "smsp__thread_inst_executed_per_inst_executed.ratio",
+        "smsp__thread_inst_executed_per_inst_executed.pct",
+        "smsp__inst_executed_pipe_xu.sum",
+    };
+
+    return counters;
+}
+
+void TunerCore::SetProfilingCounters(const std::vector<std::string>& counters)
+{
+    if (counters.empty())
+    {
+        throw std::runtime_error("Number of profiling metrics must be greater than zero");
+    }
+
+    m_ProfilingCounters = counters;
+}
+
+std::unique_ptr<KernelProfilingData> TunerCore::ProfileExecution(const KernelData& kernel,
+    const std::function<std::vector<ComputationResult>()>& execute)
+{
+    // One user range around a whole execution, replayed once per pass (coul_profiler_* in coulktt.h);
+    // the counters cover every launch of the execution.
+    const std::vector<std::string>& names = m_ProfilingCounters.empty() ? DefaultProfilingCounters() : m_ProfilingCounters;
+    std::vector<const char*> pointers;
+
+    for (const auto& name : names)
+    {
+        pointers.push_back(name.c_str());
+    }
+
+    std::vector<int> valid(names.size(), 0);
+    coul_profiler* profiler = nullptr;
+    int passes = 0;
+    CheckCoul(coul_profiler_create(Context(), pointers.data(), static_cast<int>(pointers.size()), valid.data(), &profiler,
+        &passes), "profiler set-up");
+    std::unique_ptr<coul_profiler, int (*)(coul_profiler*)> guard(profiler, coul_profiler_destroy);
+
+    for (size_t i = 0; i < names.size(); ++i)
+    {
+        if (!valid[i] && m_UnsupportedCounters.insert(names[i]).second)
+        {
+            log::Warning("Metric with name " + names[i] + " is not supported on the current device");
+        }
+    }
+
+    int done = 0;
+
+    for (int pass = 0; !done; ++pass)
+    {
+        if (pass > passes + 1)
+        {
+            throw RunFailure(ResultStatus::ComputationFailed, "profiler asked for more passes than it announced");
+        }
+
+        ResetWritableArguments(kernel);
+        CheckCoul(coul_profiler_begin_pass(profiler), "profiling pass");
+
+        try
+        {
+            (void)execute();
+        }
+        catch (...)
+        {
+            int ignored = 0;
+            (void)coul_profiler_end_pass(profiler, &ignored);
+            throw;
+        }
+
+        CheckCoul(coul_profiler_end_pass(profiler, &done), "profiling pass");
+    }
+
+    std::vector<double> values(names.size(), 0.0);
+    CheckCoul(coul_profiler_read(profiler, values.data()), "profiling counters");
+    std::vector<KernelProfilingCounter> counters;
+
+    for (size_t i = 0; i < names.size(); ++i)
+    {
+        if (valid[i])
+        {
+            counters.emplace_back(names[i], ProfilingCounterType::Double, values[i]);
+        }
+    }
+
+    log::Debug("Collected " + std::to_string(counters.size()) + " profiling counters in " + std::to_string(passes) + " passes");
+    return std::make_unique<KernelProfilingData>(counters);
+}
+
 KernelResult TunerCore::Run(const KernelId id, const KernelConfiguration& configuration,
     const std::vector<BufferOutputDescriptor>& output, const KernelRunMode mode)
 {
@@ -1191,30 +1340,55 @@ KernelResult TunerCore::Run(const KernelId id, const KernelConfiguration& config
     const auto start = Clock::now();
     std::vector<ComputationResult> computations;
 
-    try
+    // one execution of the kernel: its launcher, or each definition in turn
+    auto execute = [&]() -> std::vector<ComputationResult>
     {
-        ResetWritableArguments(kernel);
-
         if (kernel.launcher)
         {
             ComputeLayer layer(*this, kernel, configuration, mode);
             kernel.launcher(layer);
-            computations = layer.Results();
+            return layer.Results();
         }
-        else
+
+        std::vector<ComputationResult> list;
+
+        for (const auto definition : kernel.definitions)
         {
-            for (const auto definition : kernel.definitions)
-            {
-                const DimensionVector global = ModifiedSize(kernel, definition, ModifierType::Global, configuration);
-                const DimensionVector local = ModifiedSize(kernel, definition, ModifierType::Local, configuration);
-                const auto launchStart = Clock::now();
-                const Nanoseconds duration = LaunchDefinition(kernel, definition, configuration, global, local);
-                const Nanoseconds wall = ElapsedNs(launchStart);
-                ComputationResult computation(Definition(definition).name);
-                computation.SetSizeData(global, local);
-                computation.SetDurationData(duration, wall > duration ? wall - duration : 0);
-                computations.push_back(computation);
-            }
+            const DimensionVector global = ModifiedSize(kernel, definition, ModifierType::Global, configuration);
+            const DimensionVector local = ModifiedSize(kernel, definition, ModifierType::Local, configuration);
+            const auto launchStart = Clock::now();
+            const Nanoseconds duration = LaunchDefinition(kernel, definition, configuration, global, local);
+            const Nanoseconds wall = ElapsedNs(launchStart);
+            ComputationResult computation(Definition(definition).name);
+            computation.SetSizeData(GridSize(global, local), local);
+            computation.SetDurationData(duration, wall > duration ? wall - duration : 0);
+            list.push_back(computation);
+        }
+
+        return list;
+    };
+
+    std::unique_ptr<KernelProfilingData> profilingData;
+    Nanoseconds profilingOverhead = 0;
+
+    try
+    {
+        if (m_Profiling)
+        {
+            // the profiling passes run first, each from freshly reset arguments, so that the timed
+            // execution below and its validation see exactly one run (KTT repeats the whole tuning
+            // iteration per pass: Source/TuningRunner/TuningRunner.cpp:40-53)
+            const auto profilingStart = Clock::now();
+            profilingData = ProfileExecution(kernel, execute);
+            profilingOverhead = ElapsedNs(profilingStart);
+        }
+
+        ResetWritableArguments(kernel);
+        computations = execute();
+
+        if (profilingData && !computations.empty())
+        {
+            computations.front().SetProfilingData(std::move(profilingData));
         }
     }
     catch (const RunFailure& failure)
@@ -1234,6 +1408,7 @@ KernelResult TunerCore::Run(const KernelId id, const KernelConfiguration& config
     }
 
     result.SetResults(computations);
+    result.SetProfilingRunsOverhead(profilingOverhead);
     const bool validate = (mode == KernelRunMode::Running && HasFlag(m_ValidationMode, ValidationMode::Running))
         || (mode == KernelRunMode::OfflineTuning && HasFlag(m_ValidationMode, ValidationMode::OfflineTuning))
         || (mode == KernelRunMode::OnlineTuning && HasFlag(m_ValidationMode, ValidationMode::OnlineTuning));
@@ -1500,15 +1675,28 @@ KernelConfiguration TunerCore::CreateConfiguration(const KernelId id, const Para
         }
 
         const ParameterPair pair(name, value);
-        const bool known = std::any_of(it->values.cbegin(), it->values.cend(),
-            [&](const ParameterValue& v) { return pair.HasSameValue(ParameterPair(name, v)); });
+        // the parameter's own value of that number (a signed literal names an unsigned value alike:
+        // Python integers arrive as int64)
+        auto numeric = [](const ParameterValue& v, double& out)
+        {
+            if (std::holds_alternative<int64_t>(v)) { out = static_cast<double>(std::get<int64_t>(v)); return true; }
+            if (std::holds_alternative<uint64_t>(v)) { out = static_cast<double>(std::get<uint64_t>(v)); return true; }
+            if (std::holds_alternative<double>(v)) { out = std::get<double>(v); return true; }
+            return false;
+        };
+        const auto match = std::find_if(it->values.cbegin(), it->values.cend(), [&](const ParameterValue& v)
+        {
+            double a = 0.0;
+            double b = 0.0;
+            return pair.HasSameValue(ParameterPair(name, v)) || (numeric(v, a) && numeric(value, b) && a == b);
+        });
 
-        if (!known)
+        if (match == it->values.cend())
         {
             throw std::runtime_error("Value " + pair.GetValueString() + " is not a value of parameter " + name);
         }
 
-        pairs.push_back(pair);
+        pairs.emplace_back(name, *match);
     }
 
     for (const auto& p : kernel.parameters)

@@ -8,8 +8,10 @@
 #pragma once
 
 #include <cstdint>
+#include <functional>
 #include <map>
 #include <memory>
+#include <set>
 #include <string>
 #include <vector>
 
@@ -150,6 +152,8 @@ public:
     GlobalSizeType GetGlobalSizeType() const { return m_GlobalSizeType; }
     void SetProfiling(const bool flag) { m_Profiling = flag; }
     bool GetProfiling() const { return m_Profiling; }
+    void SetProfilingCounters(const std::vector<std::string>& counters);
+    static const std::vector<std::string>& DefaultProfilingCounters();
     void SetCompilerOptions(const std::string& options) { m_CompilerOptions = options; }
     ComputeApi GetApi() const { return m_Api; }
 
@@ -161,6 +165,7 @@ public:
     ArgumentData& Argument(const ArgumentId& id);
     DimensionVector ModifiedSize(const KernelData& kernel, const KernelDefinitionId id, const ModifierType type,
         const KernelConfiguration& configuration) const;
+    DimensionVector GridSize(const DimensionVector& global, const DimensionVector& local) const;
     // Runs one definition through its built-in sm_100a implementation; returns the event-timed duration.
     Nanoseconds LaunchDefinition(const KernelData& kernel, const KernelDefinitionId id, const KernelConfiguration& configuration,
         const DimensionVector& global, const DimensionVector& local);
@@ -189,8 +194,12 @@ private:
     size_t m_ScratchBytes = 0;
     // persistent batches of the coulombBatch definition, one per (arguments, tile configuration)
     std::map<std::string, coul_batch*> m_Batches;
+    std::vector<std::string> m_ProfilingCounters;  // empty: the default list
+    std::set<std::string> m_UnsupportedCounters;   // reported once each
 
     void ResetWritableArguments(const KernelData& kernel);
+    std::unique_ptr<KernelProfilingData> ProfileExecution(const KernelData& kernel,
+        const std::function<std::vector<ComputationResult>()>& execute);
     bool ValidateOutputs(const KernelData& kernel, const KernelConfiguration& configuration, KernelResult& result);
     void ComputeReference(const ArgumentId& id, ValidationData& data);
     bool Compare(const ArgumentData& argument, const ValidationData& data, const void* result, const size_t elements) const;

@@ -223,9 +223,55 @@ PYBIND11_MODULE(pyktt, m)
         .def("GetArgumentId", &ktt::BufferOutputDescriptor::GetArgumentId)
         .def("GetOutputSize", &ktt::BufferOutputDescriptor::GetOutputSize);
 
+    py::enum_<ktt::ProfilingCounterType>(m, "ProfilingCounterType")
+        .value("Int", ktt::ProfilingCounterType::Int)
+        .value("UnsignedInt", ktt::ProfilingCounterType::UnsignedInt)
+        .value("Double", ktt::ProfilingCounterType::Double)
+        .value("Percent", ktt::ProfilingCounterType::Percent)
+        .value("Throughput", ktt::ProfilingCounterType::Throughput)
+        .value("UtilizationLevel", ktt::ProfilingCounterType::UtilizationLevel);
+
+    py::class_<ktt::KernelProfilingCounter>(m, "KernelProfilingCounter")
+        .def(py::init<>())
+        .def(py::init<const std::string&, const ktt::ProfilingCounterType, const int64_t>())
+        .def(py::init<const std::string&, const ktt::ProfilingCounterType, const uint64_t>())
+        .def(py::init<const std::string&, const ktt::ProfilingCounterType, const double>())
+        .def("GetName", &ktt::KernelProfilingCounter::GetName)
+        .def("GetType", &ktt::KernelProfilingCounter::GetType)
+        .def("GetValueInt", &ktt::KernelProfilingCounter::GetValueInt)
+        .def("GetValueUint", &ktt::KernelProfilingCounter::GetValueUint)
+        .def("GetValueDouble", &ktt::KernelProfilingCounter::GetValueDouble)
+        .def("__eq__", &ktt::KernelProfilingCounter::operator==)
+        .def("__ne__", &ktt::KernelProfilingCounter::operator!=)
+        .def("__lt__", &ktt::KernelProfilingCounter::operator<);
+
+    py::class_<ktt::KernelProfilingData>(m, "KernelProfilingData")
+        .def(py::init<>())
+        .def(py::init<const uint64_t>())
+        .def(py::init<const std::vector<ktt::KernelProfilingCounter>&>())
+        .def("IsValid", &ktt::KernelProfilingData::IsValid)
+        .def("HasCounter", &ktt::KernelProfilingData::HasCounter)
+        .def("GetCounter", &ktt::KernelProfilingData::GetCounter, py::return_value_policy::copy)
+        .def("GetCounters", &ktt::KernelProfilingData::GetCounters, py::return_value_policy::copy)
+        .def("SetCounters", &ktt::KernelProfilingData::SetCounters)
+        .def("AddCounter", &ktt::KernelProfilingData::AddCounter)
+        .def("HasRemainingProfilingRuns", &ktt::KernelProfilingData::HasRemainingProfilingRuns)
+        .def("GetRemainingProfilingRuns", &ktt::KernelProfilingData::GetRemainingProfilingRuns)
+        .def("DecreaseRemainingProfilingRuns", &ktt::KernelProfilingData::DecreaseRemainingProfilingRuns);
+
     py::class_<ktt::ComputationResult>(m, "ComputationResult")
         .def(py::init<>())
         .def(py::init<const std::string&>())
+        .def(py::init<const ktt::ComputationResult&>())
+        .def("SetDurationData", &ktt::ComputationResult::SetDurationData, py::arg("duration"), py::arg("overhead"),
+            py::arg("compilationOverhead") = 0)
+        .def("SetSizeData", &ktt::ComputationResult::SetSizeData)
+        .def("SetProfilingData", [](ktt::ComputationResult& r, const ktt::KernelProfilingData& data)
+            {
+                r.SetProfilingData(std::make_unique<ktt::KernelProfilingData>(data));
+            })
+        .def("GetProfilingData", &ktt::ComputationResult::GetProfilingData, py::return_value_policy::copy)
+        .def("HasRemainingProfilingRuns", &ktt::ComputationResult::HasRemainingProfilingRuns)
         .def("GetKernelFunction", &ktt::ComputationResult::GetKernelFunction)
         .def("GetGlobalSize", &ktt::ComputationResult::GetGlobalSize)
         .def("GetLocalSize", &ktt::ComputationResult::GetLocalSize)
@@ -239,7 +285,14 @@ PYBIND11_MODULE(pyktt, m)
     py::class_<ktt::KernelResult>(m, "KernelResult")
         .def(py::init<>())
         .def(py::init<const std::string&, const ktt::KernelConfiguration&>())
+        .def(py::init<const std::string&, const ktt::KernelConfiguration&, const std::vector<ktt::ComputationResult>&>())
         .def("SetStatus", &ktt::KernelResult::SetStatus)
+        .def("SetExtraDuration", &ktt::KernelResult::SetExtraDuration)
+        .def("SetDataMovementOverhead", &ktt::KernelResult::SetDataMovementOverhead)
+        .def("SetValidationOverhead", &ktt::KernelResult::SetValidationOverhead)
+        .def("SetSearcherOverhead", &ktt::KernelResult::SetSearcherOverhead)
+        .def("GetProfilingRunsOverhead", &ktt::KernelResult::GetProfilingRunsOverhead)
+        .def("HasRemainingProfilingRuns", &ktt::KernelResult::HasRemainingProfilingRuns)
         .def("GetKernelName", &ktt::KernelResult::GetKernelName)
         .def("GetResults", &ktt::KernelResult::GetResults)
         .def("GetConfiguration", &ktt::KernelResult::GetConfiguration)
@@ -262,6 +315,34 @@ PYBIND11_MODULE(pyktt, m)
         .def(py::init<>())
         .def(py::init<const ktt::KernelConfiguration&>());
 
+    // the profile-based searcher and its counter model (native; KTT runs it as embedded Python)
+    py::class_<ktt::CounterModel>(m, "CounterModel")
+        .def(py::init<>())
+        .def_static("Load", &ktt::CounterModel::Load)
+        .def("GetParameters", &ktt::CounterModel::GetParameters)
+        .def("GetCounters", &ktt::CounterModel::GetCounters)
+        .def("GetComputeCapability", &ktt::CounterModel::GetComputeCapability)
+        .def("GetMultiprocessors", &ktt::CounterModel::GetMultiprocessors)
+        .def("IsEmpty", &ktt::CounterModel::IsEmpty)
+        .def("Predict", py::overload_cast<const std::vector<double>&>(&ktt::CounterModel::Predict, py::const_))
+        .def("PredictConfiguration", py::overload_cast<const ktt::KernelConfiguration&>(&ktt::CounterModel::Predict,
+            py::const_));
+    py::classh<ktt::ProfileBasedSearcher, ktt::Searcher>(m, "ProfileBasedSearcher")
+        .def(py::init<ktt::Tuner&, const ktt::CounterModel&, const uint32_t, const uint32_t, const uint32_t, const uint64_t>(),
+            py::arg("tuner"), py::arg("model"), py::arg("batchSize") = 5, py::arg("neighborSize") = 100,
+            py::arg("randomSize") = 10, py::arg("seed") = 0, py::keep_alive<1, 2>())
+        .def("SetDeviceProperties", &ktt::ProfileBasedSearcher::SetDeviceProperties)
+        .def("SetXuPipeAnalysis", &ktt::ProfileBasedSearcher::SetXuPipeAnalysis)
+        .def("GetScoredBatches", &ktt::ProfileBasedSearcher::GetScoredBatches);
+    py::module_ profiling = m.def_submodule("profiling", "steps of the profile-based searcher");
+    profiling.def("AnalyzeBottlenecks", &ktt::profiling::AnalyzeBottlenecks, py::arg("names"), py::arg("values"),
+        py::arg("multiprocessors"), py::arg("cores"), py::arg("reactToInstructions") = ktt::profiling::ReactToInstructionBottlenecks);
+    profiling.def("ComputeChanges", &ktt::profiling::ComputeChanges, py::arg("bottlenecks"), py::arg("counters"),
+        py::arg("xuPipe") = true, py::arg("reactToInstructions") = ktt::profiling::ReactToInstructionBottlenecks);
+    profiling.def("ScoreCandidates", &ktt::profiling::ScoreCandidates);
+    profiling.def("WeightedRandomStep", &ktt::profiling::WeightedRandomStep);
+    profiling.def("CoresPerMultiprocessor", &ktt::profiling::CoresPerMultiprocessor);
+
     py::classh<ktt::StopCondition, PyStopCondition>(m, "StopCondition")
         .def(py::init<>())
         .def("IsFulfilled", &ktt::StopCondition::IsFulfilled)
@@ -281,6 +362,13 @@ PYBIND11_MODULE(pyktt, m)
         .def("RunKernelAsync", py::overload_cast<const ktt::KernelDefinitionId, const ktt::QueueId>(
             &ktt::ComputeInterface::RunKernelAsync))
         .def("WaitForComputeAction", &ktt::ComputeInterface::WaitForComputeAction)
+        .def("RunKernelWithProfiling", py::overload_cast<const ktt::KernelDefinitionId>(
+            &ktt::ComputeInterface::RunKernelWithProfiling))
+        .def("RunKernelWithProfiling", py::overload_cast<const ktt::KernelDefinitionId, const ktt::DimensionVector&,
+            const ktt::DimensionVector&>(&ktt::ComputeInterface::RunKernelWithProfiling))
+        .def("GetRemainingProfilingRuns", py::overload_cast<const ktt::KernelDefinitionId>(
+            &ktt::ComputeInterface::GetRemainingProfilingRuns, py::const_))
+        .def("GetRemainingProfilingRuns", py::overload_cast<>(&ktt::ComputeInterface::GetRemainingProfilingRuns, py::const_))
         .def("GetDefaultQueue", &ktt::ComputeInterface::GetDefaultQueue)
         .def("GetAllQueues", &ktt::ComputeInterface::GetAllQueues)
         .def("SynchronizeQueue", &ktt::ComputeInterface::SynchronizeQueue)
@@ -408,6 +496,7 @@ PYBIND11_MODULE(pyktt, m)
 
     tuner.def("Run", &ktt::Tuner::Run, py::call_guard<py::gil_scoped_release>())
         .def("SetProfiling", &ktt::Tuner::SetProfiling)
+        .def("SetProfilingCounters", &ktt::Tuner::SetProfilingCounters)
         .def("GetProfiling", &ktt::Tuner::GetProfiling)
         .def("SetValidationMethod", &ktt::Tuner::SetValidationMethod)
         .def("SetValidationMode", &ktt::Tuner::SetValidationMode)

@@ -17,10 +17,13 @@ It writes, next to this script:
   search space for ``directCoulombSum`` as measured on an RTX 2080 Ti
   (``Examples/CoulombSum3d/coulomb_2080_full_search_space.json``): each
   configuration's parameter values, status, kernel duration, total duration,
-  global/local sizes and a few profiling counters.  Used to pin the
+  global/local sizes, its 33 profiling counters and compilation data.  Used to pin the
   configuration-space enumeration (parameters + constraints of
-  ``Examples/CoulombSum3d/CoulombSum3d.cpp:137-216``) and to drive searchers
-  in simulated tuning without a GPU.
+  ``Examples/CoulombSum3d/CoulombSum3d.cpp:137-216``), to drive searchers
+  in simulated tuning without a GPU, and to train the profile-based searcher's
+  counter model as KTT trained its shipped one
+  (``Examples/CoulombSum3d/Models/2080-coulomb_output_DT.sav`` is a pickle and is
+  not read).
 * ``ktt_prefix.json`` -- the configuration -> ``#define`` prefix expectation of
   ``Tests/KernelManagerTests.cpp:57-81``.
 * ``ktt_scripts/`` -- KTT's two JSON tuning scripts for this path, parsed and
@@ -77,19 +80,14 @@ def kat(ktt_root: str) -> None:
 def space_2080(ktt_root: str) -> None:
     src = os.path.join(ktt_root, "Examples", "CoulombSum3d", "coulomb_2080_full_search_space.json")
     d = json.load(open(src))
-    keep_counters = {
-        "smsp__inst_executed_pipe_xu.avg.pct_of_peak_sustained_active",
-        "smsp__pipe_fma_cycles_active.avg.pct_of_peak_sustained_active",
-        "smsp__issue_active.avg.pct_of_peak_sustained_active",
-        "sm__warps_active.avg.pct_of_peak_sustained_active",
-    }
     results = []
+    # every counter, in the recorded order (the profile-based searcher and its model read them all);
+    # names once, values per result
+    names = [c["Name"] for c in d["Results"][0]["ComputationResults"][0]["ProfilingData"]["Counters"]]
     for r in d["Results"]:
         cr = r["ComputationResults"][0]
-        counters = {}
-        for c in cr.get("ProfilingData", {}).get("Counters", []):
-            if c["Name"] in keep_counters:
-                counters[c["Name"]] = c["Value"]
+        recorded = {c["Name"]: c["Value"] for c in cr.get("ProfilingData", {}).get("Counters", [])}
+        counters = [recorded[n] for n in names] if recorded else []
         results.append({
             "Configuration": [[p["Name"], p["Value"]] for p in r["Configuration"]],
             "Status": r["Status"],
@@ -98,15 +96,18 @@ def space_2080(ktt_root: str) -> None:
             "GlobalSize": [cr["GlobalSize"]["X"], cr["GlobalSize"]["Y"], cr["GlobalSize"]["Z"]],
             "LocalSize": [cr["LocalSize"]["X"], cr["LocalSize"]["Y"], cr["LocalSize"]["Z"]],
             "Counters": counters,
+            "CompilationData": cr.get("CompilationData", {}),
         })
     out = {
         "source": "Examples/CoulombSum3d/coulomb_2080_full_search_space.json (KTT 2.1.0)",
         "Metadata": d["Metadata"],
         "problem": {"gridSize": 256, "atoms": 64, "gridSpacing": 0.5},
+        "CounterNames": names,
         "Results": results,
     }
     with open(os.path.join(HERE, "coulomb3d_2080_space.json"), "w") as f:
-        json.dump(out, f, indent=0, separators=(",", ":"))
+        json.dump(out, f, separators=(",", ":"))
+        f.write("\n")
 
 
 def prefix(ktt_root: str) -> None:
