@@ -313,7 +313,8 @@ PYBIND11_MODULE(pyktt, m)
     py::classh<ktt::RandomSearcher, ktt::Searcher>(m, "RandomSearcher").def(py::init<>());
     py::classh<ktt::McmcSearcher, ktt::Searcher>(m, "McmcSearcher")
         .def(py::init<>())
-        .def(py::init<const ktt::KernelConfiguration&>());
+        .def(py::init<const ktt::KernelConfiguration&>())
+        .def(py::init<const ktt::KernelConfiguration&, const uint64_t>(), py::arg("start"), py::arg("seed"));
 
     // the profile-based searcher and its counter model (native; KTT runs it as embedded Python)
     py::class_<ktt::CounterModel>(m, "CounterModel")

@@ -243,3 +243,21 @@ def test_default_metrics_on_gb100(golden):
     unsupported = [n.decode() for n, v in zip(names, valid) if not v]
     # the FP16-pipe instruction count is not offered by GB100; KTT drops such metrics with a warning
     assert unsupported == ["smsp__inst_executed_pipe_fp16.sum"]
+
+
+# ---- a profiled search recorded on the B200 ------------------------------------------------------
+
+def test_b200_recording_and_study():
+    """The profiled 720-configuration search of this library's tile space recorded on a B200
+    (tests/golden/make_b200_space.py): every configuration ran and carries KTT's counters minus the
+    FP16-pipe count GB100 lacks, plus the XU-pipe count; the convergence study replays it through
+    every searcher."""
+    from ktt_b200 import run_searchers
+    space = json.load(open(os.path.join(GOLDEN, "b200_map3d_space_64.json")))
+    assert len(space["Results"]) == 720 and all(r["Status"] == "Ok" for r in space["Results"])
+    assert "smsp__inst_executed_pipe_fp16.sum" not in space["CounterNames"]
+    assert "smsp__inst_executed_pipe_xu.sum" in space["CounterNames"]
+    report = run_searchers.main(["--seeds", "2", "--budget", "30"])
+    for name in ("random", "mcmc", "profile"):
+        assert 1.0 <= report[name]["best_ratio_after"][10] < 3.0
+        assert report[name]["best_ratio_after"][80] <= report[name]["best_ratio_after"][10]
