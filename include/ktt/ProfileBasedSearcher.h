@@ -23,9 +23,11 @@
 // (ktt_b200/profile_model.py trains and writes it from results with counters) and evaluated in C++;
 // no Python runs inside the tuner.  The analysis follows KTT's branch for compute capability 7.0 and
 // newer (the counter names of CUPTI's profiler API; older GPUs' event/metric names do not exist on
-// B200).  One addition for B200, switchable: when the XU pipe (MUFU: reciprocal square root and the
-// other special functions) is the limiting pipe, fewer XU instructions are wanted, which KTT leaves
-// as a to-do (ProfileBasedSearcher.py:385).
+// B200).  One addition for B200, off by default: when the XU pipe (MUFU: reciprocal square root and
+// the other special functions) is the limiting pipe, fewer XU instructions are wanted, which KTT
+// leaves as a to-do (ProfileBasedSearcher.py:385).  On recorded B200 searches of this library's tile
+// space it made convergence worse (it pulls toward more FMA-pipe rsqrts than the FMA pipe can take),
+// so KTT's rules are the default.
 #pragma once
 
 #include <cstdint>
@@ -106,7 +108,7 @@ KTT_API std::map<std::string, double> AnalyzeBottlenecks(const std::vector<std::
 // `counters` (negative = decrease), weighted by its bottleneck; counters the list lacks are skipped.
 // With xuPipe, a limiting XU pipe asks for fewer XU instructions (smsp__inst_executed_pipe_xu.sum).
 KTT_API std::vector<double> ComputeChanges(const std::map<std::string, double>& bottlenecks,
-    const std::vector<std::string>& counters, const bool xuPipe = true,
+    const std::vector<std::string>& counters, const bool xuPipe = false,
     const double reactToInstructions = ReactToInstructionBottlenecks);
 
 // scoreTuningConfigurationsPredictor (:490-566): score of each candidate from its predicted counters
@@ -154,7 +156,7 @@ private:
     uint32_t m_RandomSize;
     std::mt19937_64 m_Generator;
     std::uniform_real_distribution<double> m_Uniform;
-    bool m_XuPipe = true;
+    bool m_XuPipe = false;
     uint32_t m_CcMajor = 0;
     uint32_t m_CcMinor = 0;
     uint32_t m_Multiprocessors = 0;

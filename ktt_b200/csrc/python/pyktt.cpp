@@ -339,7 +339,7 @@ PYBIND11_MODULE(pyktt, m)
     profiling.def("AnalyzeBottlenecks", &ktt::profiling::AnalyzeBottlenecks, py::arg("names"), py::arg("values"),
         py::arg("multiprocessors"), py::arg("cores"), py::arg("reactToInstructions") = ktt::profiling::ReactToInstructionBottlenecks);
     profiling.def("ComputeChanges", &ktt::profiling::ComputeChanges, py::arg("bottlenecks"), py::arg("counters"),
-        py::arg("xuPipe") = true, py::arg("reactToInstructions") = ktt::profiling::ReactToInstructionBottlenecks);
+        py::arg("xuPipe") = false, py::arg("reactToInstructions") = ktt::profiling::ReactToInstructionBottlenecks);
     profiling.def("ScoreCandidates", &ktt::profiling::ScoreCandidates);
     profiling.def("WeightedRandomStep", &ktt::profiling::WeightedRandomStep);
     profiling.def("CoresPerMultiprocessor", &ktt::profiling::CoresPerMultiprocessor);

@@ -6,8 +6,9 @@ The recorded search holds, for every configuration of a tuning space, its kernel
 default counters (tests/golden/make_b200_space.py).  Each searcher is replayed through the tuner's
 SimulateTuning with that many seeds: random order (KTT's RandomSearcher, drawn here without
 replacement per seed), MCMC (KTT's McmcSearcher, seeded), and the profile-based searcher (KTT's
-algorithm, native) with a counter model trained from the same recording by ktt_b200.profile_model
-(KTT's recipe: half of the profiled configurations, ExtraTreesRegressor(10)).  Profiled reruns count
+algorithm, native) with a counter model trained by ktt_b200.profile_model (KTT's recipe: half of the
+profiled configurations, ExtraTreesRegressor(10)) from the same recording or, with --model-space,
+from another one.  Profiled reruns count
 as tested configurations.  Prints one JSON line: per searcher, the mean and median number of tested
 configurations until one within 1 % / 5 % of the space's best was found, and the mean ratio of the
 best time found to the space's best after 10, 20, 40 and 80 tested configurations.
@@ -72,11 +73,13 @@ def _curve(durations, best):
 def main(argv=None) -> dict:
     ap = argparse.ArgumentParser()
     ap.add_argument("--space", default=DEFAULT_SPACE)
+    ap.add_argument("--model-space", default="", help="train the counter model on this recording instead "
+                    "(another input size, as KTT's models come from historical runs)")
     ap.add_argument("--seeds", type=int, default=40)
     ap.add_argument("--budget", type=int, default=120)
     ap.add_argument("--cc", default="10.0", help="compute capability of the recording's device")
     ap.add_argument("--sms", type=int, default=148, help="SM count of the recording's device")
-    ap.add_argument("--no-xu", action="store_true", help="the profile-based searcher without the XU-pipe addition")
+    ap.add_argument("--xu", action="store_true", help="the profile-based searcher with the XU-pipe addition")
     args = ap.parse_args(argv)
     cc_major, cc_minor = (int(x) for x in args.cc.split("."))
 
@@ -92,7 +95,11 @@ def main(argv=None) -> dict:
         results_path = os.path.join(tmp, "space.json")
         model_path = os.path.join(tmp, "model.json")
         write_ktt_results(space, results_path)
-        profile_model.main([results_path, "--out", model_path, "--cc", args.cc, "--multiprocessors", str(args.sms)])
+        training_path = results_path
+        if args.model_space:
+            training_path = os.path.join(tmp, "training.json")
+            write_ktt_results(json.load(open(args.model_space)), training_path)
+        profile_model.main([training_path, "--out", model_path, "--cc", args.cc, "--multiprocessors", str(args.sms)])
         model = ktt.CounterModel.Load(model_path)
 
         runs = {"random": [], "mcmc": [], "profile": []}
@@ -108,14 +115,15 @@ def main(argv=None) -> dict:
                 else:
                     searcher = ktt.ProfileBasedSearcher(tuner, model, 5, 100, 10, seed + 1)
                     searcher.SetDeviceProperties(cc_major, cc_minor, args.sms)
-                    searcher.SetXuPipeAnalysis(not args.no_xu)
+                    searcher.SetXuPipeAnalysis(args.xu)
                 tuner.SetSearcher(k, searcher)
                 rec = tuner.SimulateTuning(k, tuner.LoadResults(results_path, ktt.OutputFormat.JSON),
                                            ktt.ConfigurationCount(args.budget))
                 runs[name].append([times[tuple(int(p.GetValueString()) for p in r.GetConfiguration().GetPairs())]
                                    for r in rec])
 
-    report = {"space": os.path.relpath(args.space), "configurations": len(ok), "seeds": args.seeds,
+    report = {"space": os.path.relpath(args.space),
+              "model_space": os.path.relpath(args.model_space or args.space), "configurations": len(ok), "seeds": args.seeds,
               "budget": args.budget, "best_ms": best}
     for name, lists in runs.items():
         stats = [_curve(d, best) for d in lists]
