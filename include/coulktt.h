@@ -98,8 +98,12 @@ typedef struct coul_tune {
     int unroll;       /* unroll of the atom loop; 0 and 1 mean none [INNER_UNROLL_FACTOR] */
     int atom_source;  /* COUL_ATOMS_*                          [USE_CONSTANT_MEMORY] */
     int precision;    /* COUL_PREC_* */
-    int rsqrt_soft;   /* of every 8 reciprocal square roots, how many run as FMA-pipe
-                         Newton iterations instead of on the MUFU unit (0 = all MUFU) */
+    int rsqrt_soft;   /* how many of every 8 point pairs a thread evaluates per atom take their
+                         reciprocal square root on the FMA pipe (Newton iterations) instead of the
+                         MUFU unit (0 = all MUFU).  A thread evaluates x_points * z_iterations points
+                         per atom in pairs; with n pairs, pair p is on the FMA pipe when (p % 8) <
+                         rsqrt_soft, so the share is rsqrt_soft / 8 for n = 8 or 16 and
+                         min(rsqrt_soft, n) / n below 8 pairs (e.g. 1 x 8 points: 2 -> 2 of 4) */
     int atom_split;   /* 0 or 1: one CTA per point tile; 2..8: a thread-block cluster of that many
                          CTAs shares each point tile, each streaming 1/atom_split of the atoms, the
                          partial sums reduced over distributed shared memory (for slices and small

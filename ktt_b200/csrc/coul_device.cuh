@@ -239,8 +239,9 @@ __device__ __forceinline__ float2 rsqrt_fma_x2(float2 x)
 // issue slot for two pairs.  The reciprocal square roots go to the MUFU unit one lane at a time,
 // or, for a static share of the lane pairs, to the FMA pipe (rsqrt_fma_x2).
 // ------------------------------------------------------------------------------------------
-// Static split between the MUFU unit and the FMA pipe: lane pair p uses the FMA pipe when
-// (p % 8) < SOFT.
+// Static split between the MUFU unit and the FMA pipe: lane pair p (of the x_points * z_iterations / 2
+// pairs a thread evaluates per atom) uses the FMA pipe when (p % 8) < SOFT -- a share of SOFT / 8 for
+// 8 or 16 pairs, min(SOFT, n) / n for n < 8 pairs.
 template <int SOFT>
 __device__ __forceinline__ constexpr bool pair_is_soft(int p)
 {

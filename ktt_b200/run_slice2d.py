@@ -1,6 +1,6 @@
 """The single-slice 2D case: one z slice of a 256 x 256 grid at 0.5 A, 4,000 atoms.
 
-    python -m ktt_b200.run_slice2d [--repeat 50]
+    python -m ktt_b200.run_slice2d [--repeat 50] [--only BX,BY,XP,ROWS,SPLIT,SOFT]
 
 Atoms x, y ~ U[0, 128), z ~ U[0, 32), q ~ U[-1, 1]; the slice at z = 16 A.  For each compiled 2D
 tile shape: device time of the slice kernel (median of --repeat event-timed launches), pair rate,
@@ -25,7 +25,10 @@ SHAPES = [(bx, by, xp, yi, split, soft) for (bx, by) in ((32, 4), (32, 2), (64, 
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--repeat", type=int, default=50)
+    ap.add_argument("--only", default="", help="one configuration: block x, block y, x points, rows, atom split, "
+                                               "rsqrt share (for profiling)")
     args = ap.parse_args()
+    shapes = [tuple(int(v) for v in args.only.split(","))] if args.only else SHAPES
 
     import torch
 
@@ -45,7 +48,7 @@ def main() -> None:
     d_sliced = ctx.slice_atoms(atoms, case.z_slice)
     out = torch.empty((ny, nx), dtype=torch.float32, device="cuda")
     results = []
-    for bx, by, xp, yi, split, soft in SHAPES:
+    for bx, by, xp, yi, split, soft in shapes:
         tune = ktt_b200.Tune(block_x=bx, block_y=by, x_points=xp, z_iterations=yi, atom_split=split,
                              rsqrt_soft=soft)
         if not ktt_b200.tune_supported_2d(tune):
