@@ -103,7 +103,9 @@ typedef struct coul_tune {
                          MUFU unit (0 = all MUFU).  A thread evaluates x_points * z_iterations points
                          per atom in pairs; with n pairs, pair p is on the FMA pipe when (p % 8) <
                          rsqrt_soft, so the share is rsqrt_soft / 8 for n = 8 or 16 and
-                         min(rsqrt_soft, n) / n below 8 pairs (e.g. 1 x 8 points: 2 -> 2 of 4) */
+                         min(rsqrt_soft, n) / n below 8 pairs (e.g. 1 x 8 points: 2 -> 2 of 4).
+                         10 + k (k = 0..7): consecutive atoms alternate between k and k + 1 of every
+                         8 pairs, a share of (2k + 1) / 16 for 8-pair tiles */
     int atom_split;   /* 0 or 1: one CTA per point tile; 2..8: a thread-block cluster of that many
                          CTAs shares each point tile, each streaming 1/atom_split of the atoms, the
                          partial sums reduced over distributed shared memory (for slices and small

@@ -33,7 +33,7 @@ MAP3D_SPACE = {
     "Z_ITERATIONS": [4, 8, 16],
     "X_POINTS": [1, 2, 4],
     "INNER_UNROLL_FACTOR": [0, 2, 4],
-    "RSQRT_SOFT": [0, 1, 2, 3],
+    "RSQRT_SOFT": [0, 1, 2, 3, 11, 12],
 }
 BATCH_SPACE = {
     "WORK_GROUP_SIZE_X": [4, 8, 16, 32],
@@ -41,7 +41,7 @@ BATCH_SPACE = {
     "Z_ITERATIONS": [4, 8, 16],
     "X_POINTS": [1, 2, 4],
     "INNER_UNROLL_FACTOR": [0, 2],
-    "RSQRT_SOFT": [0, 2],
+    "RSQRT_SOFT": [0, 2, 12],
 }
 
 

@@ -45,6 +45,9 @@ static const std::vector<BatchVariant>& batch_variants()
         // narrow x spans for small grids (less tile padding on 57..149-point rows)
         batch_variant<8, 1, 2, kPrecFp32, 2>(),      batch_variant<8, 1, 1, kPrecFp32, 2>(),
         batch_variant<8, 1, 2, kPrecFp32, 0>(),      batch_variant<4, 1, 2, kPrecFp32, 2>(),
+        // 5/16 of the rsqrts on the FMA pipe (atoms alternating between 2 and 3 of 8 lane pairs)
+        batch_variant<8, 2, 2, kPrecFp32, kSoftAlternate + 2>(),
+        batch_variant<8, 2, 1, kPrecFp32, kSoftAlternate + 2>(),
     };
     return v;
 }

@@ -173,8 +173,8 @@ int validate_tune(const coul_tune* t, int mode, int soa, const VariantEntry** ou
         return set_error(COUL_ERR_INVALID_ARGUMENT, "unknown atom_source");
     if (t->precision < COUL_PREC_FP32 || t->precision > COUL_PREC_FP64_MERGE)
         return set_error(COUL_ERR_INVALID_ARGUMENT, "unknown precision");
-    if (t->rsqrt_soft < 0 || t->rsqrt_soft > 8)
-        return set_error(COUL_ERR_INVALID_ARGUMENT, "rsqrt_soft must be in 0..8");
+    if (t->rsqrt_soft < 0 || (t->rsqrt_soft > 8 && t->rsqrt_soft < kSoftAlternate) || t->rsqrt_soft > kSoftAlternate + 7)
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "rsqrt_soft must be in 0..8 or 10..17");
     if (t->atom_split < 0 || t->atom_split > kMaxSplit)
         return set_error(COUL_ERR_INVALID_ARGUMENT, "atom_split must be in 0.." + std::to_string(kMaxSplit));
     const int split = t->atom_split >= 2 ? 1 : 0;

@@ -36,6 +36,12 @@ struct FwdLaunch {
     int split;      // atom-split form: CTAs per cluster sharing one point tile (0 / 1 = one CTA per tile)
 };
 
+// rsqrt_soft values from kSoftAlternate on: consecutive atoms alternate between k and k + 1 of every
+// 8 lane pairs on the FMA pipe, k = SOFT - kSoftAlternate, a share of (2k + 1) / 16 for 8-pair tiles.
+constexpr int kSoftAlternate = 10;
+constexpr int soft_even(int soft) { return soft >= kSoftAlternate ? soft - kSoftAlternate : soft; }
+constexpr int soft_odd(int soft) { return soft >= kSoftAlternate ? soft - kSoftAlternate + 1 : soft; }
+
 template <int MODE, int XP, int ZH, int SOFT>
 __device__ __forceinline__ void eval_atom(const float (&gx)[XP], float gy, const float2 (&gb)[ZH], float4 a,
                                           float2 (&dst)[XP][ZH])
@@ -190,9 +196,19 @@ __device__ __forceinline__ bool tile_accumulate(const FwdParams& p, const int x0
         (void)full;
         (void)gstage;
         const int n = static_cast<int>(p.n_atoms);
+        if constexpr (SOFT >= kSoftAlternate) {
+            int j = 0;
+            for (; j + 1 < n; j += 2) {
+                eval_atom<MODE, XP, ZH, soft_even(SOFT)>(gx, gy, gb, c_atoms[j], acc);
+                eval_atom<MODE, XP, ZH, soft_odd(SOFT)>(gx, gy, gb, c_atoms[j + 1], acc);
+            }
+            if (j < n)
+                eval_atom<MODE, XP, ZH, soft_even(SOFT)>(gx, gy, gb, c_atoms[j], acc);
+        } else {
 #pragma unroll UNR
-        for (int j = 0; j < n; ++j)
-            eval_atom<MODE, XP, ZH, SOFT>(gx, gy, gb, c_atoms[j], acc);
+            for (int j = 0; j < n; ++j)
+                eval_atom<MODE, XP, ZH, SOFT>(gx, gy, gb, c_atoms[j], acc);
+        }
     } else {
         const int nthreads = blockDim.x * blockDim.y;
         const int tid = threadIdx.y * blockDim.x + threadIdx.x;
@@ -283,16 +299,34 @@ __device__ __forceinline__ bool tile_accumulate(const FwdParams& p, const int x0
                     return make_float4(f[j], f[kTileAtoms + j], f[2 * kTileAtoms + j], f[3 * kTileAtoms + j]);
                 }
             };
+            // the stage is padded to kTileAtoms (an even count), so the alternating form pairs atoms
+            constexpr int kPairUnroll = UNR > 1 ? UNR / 2 : 1;
             if constexpr (PREC == kPrecFp32) {
+                if constexpr (SOFT >= kSoftAlternate) {
+#pragma unroll kPairUnroll
+                    for (int j = 0; j < kTileAtoms; j += 2) {
+                        eval_atom<MODE, XP, ZH, soft_even(SOFT)>(gx, gy, gb, atom_at(j), acc);
+                        eval_atom<MODE, XP, ZH, soft_odd(SOFT)>(gx, gy, gb, atom_at(j + 1), acc);
+                    }
+                } else {
 #pragma unroll UNR
-                for (int j = 0; j < kTileAtoms; ++j)
-                    eval_atom<MODE, XP, ZH, SOFT>(gx, gy, gb, atom_at(j), acc);
+                    for (int j = 0; j < kTileAtoms; ++j)
+                        eval_atom<MODE, XP, ZH, SOFT>(gx, gy, gb, atom_at(j), acc);
+                }
             } else {
                 for (int j0 = 0; j0 < kTileAtoms; j0 += kSubTile) {
                     clear_part();
+                    if constexpr (SOFT >= kSoftAlternate) {
+#pragma unroll kPairUnroll
+                        for (int j = 0; j < kSubTile; j += 2) {
+                            eval_atom<MODE, XP, ZH, soft_even(SOFT)>(gx, gy, gb, atom_at(j0 + j), part);
+                            eval_atom<MODE, XP, ZH, soft_odd(SOFT)>(gx, gy, gb, atom_at(j0 + j + 1), part);
+                        }
+                    } else {
 #pragma unroll UNR
-                    for (int j = 0; j < kSubTile; ++j)
-                        eval_atom<MODE, XP, ZH, SOFT>(gx, gy, gb, atom_at(j0 + j), part);
+                        for (int j = 0; j < kSubTile; ++j)
+                            eval_atom<MODE, XP, ZH, SOFT>(gx, gy, gb, atom_at(j0 + j), part);
+                    }
                     merge();
                 }
             }

@@ -1,6 +1,7 @@
 // Forward variants: 3D, float4 atoms through TMA-staged shared memory, with a static share of the
-// reciprocal square roots (SOFT of every 8 lane pairs) evaluated by Newton iterations on the FMA
-// pipe so the MUFU unit and the FMA pipe are both busy.  Plain FP32 accumulation (the compensated
+// reciprocal square roots (SOFT of every 8 lane pairs, or from kSoftAlternate on an alternation of two
+// neighbouring eighths over consecutive atoms) evaluated by Newton iterations on the FMA pipe so the
+// MUFU unit and the FMA pipe are both busy.  Plain FP32 accumulation (the compensated
 // and FP64-merge forms are in coul_fwd_3d_soft_precise.cu).
 #include "coul_forward.cuh"
 
@@ -31,6 +32,9 @@ static void add_soft_shares(std::vector<VariantEntry>& v)
     add_soft<PREC, 3>(v);
     add_soft<PREC, 4>(v);
     add_soft<PREC, 5>(v);
+    // alternating shares between the eighths: 3/16 and 5/16 of the lane pairs
+    add_soft<PREC, kSoftAlternate + 1>(v);
+    add_soft<PREC, kSoftAlternate + 2>(v);
 }
 
 void register_fwd_3d_soft(std::vector<VariantEntry>& v)

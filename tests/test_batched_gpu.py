@@ -18,6 +18,7 @@ def _small_batch(seed=21, n_mol=24, lo=50, hi=3000):
     ktt_b200.Tune(z_iterations=8, x_points=2, unroll=2, rsqrt_soft=2),
     ktt_b200.Tune(z_iterations=16, x_points=1, rsqrt_soft=2, block_x=64, block_y=2),
     ktt_b200.Tune(z_iterations=8, x_points=2, precision=ktt_b200.PREC_FP64_MERGE, rsqrt_soft=2),
+    ktt_b200.Tune(z_iterations=8, x_points=2, unroll=2, rsqrt_soft=12),
 ])
 def test_persistent_graph_and_separate_agree_bitwise(ctx, tune):
     import torch
