@@ -55,12 +55,13 @@ __global__ void __launch_bounds__(kAdjThreads) adjoint_kernel(const AdjParams p)
             ax[k] = ay[k] = az[k] = kPadCoord;  // far away; the result is never written
         }
     }
-    double acc[A][4];
+    // FP64 per-atom accumulators, touched once per row: kept in shared memory (component-major, so
+    // a warp's accesses fall on consecutive words) rather than in 2 * 4 * A registers per thread,
+    // which lets more warps share an SM to hide the pair loop's dependency latency
+    __shared__ double s_acc[A * 4][kAdjThreads];
 #pragma unroll
-    for (int k = 0; k < A; ++k)
-#pragma unroll
-        for (int c = 0; c < 4; ++c)
-            acc[k][c] = 0.0;
+    for (int c = 0; c < A * 4; ++c)
+        s_acc[c][tid] = 0.0;
 
     const int64_t rows = static_cast<int64_t>(p.ny) * p.nz;
     const int64_t r_begin = static_cast<int64_t>(blockIdx.y) * p.rows_per_chunk;
@@ -126,10 +127,10 @@ __global__ void __launch_bounds__(kAdjThreads) adjoint_kernel(const AdjParams p)
                 const float vq = l ? sq[m].y : sq[m].x;
                 const float vx = l ? sx[m].y : sx[m].x;
                 const float v3 = l ? s3[m].y : s3[m].x;
-                acc[k][0] += static_cast<double>(vq);
-                acc[k][1] += static_cast<double>(vx);
-                acc[k][2] += static_cast<double>(dy[k]) * static_cast<double>(v3);
-                acc[k][3] += static_cast<double>(dz[k]) * static_cast<double>(v3);
+                s_acc[4 * k + 0][tid] += static_cast<double>(vq);
+                s_acc[4 * k + 1][tid] += static_cast<double>(vx);
+                s_acc[4 * k + 2][tid] += static_cast<double>(dy[k]) * static_cast<double>(v3);
+                s_acc[4 * k + 3][tid] += static_cast<double>(dz[k]) * static_cast<double>(v3);
             }
         }
     }
@@ -141,7 +142,7 @@ __global__ void __launch_bounds__(kAdjThreads) adjoint_kernel(const AdjParams p)
             double* dst = p.partial + (static_cast<int64_t>(blockIdx.y) * p.n_atoms + j) * 4;
 #pragma unroll
             for (int c = 0; c < 4; ++c)
-                dst[c] = acc[k][c];
+                dst[c] = s_acc[4 * k + c][tid];
         }
     }
 }
