@@ -3,7 +3,8 @@
     python -m ktt_b200.run_searchers [--space tests/golden/b200_map3d_space_64.json] [--seeds 40] [--budget 120]
 
 The recorded search holds, for every configuration of a tuning space, its kernel time and KTT's
-default counters (tests/golden/make_b200_space.py).  Each searcher is replayed through the tuner's
+default counters: a compact recording (tests/golden/make_b200_space.py) or the KTT-format results file
+of `python -m ktt_b200.autotune ... --profile --results FILE`.  Each searcher is replayed through the tuner's
 SimulateTuning with that many seeds: random order (KTT's RandomSearcher, drawn here without
 replacement per seed), MCMC (KTT's McmcSearcher, seeded), and the profile-based searcher (KTT's
 algorithm, native) with a counter model trained by ktt_b200.profile_model (KTT's recipe: half of the
@@ -25,6 +26,25 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_SPACE = os.path.join(os.path.dirname(HERE), "tests", "golden", "b200_map3d_space_64.json")
+
+
+def load_space(path: str) -> dict:
+    """A compact recording (tests/golden/make_b200_space.py) or a KTT-format result file with counters."""
+    doc = json.load(open(path))
+    results = doc.get("Results", [])
+    if not results or "ComputationResults" not in results[0]:
+        return doc
+    first = next(r for r in results if r["ComputationResults"][0].get("ProfilingData"))
+    names = [c["Name"] for c in first["ComputationResults"][0]["ProfilingData"]["Counters"]]
+    compact = []
+    for r in results:
+        cr = r["ComputationResults"][0]
+        values = {c["Name"]: c["Value"] for c in cr.get("ProfilingData", {}).get("Counters", [])}
+        compact.append({"Configuration": [[p["Name"], p["Value"]] for p in r["Configuration"]], "Status": r["Status"],
+                        "Duration": cr["Duration"], "GlobalSize": [cr["GlobalSize"][k] for k in "XYZ"],
+                        "LocalSize": [cr["LocalSize"][k] for k in "XYZ"],
+                        "Counters": [values.get(n) for n in names]})
+    return {"Metadata": doc.get("Metadata", {}), "CounterNames": names, "Results": compact}
 
 
 def write_ktt_results(space: dict, path: str) -> None:
@@ -86,7 +106,7 @@ def main(argv=None) -> dict:
     from ktt_b200 import profile_model
     from ktt_b200 import pyktt as ktt
     ktt.Tuner.SetLoggingLevel(ktt.LoggingLevel.Error)
-    space = json.load(open(args.space))
+    space = load_space(args.space)
     ok = [r for r in space["Results"] if r["Status"] == "Ok"]
     best = min(r["Duration"] for r in ok)
     times = {tuple(v for _, v in r["Configuration"]): r["Duration"] for r in ok}
@@ -98,7 +118,7 @@ def main(argv=None) -> dict:
         training_path = results_path
         if args.model_space:
             training_path = os.path.join(tmp, "training.json")
-            write_ktt_results(json.load(open(args.model_space)), training_path)
+            write_ktt_results(load_space(args.model_space), training_path)
         profile_model.main([training_path, "--out", model_path, "--cc", args.cc, "--multiprocessors", str(args.sms)])
         model = ktt.CounterModel.Load(model_path)
 
