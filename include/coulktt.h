@@ -106,10 +106,12 @@ typedef struct coul_tune {
                          min(rsqrt_soft, n) / n below 8 pairs (e.g. 1 x 8 points: 2 -> 2 of 4).
                          10 + k (k = 0..7): consecutive atoms alternate between k and k + 1 of every
                          8 pairs, a share of (2k + 1) / 16 for 8-pair tiles */
-    int atom_split;   /* 0 or 1: one CTA per point tile; 2..8: a thread-block cluster of that many
+    int atom_split;   /* 0 or 1: one CTA per point tile; 2..16: a thread-block cluster of that many
                          CTAs shares each point tile, each streaming 1/atom_split of the atoms, the
                          partial sums reduced over distributed shared memory (for slices and small
-                         maps with too few tiles to fill the GPU; FP32, shared-memory atoms) */
+                         maps with too few tiles to fill the GPU; FP32, shared-memory atoms).  Above 8
+                         the cluster uses a non-portable size; a block too large for such a cluster
+                         is refused with COUL_ERR_DEVICE_LIMITS */
 } coul_tune;
 
 typedef struct coul_grid {

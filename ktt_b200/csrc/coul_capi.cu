@@ -246,6 +246,8 @@ int launch_forward(coul_ctx* ctx, const VariantEntry* v, const FwdParams& prm, i
                       ? 1
                       : 0;
     cudaError_t e = v->launch(L, ctx->stream);
+    if (e == cudaErrorLaunchOutOfResources)
+        return set_error(COUL_ERR_DEVICE_LIMITS, std::string("forward launch: ") + cudaGetErrorString(e));
     if (e != cudaSuccess)
         return cuda_error(e, "forward launch");
     return COUL_OK;

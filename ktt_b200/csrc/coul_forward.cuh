@@ -421,7 +421,8 @@ __global__ void __launch_bounds__(kMaxThreads) fwd_kernel(const FwdParams p, con
 // small 3D map): a thread-block cluster of S CTAs shares one point tile, CTA rank r takes the r-th
 // of S contiguous atom ranges through its own TMA ring, and rank 0 sums the S partial blocks from
 // the peers' shared memory in rank order (deterministic) and stores them.  The cluster size is a
-// launch-time choice (2..8, the portable cluster limit); plain FP32 accumulation, AoS atoms.
+// launch-time choice (2..8 portable, up to 16 with the B200's non-portable cluster sizes); plain FP32
+// accumulation, AoS atoms.
 template <int ZI, int XP, int UNR, int SOFT, int MODE>
 __global__ void __launch_bounds__(kMaxThreads) split_kernel(const FwdParams p, const int vec_ok)
 {
@@ -489,7 +490,10 @@ struct VariantKey {
     }
 };
 
-constexpr int kMaxSplit = 8;  // portable thread-block cluster size
+// Cluster sizes of the atom-split form: 2..8 are portable; 9..16 use the B200's non-portable
+// cluster sizes (opted into per kernel; refused with a device-limits error where the block does not fit).
+constexpr int kMaxPortableSplit = 8;
+constexpr int kMaxSplit = 16;
 
 // Dynamic shared memory of the atom-split form: the TMA ring, its barriers, the partial block.
 inline size_t split_smem_bytes(int threads, int values_per_thread)
@@ -572,6 +576,17 @@ cudaError_t launch_split(const FwdLaunch& L, cudaStream_t stream)
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
+    if (S > static_cast<unsigned>(kMaxPortableSplit)) {
+        cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        if (e != cudaSuccess)
+            return e;
+        int clusters = 0;
+        e = cudaOccupancyMaxActiveClusters(&clusters, kernel, &cfg);
+        if (e != cudaSuccess)
+            return e;
+        if (clusters < 1)
+            return cudaErrorLaunchOutOfResources;  // no SM group can hold such a cluster of these blocks
+    }
     return cudaLaunchKernelEx(&cfg, kernel, L.p, L.vec_store);
 }
 

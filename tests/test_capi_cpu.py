@@ -49,12 +49,12 @@ def test_tune_validation_without_device():
     t = T(block_x=0).c()
     assert lib.coul_tune_supported(ctypes.byref(t)) == ktt_b200.COUL_ERR_DEVICE_LIMITS
     assert b"block" in lib.coul_last_error()
-    # atom-split form: cluster sizes 2..8, FP32 shared-memory atoms only
+    # atom-split form: cluster sizes 2..16 (above 8 non-portable), FP32 shared-memory atoms only
     split = dict(z_iterations=8, x_points=2, rsqrt_soft=2)
-    for s in (2, 3, 5, 8):
+    for s in (2, 3, 5, 8, 9, 16):
         assert ktt_b200.tune_supported(T(atom_split=s, **split))
     assert ktt_b200.tune_supported(T(atom_split=1, z_iterations=16, x_points=4))  # 1 = off
-    assert not ktt_b200.tune_supported(T(atom_split=9, **split))
+    assert not ktt_b200.tune_supported(T(atom_split=17, **split))
     assert not ktt_b200.tune_supported(T(atom_split=-1, **split))
     assert not ktt_b200.tune_supported(T(atom_split=4, precision=ktt_b200.PREC_FP64_MERGE, **split))
     assert not ktt_b200.tune_supported(T(atom_split=4, z_iterations=4, x_points=1,
