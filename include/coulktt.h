@@ -240,9 +240,11 @@ typedef struct coul_nbody_tune {
     int block_x;           /* threads per block, a multiple of 32 up to 512      [WORK_GROUP_SIZE_X] */
     int bodies_per_thread; /* bodies i per thread in registers: 1, 2, 4 or 8     [OUTER_UNROLL_FACTOR] */
     int unroll;            /* unroll of the loop over bodies j: 1, 2 or 4        [INNER_UNROLL_FACTOR1] */
-    int j_split;           /* 0 / 1: one CTA per tile of bodies i; 2..8: a thread-block cluster of that
+    int j_split;           /* 0 / 1: one CTA per tile of bodies i; 2..16: a thread-block cluster of that
                               many CTAs shares the tile, each taking a share of the bodies j, partial
-                              accelerations reduced over distributed shared memory  [WORK_GROUP_SIZE_Y] */
+                              accelerations reduced over distributed shared memory; above 8 a
+                              non-portable cluster size, refused with COUL_ERR_DEVICE_LIMITS where the
+                              blocks do not fit such a cluster                  [WORK_GROUP_SIZE_Y] */
 } coul_nbody_tune;
 COUL_API int coul_nbody_tune_default(coul_nbody_tune* tune);
 COUL_API int coul_nbody_tune_supported(const coul_nbody_tune* tune);

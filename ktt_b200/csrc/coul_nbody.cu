@@ -39,7 +39,8 @@ struct NbodyParams {
 };
 
 constexpr int kNbodyMaxThreads = 512;
-constexpr int kNbodyMaxSplit = 8;
+constexpr int kNbodyMaxPortableSplit = 8;
+constexpr int kNbodyMaxSplit = 16;  // above 8 the B200's non-portable cluster sizes
 // dynamic shared memory: the TMA ring, its barriers, the transposed stage, the split's partial sums
 constexpr int kNbodySoaOffset = kStages * kTileAtoms * 16 + 16;
 constexpr int kNbodyRedOffset = kNbodySoaOffset + kTileAtoms * 16;
@@ -238,6 +239,17 @@ cudaError_t launch_nbody(const NbodyParams& p, dim3 grid, dim3 block, size_t sme
         attr[0].val.clusterDim.z = 1;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
+        if (split > kNbodyMaxPortableSplit) {
+            cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+            if (e != cudaSuccess)
+                return e;
+            int clusters = 0;
+            e = cudaOccupancyMaxActiveClusters(&clusters, kernel, &cfg);
+            if (e != cudaSuccess)
+                return e;
+            if (clusters < 1)
+                return cudaErrorLaunchOutOfResources;  // no SM group can hold such a cluster of these blocks
+        }
         return cudaLaunchKernelEx(&cfg, kernel, p);
     }
 }
@@ -284,7 +296,7 @@ int find_nbody(const coul_nbody_tune* t, const NbodyVariant** out)
                                                      std::to_string(kNbodyMaxThreads));
     if (t->j_split < 0)
         return set_error(COUL_ERR_INVALID_ARGUMENT, "j_split must not be negative");
-    if (t->j_split > kNbodyMaxSplit)  // beyond the portable cluster size: no compiled form
+    if (t->j_split > kNbodyMaxSplit)  // beyond the largest cluster: no form
         return set_error(COUL_ERR_UNSUPPORTED, "j_split above " + std::to_string(kNbodyMaxSplit) + " is not supported");
     if (t->block_x > nbody_max_threads(t->bodies_per_thread))
         return set_error(COUL_ERR_DEVICE_LIMITS, "8 bodies per thread allow at most 256 threads per block");
@@ -364,6 +376,8 @@ COUL_API int coul_nbody_step(coul_ctx* ctx, const float* d_pos_mass, const float
         return rc;
     cudaError_t e = v->launch(p, dim3(static_cast<unsigned>(tiles)), dim3(static_cast<unsigned>(tune->block_x)), smem, split,
                               ctx->stream);
+    if (e == cudaErrorLaunchOutOfResources)
+        return set_error(COUL_ERR_DEVICE_LIMITS, std::string("N-body launch: ") + cudaGetErrorString(e));
     if (e != cudaSuccess)
         return cuda_error(e, "N-body launch");
     return ctx_end_timing(ctx);

@@ -50,7 +50,7 @@ def test_nbody_matches_oracle(ctx, n, ti):
     assert np.abs(a.cpu().numpy()[:, :3].astype(np.float64) - ref_acc).max() <= 1e-5 * max(np.abs(ref_acc).max(), 1e-30)
 
 
-@pytest.mark.parametrize("split", [2, 3, 8])
+@pytest.mark.parametrize("split", [2, 3, 8, 16])
 def test_nbody_j_split(ctx, split):
     import torch
     pos, vel = _bodies(3001, seed=5)
