@@ -574,6 +574,118 @@ void TestNbodyExample()
     std::cout << "nbody: " << ok << " of " << results.size() << " configurations validated" << std::endl;
 }
 
+// Counters and KTT's profile-based searcher through the C++ surface: a profiled Run of one
+// configuration of this library's directCoulombSum tile space (64^3 map, 2,048 atoms) carries KTT's
+// default counters through SaveResults / LoadResults; then SetProfileBasedSearcher with the counter
+// model trained (ktt_b200/profile_model.py) from the B200 recording of the same space
+// (<work-dir>/b200_64.model.json) runs a search that reruns each batch's fastest with profiling.
+void TestProfileBasedSearcher()
+{
+    const int grid = 64;
+    const int n = 2048;
+    const float h = 0.5f;
+    const Atoms atoms = MakeAtoms(n, grid * h, 3);
+    ktt::Tuner tuner(0, 0, ktt::ComputeApi::CUDA);
+    tuner.SetGlobalSizeType(ktt::GlobalSizeType::CUDA);
+    const auto definition = tuner.AddKernelDefinition("directCoulombSum", "", ktt::DimensionVector(grid, grid, grid),
+        ktt::DimensionVector());
+    const auto kernel = tuner.CreateSimpleKernel("CoulombSum", definition);
+    const std::vector<std::pair<std::string, std::vector<uint64_t>>> space{{"WORK_GROUP_SIZE_X", {16, 32, 64, 128}},
+        {"WORK_GROUP_SIZE_Y", {1, 2, 4, 8}}, {"Z_ITERATIONS", {4, 8, 16}}, {"X_POINTS", {1, 2, 4}},
+        {"INNER_UNROLL_FACTOR", {0, 2, 4}}, {"RSQRT_SOFT", {0, 1, 2, 3}}, {"PRECISION", {0}}};
+
+    for (const auto& [name, values] : space)
+    {
+        tuner.AddParameter(kernel, name, values);
+    }
+
+    tuner.AddThreadModifier(kernel, {definition}, ktt::ModifierType::Local, ktt::ModifierDimension::X, "WORK_GROUP_SIZE_X",
+        ktt::ModifierAction::Multiply);
+    tuner.AddThreadModifier(kernel, {definition}, ktt::ModifierType::Local, ktt::ModifierDimension::Y, "WORK_GROUP_SIZE_Y",
+        ktt::ModifierAction::Multiply);
+    tuner.AddThreadModifier(kernel, {definition}, ktt::ModifierType::Global, ktt::ModifierDimension::X, "WORK_GROUP_SIZE_X",
+        ktt::ModifierAction::DivideCeil);
+    tuner.AddThreadModifier(kernel, {definition}, ktt::ModifierType::Global, ktt::ModifierDimension::Y, "WORK_GROUP_SIZE_Y",
+        ktt::ModifierAction::DivideCeil);
+    tuner.AddThreadModifier(kernel, {definition}, ktt::ModifierType::Global, ktt::ModifierDimension::Z, "Z_ITERATIONS",
+        ktt::ModifierAction::DivideCeil);
+    tuner.AddConstraint(kernel, {"WORK_GROUP_SIZE_X", "WORK_GROUP_SIZE_Y"},
+        [](const std::vector<uint64_t>& v) { return v[0] * v[1] >= 32 && v[0] * v[1] <= 256; });
+    // only the compiled variants
+    tuner.AddConstraint(kernel, {"WORK_GROUP_SIZE_X", "WORK_GROUP_SIZE_Y", "Z_ITERATIONS", "X_POINTS",
+        "INNER_UNROLL_FACTOR", "RSQRT_SOFT"}, [](const std::vector<uint64_t>& v)
+    {
+        coul_tune t;
+        coul_tune_default(&t);
+        t.block_x = static_cast<int>(v[0]);
+        t.block_y = static_cast<int>(v[1]);
+        t.z_iterations = static_cast<int>(v[2]);
+        t.x_points = static_cast<int>(v[3]);
+        t.unroll = v[4] <= 1 ? 1 : (v[4] < 4 ? 2 : 4);
+        t.rsqrt_soft = static_cast<int>(v[5]);
+        return coul_tune_supported(&t) == COUL_OK;
+    });
+
+    std::vector<float> energy(static_cast<size_t>(grid) * grid * grid, 0.0f);
+    const auto aos = tuner.AddArgumentVector(atoms.aos, ktt::ArgumentAccessType::ReadOnly);
+    const auto xs = tuner.AddArgumentVector(atoms.x, ktt::ArgumentAccessType::ReadOnly);
+    const auto ys = tuner.AddArgumentVector(atoms.y, ktt::ArgumentAccessType::ReadOnly);
+    const auto zs = tuner.AddArgumentVector(atoms.z, ktt::ArgumentAccessType::ReadOnly);
+    const auto ws = tuner.AddArgumentVector(atoms.w, ktt::ArgumentAccessType::ReadOnly);
+    const auto count = tuner.AddArgumentScalar(n);
+    const auto spacing = tuner.AddArgumentScalar(h);
+    const auto size = tuner.AddArgumentScalar(grid);
+    const auto out = tuner.AddArgumentVector(energy, ktt::ArgumentAccessType::WriteOnly);
+    tuner.SetArguments(definition, {aos, xs, ys, zs, ws, count, spacing, size, out});
+
+    // one profiled run
+    const auto configuration = tuner.CreateConfiguration(kernel, {{"WORK_GROUP_SIZE_X", uint64_t{32}},
+        {"WORK_GROUP_SIZE_Y", uint64_t{4}}, {"Z_ITERATIONS", uint64_t{8}}, {"X_POINTS", uint64_t{2}},
+        {"INNER_UNROLL_FACTOR", uint64_t{2}}, {"RSQRT_SOFT", uint64_t{2}}});
+    tuner.SetProfiling(true);
+    const auto profiled = tuner.Run(kernel, configuration, {});
+    tuner.SetProfiling(false);
+    CHECK(profiled.IsValid());
+    CHECK(!profiled.GetResults().empty() && profiled.GetResults()[0].HasProfilingData());
+
+    if (profiled.GetResults().empty() || !profiled.GetResults()[0].HasProfilingData())
+    {
+        return;
+    }
+
+    const auto& data = profiled.GetResults()[0].GetProfilingData();
+    CHECK(data.IsValid() && data.GetCounters().size() >= 30);
+    CHECK(data.HasCounter("smsp__inst_executed.sum") && data.GetCounter("smsp__inst_executed.sum").GetValueDouble() > 0.0);
+    CHECK(!data.HasCounter("smsp__inst_executed_pipe_fp16.sum"));  // not offered by GB100
+    CHECK(profiled.GetProfilingRunsOverhead() > 0);
+    const std::string file = workDir + "/profiled_run";
+    tuner.SaveResults({profiled}, file, ktt::OutputFormat::JSON);
+    const auto loaded = tuner.LoadResults(file + ".json", ktt::OutputFormat::JSON);
+    CHECK(loaded.size() == 1 && loaded[0].GetResults()[0].HasProfilingData());
+    CHECK(loaded.size() == 1 && loaded[0].GetResults()[0].GetProfilingData().GetCounters().size() == data.GetCounters().size());
+
+    // the profile-based searcher with the B200 model of this space
+    tuner.SetProfileBasedSearcher(kernel, workDir + "/b200_64.model.json", true, 5, 100, 10);
+    const auto results = tuner.Tune(kernel, std::make_unique<ktt::ConfigurationCount>(18));
+    CHECK(results.size() == 18);
+    std::vector<size_t> rerun;
+
+    for (size_t i = 0; i < results.size(); ++i)
+    {
+        CHECK(results[i].IsValid());
+
+        if (!results[i].GetResults().empty() && results[i].GetResults()[0].HasProfilingData())
+        {
+            rerun.push_back(i);
+        }
+    }
+
+    // batches of 5, each followed by a profiled rerun of its fastest
+    CHECK((rerun == std::vector<size_t>{5, 11, 17}));
+    CHECK(!tuner.GetProfiling());
+    std::cout << "profile-based: " << results.size() << " runs, profiled reruns at 5, 11, 17" << std::endl;
+}
+
 } // namespace
 
 int main(int argc, char** argv)
@@ -593,6 +705,7 @@ int main(int argc, char** argv)
         {"iterative_launcher", TestIterativeLauncher},
         {"user_buffers", TestUserDeviceBuffers},
         {"nbody_example", TestNbodyExample},
+        {"profile_based", TestProfileBasedSearcher},
     };
     const auto it = tests.find(argv[1]);
 

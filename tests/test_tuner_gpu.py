@@ -28,3 +28,14 @@ def gpu_tests_binary(tmp_path_factory):
 def test_tuner_gpu(gpu_tests_binary, workdir, name):  # noqa: F811
     r = subprocess.run([gpu_tests_binary, name, workdir], capture_output=True, text=True, timeout=900)
     assert r.returncode == 0, r.stdout[-4000:] + r.stderr[-4000:]
+
+
+def test_profile_based_searcher_cpp(gpu_tests_binary, tmp_path):
+    """Counters and the profile-based searcher from a C++ host program; the counter model is trained
+    from the B200 recording of the same tile space (tests/golden/b200_map3d_space_64.json)."""
+    from ktt_b200 import profile_model, run_searchers
+    space = run_searchers.load_space(os.path.join(REPO, "tests", "golden", "b200_map3d_space_64.json"))
+    run_searchers.write_ktt_results(space, str(tmp_path / "space.json"))
+    profile_model.main([str(tmp_path / "space.json"), "--out", str(tmp_path / "b200_64.model.json")])
+    r = subprocess.run([gpu_tests_binary, "profile_based", str(tmp_path)], capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stdout[-4000:] + r.stderr[-4000:]
