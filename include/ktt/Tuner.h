@@ -200,6 +200,8 @@ public:
     // Profiled runs collect hardware counters with CUPTI's range profiler: before the timed run the
     // kernel's whole execution (its launcher, or each definition) is replayed once per counter pass,
     // each time from reset arguments, and the counters are attached to the first ComputationResult.
+    // Where counters cannot be collected (no libcupti, profiling not permitted) runs go on without
+    // them after one warning.
     void SetProfiling(const bool flag);
     bool GetProfiling();
     // Counters to collect (names of CUPTI's metrics; ones the device does not offer are dropped with

@@ -1379,7 +1379,21 @@ KernelResult TunerCore::Run(const KernelId id, const KernelConfiguration& config
             // execution below and its validation see exactly one run (KTT repeats the whole tuning
             // iteration per pass: Source/TuningRunner/TuningRunner.cpp:40-53)
             const auto profilingStart = Clock::now();
-            profilingData = ProfileExecution(kernel, execute);
+
+            try
+            {
+                profilingData = ProfileExecution(kernel, execute);
+            }
+            catch (const std::exception& failure)
+            {
+                // no counters (no libcupti, profiling not permitted, ...): the run itself goes on
+                if (!m_ProfilingFailureReported)
+                {
+                    log::Warning(std::string("Profiling counters are not collected: ") + failure.what());
+                    m_ProfilingFailureReported = true;
+                }
+            }
+
             profilingOverhead = ElapsedNs(profilingStart);
         }
 

@@ -196,6 +196,7 @@ private:
     std::map<std::string, coul_batch*> m_Batches;
     std::vector<std::string> m_ProfilingCounters;  // empty: the default list
     std::set<std::string> m_UnsupportedCounters;   // reported once each
+    bool m_ProfilingFailureReported = false;
 
     void ResetWritableArguments(const KernelData& kernel);
     std::unique_ptr<KernelProfilingData> ProfileExecution(const KernelData& kernel,
