@@ -371,7 +371,28 @@ void Tuner::SaveResults(const std::vector<KernelResult>& results, const std::str
             for (const auto& cr : result.GetResults())
             {
                 out << "        <ComputationResult KernelFunction=\"" << cr.GetKernelFunction() << "\" Duration=\""
-                    << t(cr.GetDuration()) << "\" Overhead=\"" << t(cr.GetOverhead()) << "\"/>\n";
+                    << t(cr.GetDuration()) << "\" Overhead=\"" << t(cr.GetOverhead()) << "\"";
+
+                if (!cr.HasProfilingData())
+                {
+                    out << "/>\n";
+                    continue;
+                }
+
+                // Source/Output/XmlConverters.cpp:438-535: ProfilingData > Counters > Counter
+                const KernelProfilingData& profiling = cr.GetProfilingData();
+                out << ">\n          <ProfilingData RemainingProfilingRuns=\"" << profiling.GetRemainingProfilingRuns()
+                    << "\">\n            <Counters>\n";
+
+                for (const auto& counter : profiling.GetCounters())
+                {
+                    std::string value = CounterValueJson(counter);
+                    value = value == "null" ? "nan" : value;
+                    out << "              <Counter Name=\"" << counter.GetName() << "\" Type=\""
+                        << CounterTypeName(counter.GetType()) << "\" Value=\"" << value << "\"/>\n";
+                }
+
+                out << "            </Counters>\n          </ProfilingData>\n        </ComputationResult>\n";
             }
 
             out << "      </ComputationResults>\n    </Result>\n";

@@ -261,3 +261,18 @@ def test_b200_recording_and_study():
     for name in ("random", "mcmc", "profile"):
         assert 1.0 <= report[name]["best_ratio_after"][10] < 3.0
         assert report[name]["best_ratio_after"][80] <= report[name]["best_ratio_after"][10]
+
+
+def test_xml_results_carry_counters(recorded, tmp_path):
+    """KTT's XML output (Source/Output/XmlConverters.cpp:438-535): ProfilingData > Counters > Counter."""
+    import xml.etree.ElementTree as ET
+    path, _, g, _ = recorded
+    tuner = ktt.Tuner(0, 0, ktt.ComputeApi.CUDA)
+    loaded = tuner.LoadResults(path, ktt.OutputFormat.JSON)
+    tuner.SaveResults(loaded[:3], str(tmp_path / "out"), ktt.OutputFormat.XML)
+    root = ET.parse(tmp_path / "out.xml").getroot()
+    counters = root.findall("./Results/Result/ComputationResults/ComputationResult/ProfilingData/Counters")
+    assert len(counters) == 3
+    first = counters[0].findall("Counter")
+    assert [c.get("Name") for c in first] == g["CounterNames"]
+    assert float(first[0].get("Value")) == pytest.approx(g["Results"][0]["Counters"][0])
