@@ -324,6 +324,9 @@ def run_ours(args) -> None:
         line["cpu_baseline"] = {"value": cpu_value, "unit": UNIT, "cores": threads, "kind": "port",
                                 "sample": f"{len(idx)} seeded grid points x {w.atoms.shape[0]} atoms, FP64, "
                                           f"{cpu_s:.1f} s"}
+        kat = _reference_generator_rate()
+        if kat:
+            line["cpu_baseline"]["reference_generator"] = kat
         line["accuracy"] = {
             "chosen": errors.report(chosen_map.cpu().numpy().reshape(-1)[idx], ref, sumabs=sabs),
             "plain": errors.report(plain_map.cpu().numpy().reshape(-1)[idx], ref, sumabs=sabs),
@@ -335,6 +338,26 @@ def run_ours(args) -> None:
     if world > 1:
         torch.distributed.destroy_process_group()
 
+
+
+def _reference_generator_rate():
+    """Secondary CPU figure: KTT's own CPU code for this path, Examples/JSON/generate-coulomb-output.c
+    (FP32, one thread, the 256^3 x 64-atom known-answer map), compiled from the KTT tree by
+    `make -C oracle ref`; timed by wall clock around the process (its 64 MiB output file included).
+    None when the binary was not built."""
+    import tempfile
+    gen = os.path.join(REPO, "oracle", "_ref", "generate-coulomb-output")
+    if not os.access(gen, os.X_OK):
+        return None
+    with tempfile.TemporaryDirectory() as d:
+        t0 = time.perf_counter()
+        r = subprocess.run([gen], cwd=d, capture_output=True)
+        seconds = time.perf_counter() - t0
+    if r.returncode != 0:
+        return None
+    pairs = 256 ** 3 * 64
+    return {"value": pairs / seconds / 1e9, "unit": UNIT, "cores": 1, "kind": "reference",
+            "sample": f"Examples/JSON/generate-coulomb-output.c: 256^3 x 64 atoms, FP32, one thread, {seconds:.2f} s"}
 
 def main() -> None:
     ap = argparse.ArgumentParser()
