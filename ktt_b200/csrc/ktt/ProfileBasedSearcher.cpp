@@ -775,9 +775,20 @@ void ProfileBasedSearcher::ScoreAndSelect(const KernelResult& profiled)
     {
         std::set<size_t> chosen;
 
-        while (m_Batch.size() < m_BatchSize)
+        for (int draws = 0; m_Batch.size() < m_BatchSize; ++draws)
         {
-            const size_t index = profiling::WeightedRandomStep(score, m_Uniform(m_Generator));
+            size_t index = profiling::WeightedRandomStep(score, m_Uniform(m_Generator));
+
+            if (draws > 10000)
+            {
+                // never reached with scores of at least MinimumScore; keeps the loop finite regardless
+                index = 0;
+
+                while (chosen.count(index) != 0)
+                {
+                    ++index;
+                }
+            }
 
             if (chosen.insert(index).second)
             {
