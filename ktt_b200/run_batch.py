@@ -6,9 +6,10 @@
 512 molecules with atom counts log-uniform in [200, 20000] (seeded), atoms uniform in a cube of side
 (n / 0.1)^(1/3) A, grids = bounding box + `margin` A on every side at 0.5 A.  Prints one JSON line
 with the device time and pair rate of: one persistent launch, its CUDA-graph replay, one launch of
-the same kernel form per molecule, and one synchronous launch per molecule of KTT's kernel form
-(atoms in __constant__ memory, all rsqrts on MUFU, FP32; what a KTT user's per-molecule Tuner::Run
-loop launches).
+the same kernel form per molecule, one synchronous launch per molecule of KTT's kernel form (atoms
+in __constant__ memory, all rsqrts on MUFU, FP32; what a KTT user's per-molecule Tuner::Run loop
+launches), and one synchronous launch per molecule of KTT's plain reference kernel form
+(directCoulombSumReference: one point per thread, Examples/CoulombSum3d/CoulombSum3dReference.cu).
 
 The batched kernel's tile comes from `python -m ktt_b200.autotune batch` (KTT's searchers over the
 tuner's coulombBatch definition), stored under "batched"; --autotune-ktt-form searches the KTT-form
@@ -26,9 +27,10 @@ KTT_CTA_SHAPES = [(32, 4), (16, 8), (32, 8), (64, 4)]
 DEFAULT_TUNED = os.path.join(os.path.dirname(__file__), "tuned", "b200_batch.json")
 
 
-def _time_ktt_form(ctx, inputs, outs, tune, repeat):
+def _time_ktt_form(ctx, inputs, outs, tune, repeat, reference=False):
     """One forward call per molecule, synchronised after each, as Tuner::Run does; device time of
-    the whole loop from one event pair around it."""
+    the whole loop from one event pair around it.  With `reference`, the calls run the plain
+    one-point-per-thread reference kernel instead of the tiled kernel form `tune`."""
     import torch
     stream = torch.cuda.current_stream()
     best = float("inf")
@@ -36,7 +38,10 @@ def _time_ktt_form(ctx, inputs, outs, tune, repeat):
         start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         start.record(stream)
         for (atoms, dims, h, origin), out in zip(inputs, outs):
-            ctx.forward_3d(atoms, dims, h, origin, tune=tune, out=out)
+            if reference:
+                ctx.forward_3d_reference(atoms, dims, h, origin, out=out)
+            else:
+                ctx.forward_3d(atoms, dims, h, origin, tune=tune, out=out)
             ctx.synchronize()
         stop.record(stream)
         stop.synchronize()
@@ -116,8 +121,11 @@ def main() -> None:
         out[name] = {"ms": min(ms), "gpairs_per_s": batch.total_pairs / (min(ms) * 1e-3) / 1e9}
     ms = _time_ktt_form(ctx, inputs, outs, ktt_tune, args.repeat)
     out["ktt_form_separate"] = {"ms": ms, "gpairs_per_s": pairs / (ms * 1e-3) / 1e9}
+    ms = _time_ktt_form(ctx, inputs, outs, None, args.repeat, reference=True)
+    out["reference_separate"] = {"ms": ms, "gpairs_per_s": pairs / (ms * 1e-3) / 1e9}
     out["speedup_graph_vs_separate"] = out["separate"]["ms"] / out["graph"]["ms"]
     out["speedup_graph_vs_ktt_form"] = out["ktt_form_separate"]["ms"] / out["graph"]["ms"]
+    out["speedup_graph_vs_reference"] = out["reference_separate"]["ms"] / out["graph"]["ms"]
     print(json.dumps(out))
     batch.close()
     ctx.close()
