@@ -133,6 +133,24 @@ COUL_API void* coul_ctx_get_stream(coul_ctx* ctx);
 COUL_API void* coul_ctx_own_stream(coul_ctx* ctx);
 /* Number of SMs and compute capability of the context's device. */
 COUL_API int coul_ctx_device_info(coul_ctx* ctx, int* sm_count, int* cc_major, int* cc_minor);
+
+/* Properties of a CUDA device, without a context: what KTT's CUDA engine reads with
+   cuDeviceGetName / cuDeviceTotalMem / cuDeviceGetAttribute for its DeviceInfo
+   (Source/ComputeEngine/Cuda/CudaDevice.cpp:26-58) and cuDriverGetVersion for its PlatformInfo
+   (CudaEngine.cpp:696-707). */
+typedef struct coul_device_props {
+    char name[256];
+    uint64_t global_memory;        /* bytes */
+    uint64_t shared_memory_block;  /* bytes of shared memory per block without opt-in (KTT: local memory) */
+    uint64_t constant_memory;      /* bytes */
+    int max_threads_block;         /* KTT: maximum work-group size */
+    int sm_count;
+    int cc_major, cc_minor;
+    int driver_version;            /* cudaDriverGetVersion, e.g. 12090 */
+} coul_device_props;
+/* Number of CUDA devices (0 with no device or no driver: returns COUL_OK). */
+COUL_API int coul_device_count(int* count);
+COUL_API int coul_device_query(int device, coul_device_props* props);
 /* Wait for the context's stream; returns COUL_ERR_TIMEOUT if a kernel reported a bounded-wait expiry. */
 COUL_API int coul_synchronize(coul_ctx* ctx);
 /* Duration in ms between the events bracketing the most recent forward/adjoint/batched call

@@ -75,6 +75,7 @@ enum class ResultStatus { Ok, ComputationFailed, ValidationFailed, CompilationFa
 enum class TimeUnit { Nanoseconds, Microseconds, Milliseconds, Seconds };
 enum class OutputFormat { JSON, XML };
 enum class LoggingLevel { Off, Error, Warning, Info, Debug };
+enum class DeviceType { CPU, GPU, Custom };
 enum class ExceptionReason { General, CompilerError, DeviceLimitsExceeded };
 
 inline ValidationMode operator|(ValidationMode a, ValidationMode b)

@@ -43,26 +43,78 @@ namespace ktt
 
 class TunerCore;
 
+// Description of a compute device (Source/Api/Info/DeviceInfo.h); for CUDA devices filled as KTT's
+// CUDA engine fills it (CudaDevice.cpp:26-58).
 class KTT_API DeviceInfo
 {
 public:
+    explicit DeviceInfo(const DeviceIndex index, const std::string& name);
     DeviceInfo(const DeviceIndex index, const std::string& name, const uint64_t globalMemorySize, const uint32_t smCount,
         const uint32_t ccMajor, const uint32_t ccMinor);
     DeviceIndex GetIndex() const;
     const std::string& GetName() const;
+    const std::string& GetVendor() const;
+    const std::string& GetExtensions() const;
+    DeviceType GetDeviceType() const;
+    std::string GetDeviceTypeString() const;
     uint64_t GetGlobalMemorySize() const;
+    uint64_t GetLocalMemorySize() const;
+    uint64_t GetMaxConstantBufferSize() const;
+    uint64_t GetMaxWorkGroupSize() const;
     uint32_t GetMaxComputeUnits() const;
     uint32_t GetCudaComputeCapabilityMajor() const;
     uint32_t GetCudaComputeCapabilityMinor() const;
     std::string GetString() const;
 
+    void SetVendor(const std::string& vendor);
+    void SetExtensions(const std::string& extensions);
+    void SetDeviceType(const DeviceType deviceType);
+    void SetGlobalMemorySize(const uint64_t size);
+    void SetLocalMemorySize(const uint64_t size);
+    void SetMaxConstantBufferSize(const uint64_t size);
+    void SetMaxWorkGroupSize(const uint64_t size);
+    void SetMaxComputeUnits(const uint32_t units);
+    void SetCudaComputeCapabilityMajor(const uint32_t major);
+    void SetCudaComputeCapabilityMinor(const uint32_t minor);
+
 private:
     DeviceIndex m_Index;
     std::string m_Name;
-    uint64_t m_GlobalMemorySize;
-    uint32_t m_SmCount;
-    uint32_t m_CcMajor;
-    uint32_t m_CcMinor;
+    std::string m_Vendor;
+    std::string m_Extensions;
+    DeviceType m_DeviceType = DeviceType::GPU;
+    uint64_t m_GlobalMemorySize = 0;
+    uint64_t m_LocalMemorySize = 0;
+    uint64_t m_MaxConstantBufferSize = 0;
+    uint64_t m_MaxWorkGroupSize = 0;
+    uint32_t m_SmCount = 0;
+    uint32_t m_CcMajor = 0;
+    uint32_t m_CcMinor = 0;
+};
+
+// Description of a compute platform (Source/Api/Info/PlatformInfo.h); CUDA has one, "NVIDIA CUDA",
+// whose version is the driver's (CudaEngine.cpp:696-707).
+class KTT_API PlatformInfo
+{
+public:
+    explicit PlatformInfo(const PlatformIndex index, const std::string& name);
+    PlatformIndex GetIndex() const;
+    const std::string& GetName() const;
+    const std::string& GetVendor() const;
+    const std::string& GetVersion() const;
+    const std::string& GetExtensions() const;
+    std::string GetString() const;
+
+    void SetVendor(const std::string& vendor);
+    void SetVersion(const std::string& version);
+    void SetExtensions(const std::string& extensions);
+
+private:
+    PlatformIndex m_Index;
+    std::string m_Name;
+    std::string m_Vendor;
+    std::string m_Version;
+    std::string m_Extensions;
 };
 
 class KTT_API Tuner
@@ -180,6 +232,27 @@ public:
             &data, sizeof(T), customId);
     }
 
+    // Scalar of raw bytes (data type Custom).
+    ArgumentId AddArgumentScalar(const void* data, const size_t dataSize, const ArgumentId& customId = "");
+
+    // Local (CUDA: dynamic shared) memory of localMemorySize bytes; placed last in SetArguments.  The
+    // built-in kernels stage their operands in shared memory of their own, so such an argument is
+    // accepted and does not change a launch.
+    template <typename T>
+    ArgumentId AddArgumentLocal(const size_t localMemorySize, const ArgumentId& customId = "")
+    {
+        return AddSpecialArgument(sizeof(T), DeriveDataType<T>(), ArgumentMemoryType::Local, nullptr, localMemorySize,
+            "", customId);
+    }
+
+    // Value for a __constant__ variable named symbolName (CUDA); not a kernel function parameter.
+    template <typename T>
+    ArgumentId AddArgumentSymbol(const T& data, const ArgumentId& customId = "", const std::string& symbolName = "")
+    {
+        return AddSpecialArgument(sizeof(T), DeriveDataType<T>(), ArgumentMemoryType::Symbol, &data, sizeof(T), symbolName,
+            customId);
+    }
+
     // Vector argument read from a raw binary file, or generated by a script evaluated once per
     // element index (bound to "i") and converted to dataType.
     ArgumentId AddArgumentVectorFromFile(const std::string& filePath, const ArgumentDataType dataType, const size_t elementSize,
@@ -207,6 +280,10 @@ public:
     // Counters to collect (names of CUPTI's metrics; ones the device does not offer are dropped with
     // a warning); by default KTT's list plus the XU-pipe instruction count.
     void SetProfilingCounters(const std::vector<std::string>& counters);
+    // Definitions of a composite kernel whose computation results carry the counters (by default the
+    // first definition).  One counter set is collected per execution, over all of its launches, and
+    // attached to the first computation of the first of these definitions.
+    void SetProfiledDefinitions(const KernelId id, const std::vector<KernelDefinitionId>& definitionIds);
     void SetValidationMethod(const ValidationMethod method, const double toleranceThreshold);
     void SetValidationMode(const ValidationMode mode);
     void SetValidationRange(const ArgumentId& id, const size_t range);
@@ -253,6 +330,9 @@ public:
     void SetGlobalSizeType(const GlobalSizeType type);
     void SetAutomaticGlobalSizeCorrection(const bool flag);
     void SetKernelCacheCapacity(const uint64_t capacity);
+    // All platforms (CUDA: one) and the devices of one platform, as Tutorials/01ComputeApiInfo prints them.
+    std::vector<PlatformInfo> GetPlatformInfo() const;
+    std::vector<DeviceInfo> GetDeviceInfo(const PlatformIndex platform) const;
     DeviceInfo GetCurrentDeviceInfo() const;
 
     static void SetLoggingLevel(const LoggingLevel level);
@@ -268,6 +348,8 @@ private:
         const ArgumentId& customId);
     ArgumentId AddArgumentWithReferencedData(const size_t elementSize, const ArgumentDataType dataType,
         const ArgumentAccessType accessType, void* data, const size_t dataSize, const ArgumentId& customId);
+    ArgumentId AddSpecialArgument(const size_t elementSize, const ArgumentDataType dataType, const ArgumentMemoryType memoryType,
+        const void* data, const size_t dataSize, const std::string& symbolName, const ArgumentId& customId);
     ArgumentId AddUserArgument(ComputeBuffer buffer, const size_t elementSize, const ArgumentDataType dataType,
         const ArgumentAccessType accessType, const size_t bufferSize, const ArgumentId& customId);
     void AddParameterInternal(const KernelId id, const std::string& name, const std::vector<ParameterValue>& values,

@@ -366,6 +366,45 @@ COUL_API int coul_ctx_device_info(coul_ctx* ctx, int* sm_count, int* cc_major, i
     return COUL_OK;
 }
 
+COUL_API int coul_device_count(int* count)
+{
+    if (count == nullptr)
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "count is NULL");
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();  // no driver or no device: report zero devices
+        n = 0;
+    }
+    *count = n;
+    return COUL_OK;
+}
+
+COUL_API int coul_device_query(int device, coul_device_props* props)
+{
+    if (props == nullptr)
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "props is NULL");
+    int n = 0;
+    coul_device_count(&n);
+    if (device < 0 || device >= n)
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "no CUDA device with index " + std::to_string(device));
+    cudaDeviceProp p{};
+    cudaError_t e = cudaGetDeviceProperties(&p, device);
+    if (e != cudaSuccess)
+        return cuda_error(e, "cudaGetDeviceProperties");
+    std::memset(props, 0, sizeof(*props));
+    std::snprintf(props->name, sizeof(props->name), "%s", p.name);
+    props->global_memory = static_cast<uint64_t>(p.totalGlobalMem);
+    props->shared_memory_block = static_cast<uint64_t>(p.sharedMemPerBlock);
+    props->constant_memory = static_cast<uint64_t>(p.totalConstMem);
+    props->max_threads_block = p.maxThreadsPerBlock;
+    props->sm_count = p.multiProcessorCount;
+    props->cc_major = p.major;
+    props->cc_minor = p.minor;
+    if ((e = cudaDriverGetVersion(&props->driver_version)) != cudaSuccess)
+        return cuda_error(e, "cudaDriverGetVersion");
+    return COUL_OK;
+}
+
 COUL_API int coul_synchronize(coul_ctx* ctx)
 {
     if (ctx == nullptr)

@@ -52,7 +52,9 @@ void GuardedVoid(F&& f)
 
 } // namespace
 
-// ---- DeviceInfo ---------------------------------------------------------------------------------
+// ---- DeviceInfo, PlatformInfo ---------------------------------------------------------------------
+
+DeviceInfo::DeviceInfo(const DeviceIndex index, const std::string& name) : m_Index(index), m_Name(name) {}
 
 DeviceInfo::DeviceInfo(const DeviceIndex index, const std::string& name, const uint64_t globalMemorySize, const uint32_t smCount,
     const uint32_t ccMajor, const uint32_t ccMinor) :
@@ -62,15 +64,79 @@ DeviceInfo::DeviceInfo(const DeviceIndex index, const std::string& name, const u
 
 DeviceIndex DeviceInfo::GetIndex() const { return m_Index; }
 const std::string& DeviceInfo::GetName() const { return m_Name; }
+const std::string& DeviceInfo::GetVendor() const { return m_Vendor; }
+const std::string& DeviceInfo::GetExtensions() const { return m_Extensions; }
+DeviceType DeviceInfo::GetDeviceType() const { return m_DeviceType; }
 uint64_t DeviceInfo::GetGlobalMemorySize() const { return m_GlobalMemorySize; }
+uint64_t DeviceInfo::GetLocalMemorySize() const { return m_LocalMemorySize; }
+uint64_t DeviceInfo::GetMaxConstantBufferSize() const { return m_MaxConstantBufferSize; }
+uint64_t DeviceInfo::GetMaxWorkGroupSize() const { return m_MaxWorkGroupSize; }
 uint32_t DeviceInfo::GetMaxComputeUnits() const { return m_SmCount; }
 uint32_t DeviceInfo::GetCudaComputeCapabilityMajor() const { return m_CcMajor; }
 uint32_t DeviceInfo::GetCudaComputeCapabilityMinor() const { return m_CcMinor; }
 
+std::string DeviceInfo::GetDeviceTypeString() const
+{
+    switch (m_DeviceType)
+    {
+    case DeviceType::CPU:
+        return "CPU";
+    case DeviceType::GPU:
+        return "GPU";
+    default:
+        return "Custom";
+    }
+}
+
+// The same fields, labels and order as KTT's DeviceInfo::GetString (DeviceInfo.cpp:96-113).
 std::string DeviceInfo::GetString() const
 {
-    return "Device " + std::to_string(m_Index) + ": " + m_Name + ", compute units " + std::to_string(m_SmCount)
-        + ", compute capability " + std::to_string(m_CcMajor) + "." + std::to_string(m_CcMinor);
+    std::string result;
+    result += "Information about device with index: " + std::to_string(m_Index) + "\n";
+    result += "Name: " + m_Name + "\n";
+    result += "Vendor: " + m_Vendor + "\n";
+    result += "Device type: " + GetDeviceTypeString() + "\n";
+    result += "Global memory size: " + std::to_string(m_GlobalMemorySize) + "\n";
+    result += "Local memory size: " + std::to_string(m_LocalMemorySize) + "\n";
+    result += "Maximum constant buffer size: " + std::to_string(m_MaxConstantBufferSize) + "\n";
+    result += "Maximum work-group size: " + std::to_string(m_MaxWorkGroupSize) + "\n";
+    result += "Maximum parallel compute units: " + std::to_string(m_SmCount) + "\n";
+    result += "Extensions: " + m_Extensions + "\n";
+    result += "CUDA compute capability: " + std::to_string(m_CcMajor) + "." + std::to_string(m_CcMinor) + "\n";
+    return result;
+}
+
+void DeviceInfo::SetVendor(const std::string& vendor) { m_Vendor = vendor; }
+void DeviceInfo::SetExtensions(const std::string& extensions) { m_Extensions = extensions; }
+void DeviceInfo::SetDeviceType(const DeviceType deviceType) { m_DeviceType = deviceType; }
+void DeviceInfo::SetGlobalMemorySize(const uint64_t size) { m_GlobalMemorySize = size; }
+void DeviceInfo::SetLocalMemorySize(const uint64_t size) { m_LocalMemorySize = size; }
+void DeviceInfo::SetMaxConstantBufferSize(const uint64_t size) { m_MaxConstantBufferSize = size; }
+void DeviceInfo::SetMaxWorkGroupSize(const uint64_t size) { m_MaxWorkGroupSize = size; }
+void DeviceInfo::SetMaxComputeUnits(const uint32_t units) { m_SmCount = units; }
+void DeviceInfo::SetCudaComputeCapabilityMajor(const uint32_t major) { m_CcMajor = major; }
+void DeviceInfo::SetCudaComputeCapabilityMinor(const uint32_t minor) { m_CcMinor = minor; }
+
+PlatformInfo::PlatformInfo(const PlatformIndex index, const std::string& name) : m_Index(index), m_Name(name) {}
+PlatformIndex PlatformInfo::GetIndex() const { return m_Index; }
+const std::string& PlatformInfo::GetName() const { return m_Name; }
+const std::string& PlatformInfo::GetVendor() const { return m_Vendor; }
+const std::string& PlatformInfo::GetVersion() const { return m_Version; }
+const std::string& PlatformInfo::GetExtensions() const { return m_Extensions; }
+void PlatformInfo::SetVendor(const std::string& vendor) { m_Vendor = vendor; }
+void PlatformInfo::SetVersion(const std::string& version) { m_Version = version; }
+void PlatformInfo::SetExtensions(const std::string& extensions) { m_Extensions = extensions; }
+
+// KTT's PlatformInfo::GetString layout (PlatformInfo.cpp:36-47).
+std::string PlatformInfo::GetString() const
+{
+    std::string result;
+    result += "Information about platform with index: " + std::to_string(m_Index) + "\n";
+    result += "Name: " + m_Name + "\n";
+    result += "Vendor: " + m_Vendor + "\n";
+    result += "Compute API version: " + m_Version + "\n";
+    result += "Extensions: " + m_Extensions + "\n";
+    return result;
 }
 
 // ---- Tuner ------------------------------------------------------------------------------------
@@ -512,6 +578,48 @@ ArgumentId Tuner::AddArgumentWithOwnedData(const size_t elementSize, const Argum
     }, InvalidArgumentId);
 }
 
+ArgumentId Tuner::AddArgumentScalar(const void* data, const size_t dataSize, const ArgumentId& customId)
+{
+    if (data == nullptr || dataSize == 0)
+    {
+        log::Error("Scalar argument data must not be empty");
+        return InvalidArgumentId;
+    }
+
+    return AddArgumentWithOwnedData(dataSize, ArgumentDataType::Custom, ArgumentMemoryType::Scalar, ArgumentAccessType::ReadOnly,
+        data, dataSize, customId);
+}
+
+ArgumentId Tuner::AddSpecialArgument(const size_t elementSize, const ArgumentDataType dataType,
+    const ArgumentMemoryType memoryType, const void* data, const size_t dataSize, const std::string& symbolName,
+    const ArgumentId& customId)
+{
+    return Guarded([&]
+    {
+        if (dataSize == 0)
+        {
+            throw std::runtime_error(memoryType == ArgumentMemoryType::Local ? "Local memory size must be positive"
+                : "Symbol argument data must not be empty");
+        }
+
+        ArgumentData argument;
+        argument.dataType = dataType;
+        argument.memoryType = memoryType;
+        argument.accessType = ArgumentAccessType::ReadOnly;
+        argument.ownership = ArgumentOwnership::Owned;
+        argument.elementSize = elementSize;
+        argument.bytes = dataSize;
+        argument.symbolName = symbolName;
+
+        if (data != nullptr)
+        {
+            argument.owned.assign(static_cast<const uint8_t*>(data), static_cast<const uint8_t*>(data) + dataSize);
+        }
+
+        return m_Core->AddArgument(std::move(argument), customId);
+    }, InvalidArgumentId);
+}
+
 ArgumentId Tuner::AddArgumentWithReferencedData(const size_t elementSize, const ArgumentDataType dataType,
     const ArgumentAccessType accessType, void* data, const size_t dataSize, const ArgumentId& customId)
 {
@@ -561,6 +669,11 @@ void Tuner::SetProfiling(const bool flag) { m_Core->SetProfiling(flag); }
 void Tuner::SetProfilingCounters(const std::vector<std::string>& counters)
 {
     GuardedVoid([&] { m_Core->SetProfilingCounters(counters); });
+}
+
+void Tuner::SetProfiledDefinitions(const KernelId id, const std::vector<KernelDefinitionId>& definitionIds)
+{
+    GuardedVoid([&] { m_Core->SetProfiledDefinitions(id, definitionIds); });
 }
 
 bool Tuner::GetProfiling() { return m_Core->GetProfiling(); }
@@ -722,6 +835,16 @@ void Tuner::SetCompilerOptions(const std::string& options, [[maybe_unused]] cons
 void Tuner::SetGlobalSizeType(const GlobalSizeType type) { m_Core->SetGlobalSizeType(type); }
 void Tuner::SetAutomaticGlobalSizeCorrection([[maybe_unused]] const bool flag) {}
 void Tuner::SetKernelCacheCapacity([[maybe_unused]] const uint64_t capacity) {}
+
+std::vector<PlatformInfo> Tuner::GetPlatformInfo() const
+{
+    return Guarded([&] { return m_Core->GetPlatformInfo(); }, std::vector<PlatformInfo>{});
+}
+
+std::vector<DeviceInfo> Tuner::GetDeviceInfo(const PlatformIndex platform) const
+{
+    return Guarded([&] { return m_Core->GetDeviceInfo(platform); }, std::vector<DeviceInfo>{});
+}
 
 DeviceInfo Tuner::GetCurrentDeviceInfo() const
 {

@@ -308,12 +308,60 @@ void TunerCore::Synchronize()
     }
 }
 
+// KTT's CUDA device description (CudaDevice.cpp:26-58) from the C ABI's property query.
+DeviceInfo TunerCore::QueryDevice(const DeviceIndex index)
+{
+    coul_device_props props{};
+    CheckCoul(coul_device_query(static_cast<int>(index), &props), "device query");
+    DeviceInfo info(index, props.name);
+    info.SetVendor("NVIDIA Corporation");
+    info.SetExtensions("N/A");
+    info.SetDeviceType(DeviceType::GPU);
+    info.SetGlobalMemorySize(props.global_memory);
+    info.SetLocalMemorySize(props.shared_memory_block);
+    info.SetMaxConstantBufferSize(props.constant_memory);
+    info.SetMaxWorkGroupSize(static_cast<uint64_t>(props.max_threads_block));
+    info.SetMaxComputeUnits(static_cast<uint32_t>(props.sm_count));
+    info.SetCudaComputeCapabilityMajor(static_cast<uint32_t>(props.cc_major));
+    info.SetCudaComputeCapabilityMinor(static_cast<uint32_t>(props.cc_minor));
+    return info;
+}
+
 DeviceInfo TunerCore::GetDeviceInfo()
 {
-    int sm = 0, major = 0, minor = 0;
-    CheckCoul(coul_ctx_device_info(Context(), &sm, &major, &minor), "device info");
-    return DeviceInfo(m_Device, "NVIDIA sm_" + std::to_string(major) + std::to_string(minor) + " (" + std::to_string(sm) + " SMs)",
-        0, static_cast<uint32_t>(sm), static_cast<uint32_t>(major), static_cast<uint32_t>(minor));
+    Context();  // the tuner's device must be usable
+    return QueryDevice(m_Device);
+}
+
+std::vector<DeviceInfo> TunerCore::GetDeviceInfo(const PlatformIndex platform)
+{
+    if (platform != 0)
+    {
+        throw std::runtime_error("CUDA has one platform, index 0; requested " + std::to_string(platform));
+    }
+
+    int count = 0;
+    CheckCoul(coul_device_count(&count), "device count");
+    std::vector<DeviceInfo> result;
+
+    for (int i = 0; i < count; ++i)
+    {
+        result.push_back(QueryDevice(static_cast<DeviceIndex>(i)));
+    }
+
+    return result;
+}
+
+std::vector<PlatformInfo> TunerCore::GetPlatformInfo()
+{
+    int count = 0;
+    CheckCoul(coul_device_count(&count), "device count");
+    coul_device_props props{};
+    PlatformInfo info(0, "NVIDIA CUDA");
+    info.SetVendor("NVIDIA Corporation");
+    info.SetVersion(count > 0 && coul_device_query(0, &props) == COUL_OK ? std::to_string(props.driver_version) : "N/A");
+    info.SetExtensions("N/A");
+    return {info};
 }
 
 std::string TunerCore::DeviceName()
@@ -741,7 +789,21 @@ Nanoseconds TunerCore::LaunchDefinition(const KernelData& kernel, const KernelDe
 {
     (void)kernel;
     const DefinitionData& definition = Definition(id);
-    const auto& args = definition.arguments;
+    // Local (shared-memory size) and symbol (__constant__ variable) arguments are not kernel function
+    // parameters in KTT's CUDA engine (Tuner.h:488-510: local ones go last in SetArguments); the
+    // built-in kernels take neither, so they are dropped before the argument list is matched.
+    std::vector<ArgumentId> args;
+
+    for (const auto& a : definition.arguments)
+    {
+        const ArgumentMemoryType type = Argument(a).memoryType;
+
+        if (type != ArgumentMemoryType::Local && type != ArgumentMemoryType::Symbol)
+        {
+            args.push_back(a);
+        }
+    }
+
     coul_ctx* ctx = Context();
 
     auto parameter = [&](const char* name, const int64_t fallback) -> int64_t
@@ -1262,6 +1324,26 @@ void TunerCore::SetProfilingCounters(const std::vector<std::string>& counters)
     m_ProfilingCounters = counters;
 }
 
+void TunerCore::SetProfiledDefinitions(const KernelId id, const std::vector<KernelDefinitionId>& definitionIds)
+{
+    KernelData& kernel = Kernel(id);
+
+    if (definitionIds.empty())
+    {
+        throw std::runtime_error("Number of profiled definitions must be greater than zero");
+    }
+
+    for (const auto definition : definitionIds)
+    {
+        if (std::find(kernel.definitions.cbegin(), kernel.definitions.cend(), definition) == kernel.definitions.cend())
+        {
+            throw std::runtime_error("Definition " + std::to_string(definition) + " is not part of kernel " + kernel.name);
+        }
+    }
+
+    kernel.profiledDefinitions = definitionIds;
+}
+
 std::unique_ptr<KernelProfilingData> TunerCore::ProfileExecution(const KernelData& kernel,
     const std::function<std::vector<ComputationResult>()>& execute)
 {
@@ -1402,7 +1484,14 @@ KernelResult TunerCore::Run(const KernelId id, const KernelConfiguration& config
 
         if (profilingData && !computations.empty())
         {
-            computations.front().SetProfilingData(std::move(profilingData));
+            // the counters go to the first computation of a profiled definition (by default the
+            // kernel's first definition), else to the first computation
+            const KernelDefinitionId profiled = kernel.profiledDefinitions.empty() ? kernel.definitions.front()
+                : kernel.profiledDefinitions.front();
+            const std::string& function = Definition(profiled).name;
+            auto target = std::find_if(computations.begin(), computations.end(),
+                [&function](const ComputationResult& c) { return c.GetKernelFunction() == function; });
+            (target == computations.end() ? computations.front() : *target).SetProfilingData(std::move(profilingData));
         }
     }
     catch (const RunFailure& failure)

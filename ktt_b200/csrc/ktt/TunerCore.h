@@ -57,6 +57,7 @@ struct KernelData
     std::vector<KernelConstraintInfo> constraints;
     std::vector<ModifierData> modifiers;
     KernelLauncher launcher;
+    std::vector<KernelDefinitionId> profiledDefinitions;  // empty: the first definition
     std::unique_ptr<Searcher> searcher;
     std::unique_ptr<ConfigurationSpace> space;
     bool searcherActive = false;
@@ -75,7 +76,8 @@ struct ArgumentData
     std::vector<uint8_t> owned;      // owned host copy (vectors and scalars)
     void* referenced = nullptr;      // caller's host memory (referenced vectors)
     void* userDevice = nullptr;      // caller's device buffer (user vectors)
-    size_t bytes = 0;
+    size_t bytes = 0;                // data bytes; for local arguments the shared-memory size
+    std::string symbolName;          // symbol arguments: the __constant__ variable's name
     void* device = nullptr;          // framework device buffer
     size_t deviceBytes = 0;
     bool deviceCurrent = false;      // device copy matches the host data
@@ -147,12 +149,16 @@ public:
     coul_ctx* Context();
     void Synchronize();
     DeviceInfo GetDeviceInfo();
+    std::vector<DeviceInfo> GetDeviceInfo(const PlatformIndex platform);
+    std::vector<PlatformInfo> GetPlatformInfo();
+    static DeviceInfo QueryDevice(const DeviceIndex index);
     std::string DeviceName();
     void SetGlobalSizeType(const GlobalSizeType type) { m_GlobalSizeType = type; }
     GlobalSizeType GetGlobalSizeType() const { return m_GlobalSizeType; }
     void SetProfiling(const bool flag) { m_Profiling = flag; }
     bool GetProfiling() const { return m_Profiling; }
     void SetProfilingCounters(const std::vector<std::string>& counters);
+    void SetProfiledDefinitions(const KernelId id, const std::vector<KernelDefinitionId>& definitionIds);
     static const std::vector<std::string>& DefaultProfilingCounters();
     void SetCompilerOptions(const std::string& options) { m_CompilerOptions = options; }
     ComputeApi GetApi() const { return m_Api; }

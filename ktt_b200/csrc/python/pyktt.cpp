@@ -65,6 +65,22 @@ void BindScalarArgument(C& tuner, const char* name)
 }
 
 template <typename T, typename C>
+void BindLocalArgument(C& tuner, const char* name)
+{
+    tuner.def(name, [](ktt::Tuner& t, const size_t size, const ktt::ArgumentId& customId) { return t.AddArgumentLocal<T>(size, customId); },
+        py::arg("localMemorySize"), py::arg("customId") = ktt::ArgumentId());
+}
+
+// Keyword names as KTT's module gives them (data, symbolName, customId), each passed to its C++ meaning.
+template <typename T, typename C>
+void BindSymbolArgument(C& tuner, const char* name)
+{
+    tuner.def(name, [](ktt::Tuner& t, const T value, const std::string& symbolName, const ktt::ArgumentId& customId)
+        { return t.AddArgumentSymbol<T>(value, customId, symbolName); },
+        py::arg("data"), py::arg("symbolName") = std::string(), py::arg("customId") = ktt::ArgumentId());
+}
+
+template <typename T, typename C>
 void BindScalarUpdate(C& ci, const char* name)
 {
     ci.def(name, [](ktt::ComputeInterface& c, const ktt::ArgumentId& id, const T value) { c.UpdateScalarArgument(id, &value); });
@@ -114,6 +130,11 @@ PYBIND11_MODULE(pyktt, m)
     py::enum_<ktt::KernelRunMode>(m, "KernelRunMode")
         .value("Running", ktt::KernelRunMode::Running).value("OfflineTuning", ktt::KernelRunMode::OfflineTuning)
         .value("OnlineTuning", ktt::KernelRunMode::OnlineTuning).value("ResultValidation", ktt::KernelRunMode::ResultValidation);
+    py::enum_<ktt::DeviceType>(m, "DeviceType")
+        .value("CPU", ktt::DeviceType::CPU)
+        .value("GPU", ktt::DeviceType::GPU)
+        .value("Custom", ktt::DeviceType::Custom);
+
     py::enum_<ktt::LoggingLevel>(m, "LoggingLevel")
         .value("Off", ktt::LoggingLevel::Off).value("Error", ktt::LoggingLevel::Error).value("Warning", ktt::LoggingLevel::Warning)
         .value("Info", ktt::LoggingLevel::Info).value("Debug", ktt::LoggingLevel::Debug);
@@ -200,14 +221,45 @@ PYBIND11_MODULE(pyktt, m)
         .def("__repr__", &ktt::KernelConfiguration::GetString);
 
     py::class_<ktt::DeviceInfo>(m, "DeviceInfo")
+        .def(py::init<const ktt::DeviceIndex, const std::string&>())
         .def("GetIndex", &ktt::DeviceInfo::GetIndex)
         .def("GetName", &ktt::DeviceInfo::GetName)
+        .def("GetVendor", &ktt::DeviceInfo::GetVendor)
+        .def("GetExtensions", &ktt::DeviceInfo::GetExtensions)
+        .def("GetDeviceType", &ktt::DeviceInfo::GetDeviceType)
+        .def("GetDeviceTypeString", &ktt::DeviceInfo::GetDeviceTypeString)
         .def("GetGlobalMemorySize", &ktt::DeviceInfo::GetGlobalMemorySize)
+        .def("GetLocalMemorySize", &ktt::DeviceInfo::GetLocalMemorySize)
+        .def("GetMaxConstantBufferSize", &ktt::DeviceInfo::GetMaxConstantBufferSize)
+        .def("GetMaxWorkGroupSize", &ktt::DeviceInfo::GetMaxWorkGroupSize)
         .def("GetMaxComputeUnits", &ktt::DeviceInfo::GetMaxComputeUnits)
-        .def("GetCUDAComputeCapabilityMajor", &ktt::DeviceInfo::GetCudaComputeCapabilityMajor)
-        .def("GetCUDAComputeCapabilityMinor", &ktt::DeviceInfo::GetCudaComputeCapabilityMinor)
+        .def("GetCudaComputeCapabilityMajor", &ktt::DeviceInfo::GetCudaComputeCapabilityMajor)
+        .def("GetCudaComputeCapabilityMinor", &ktt::DeviceInfo::GetCudaComputeCapabilityMinor)
         .def("GetString", &ktt::DeviceInfo::GetString)
+        .def("SetVendor", &ktt::DeviceInfo::SetVendor)
+        .def("SetExtensions", &ktt::DeviceInfo::SetExtensions)
+        .def("SetDeviceType", &ktt::DeviceInfo::SetDeviceType)
+        .def("SetGlobalMemorySize", &ktt::DeviceInfo::SetGlobalMemorySize)
+        .def("SetLocalMemorySize", &ktt::DeviceInfo::SetLocalMemorySize)
+        .def("SetMaxConstantBufferSize", &ktt::DeviceInfo::SetMaxConstantBufferSize)
+        .def("SetMaxWorkGroupSize", &ktt::DeviceInfo::SetMaxWorkGroupSize)
+        .def("SetMaxComputeUnits", &ktt::DeviceInfo::SetMaxComputeUnits)
+        .def("SetCudaComputeCapabilityMajor", &ktt::DeviceInfo::SetCudaComputeCapabilityMajor)
+        .def("SetCudaComputeCapabilityMinor", &ktt::DeviceInfo::SetCudaComputeCapabilityMinor)
         .def("__repr__", &ktt::DeviceInfo::GetString);
+
+    py::class_<ktt::PlatformInfo>(m, "PlatformInfo")
+        .def(py::init<const ktt::PlatformIndex, const std::string&>())
+        .def("GetIndex", &ktt::PlatformInfo::GetIndex)
+        .def("GetName", &ktt::PlatformInfo::GetName)
+        .def("GetVendor", &ktt::PlatformInfo::GetVendor)
+        .def("GetVersion", &ktt::PlatformInfo::GetVersion)
+        .def("GetExtensions", &ktt::PlatformInfo::GetExtensions)
+        .def("GetString", &ktt::PlatformInfo::GetString)
+        .def("SetVendor", &ktt::PlatformInfo::SetVendor)
+        .def("SetVersion", &ktt::PlatformInfo::SetVersion)
+        .def("SetExtensions", &ktt::PlatformInfo::SetExtensions)
+        .def("__repr__", &ktt::PlatformInfo::GetString);
 
     // The caller's buffer must outlive the descriptor's use in Run / TuneIteration (as in KTT).
     py::class_<ktt::BufferOutputDescriptor>(m, "BufferOutputDescriptor")
@@ -494,10 +546,23 @@ PYBIND11_MODULE(pyktt, m)
     BindScalarArgument<int64_t>(tuner, "AddArgumentScalarLong");
     BindScalarArgument<float>(tuner, "AddArgumentScalarFloat");
     BindScalarArgument<double>(tuner, "AddArgumentScalarDouble");
+    BindLocalArgument<int8_t>(tuner, "AddArgumentLocalChar");
+    BindLocalArgument<int16_t>(tuner, "AddArgumentLocalShort");
+    BindLocalArgument<int32_t>(tuner, "AddArgumentLocalInt");
+    BindLocalArgument<int64_t>(tuner, "AddArgumentLocalLong");
+    BindLocalArgument<float>(tuner, "AddArgumentLocalFloat");
+    BindLocalArgument<double>(tuner, "AddArgumentLocalDouble");
+    BindSymbolArgument<int8_t>(tuner, "AddArgumentSymbolChar");
+    BindSymbolArgument<int16_t>(tuner, "AddArgumentSymbolShort");
+    BindSymbolArgument<int32_t>(tuner, "AddArgumentSymbolInt");
+    BindSymbolArgument<int64_t>(tuner, "AddArgumentSymbolLong");
+    BindSymbolArgument<float>(tuner, "AddArgumentSymbolFloat");
+    BindSymbolArgument<double>(tuner, "AddArgumentSymbolDouble");
 
     tuner.def("Run", &ktt::Tuner::Run, py::call_guard<py::gil_scoped_release>())
         .def("SetProfiling", &ktt::Tuner::SetProfiling)
         .def("SetProfilingCounters", &ktt::Tuner::SetProfilingCounters)
+        .def("SetProfiledDefinitions", &ktt::Tuner::SetProfiledDefinitions)
         .def("GetProfiling", &ktt::Tuner::GetProfiling)
         .def("SetValidationMethod", &ktt::Tuner::SetValidationMethod)
         .def("SetValidationMode", &ktt::Tuner::SetValidationMode)
@@ -552,6 +617,8 @@ PYBIND11_MODULE(pyktt, m)
         .def("SetGlobalSizeType", &ktt::Tuner::SetGlobalSizeType)
         .def("SetAutomaticGlobalSizeCorrection", &ktt::Tuner::SetAutomaticGlobalSizeCorrection)
         .def("SetKernelCacheCapacity", &ktt::Tuner::SetKernelCacheCapacity)
+        .def("GetPlatformInfo", &ktt::Tuner::GetPlatformInfo)
+        .def("GetDeviceInfo", &ktt::Tuner::GetDeviceInfo)
         .def("GetCurrentDeviceInfo", &ktt::Tuner::GetCurrentDeviceInfo)
         .def_static("SetLoggingLevel", &ktt::Tuner::SetLoggingLevel)
         .def_static("GetLoggingLevel", &ktt::Tuner::GetLoggingLevel)

@@ -125,6 +125,46 @@ def test_invalid_ids_and_arguments():
     assert g != ktt.InvalidArgumentId
 
 
+def test_platform_and_device_info_without_a_device():
+    """Tutorials/01ComputeApiInfo: one CUDA platform; with no device (this machine) an empty device
+    list, and KTT's GetString layout for both descriptions."""
+    tuner = ktt.Tuner(0, 0, ktt.ComputeApi.CUDA)
+    platforms = tuner.GetPlatformInfo()
+    assert len(platforms) == 1
+    p = platforms[0]
+    assert (p.GetIndex(), p.GetName(), p.GetVendor()) == (0, "NVIDIA CUDA", "NVIDIA Corporation")
+    assert p.GetString().splitlines() == [
+        "Information about platform with index: 0", "Name: NVIDIA CUDA", "Vendor: NVIDIA Corporation",
+        f"Compute API version: {p.GetVersion()}", "Extensions: N/A"]
+    assert tuner.GetDeviceInfo(0) == []
+    assert tuner.GetDeviceInfo(3) == []  # no such platform: logged, empty
+    d = ktt.DeviceInfo(2, "B200")
+    d.SetVendor("NVIDIA Corporation")
+    d.SetDeviceType(ktt.DeviceType.GPU)
+    d.SetGlobalMemorySize(1 << 30)
+    d.SetMaxWorkGroupSize(1024)
+    d.SetMaxComputeUnits(148)
+    d.SetCudaComputeCapabilityMajor(10)
+    lines = d.GetString().splitlines()
+    assert lines[0] == "Information about device with index: 2" and "Device type: GPU" in lines
+    assert "Maximum work-group size: 1024" in lines and "Maximum parallel compute units: 148" in lines
+    assert lines[-1] == "CUDA compute capability: 10.0"
+
+
+def test_local_symbol_arguments_and_profiled_definitions():
+    tuner = ktt.Tuner(0, 0, ktt.ComputeApi.CUDA)
+    assert tuner.AddArgumentLocalFloat(1024, "lm") == "lm"
+    assert tuner.AddArgumentLocalFloat(0) == ktt.InvalidArgumentId
+    assert tuner.AddArgumentSymbolInt(7, symbolName="cSize", customId="sym") == "sym"
+    d1, k = _space(tuner)
+    d2 = tuner.AddKernelDefinition("second", "", ktt.DimensionVector(16), ktt.DimensionVector(16))
+    tuner.SetProfiledDefinitions(k, [d1])  # part of the kernel: accepted silently
+    tuner.SetProfiledDefinitions(k, [d2])  # not part of it: logged, kept as before
+    c = tuner.CreateCompositeKernel("pair", [d1, d2])
+    tuner.SetProfiledDefinitions(c, [d2])
+    tuner.SetArguments(d1, ["lm"])  # local memory goes last; the argument list is accepted
+
+
 def test_tuning_loader_from_python(tmp_path, recorded):
     path, _, best = recorded
     shutil.copy(os.path.join(GOLDEN, "ktt_scripts", "CoulombSum3dCudaScript.json"), tmp_path)

@@ -67,3 +67,51 @@ def test_coulomb3d_python_host_program():
     result = tuner.Run(k, best, [ktt.BufferOutputDescriptor(grid_id, out)])
     assert result.GetStatus() == ktt.ResultStatus.Ok
     assert errors.report(out, reference)["rel_norm"] <= 1e-5
+
+
+def test_device_info_and_local_symbol_arguments():
+    """Tutorials/01ComputeApiInfo on the B200, and a CoulombSum3d definition whose argument list ends
+    in a local-memory and a symbol argument (neither is a CUDA function parameter in KTT's CUDA
+    engine): it still maps onto the built-in kernel and validates."""
+    tuner = ktt.Tuner(0, 0, ktt.ComputeApi.CUDA)
+    devices = tuner.GetDeviceInfo(0)
+    assert devices and devices[0].GetCudaComputeCapabilityMajor() == 10
+    current = tuner.GetCurrentDeviceInfo()
+    assert current.GetName() == devices[0].GetName() and current.GetMaxComputeUnits() >= 100
+    assert current.GetMaxWorkGroupSize() == 1024 and current.GetGlobalMemorySize() > (64 << 30)
+    assert current.GetDeviceTypeString() == "GPU" and "CUDA compute capability: 10." in current.GetString()
+    assert int(tuner.GetPlatformInfo()[0].GetVersion()) >= 12000
+
+    grid, n, h = 32, 96, 0.5
+    rng = np.random.default_rng(5)
+    atoms = np.empty((n, 4), dtype=np.float32)
+    atoms[:, :3] = rng.uniform(0.0, grid * h, (n, 3))
+    atoms[:, 3] = rng.uniform(-1.0, 1.0, n)
+    reference = oracle.grid3d(atoms, h, (grid, grid, grid)).astype(np.float32).reshape(-1)
+    tuner.SetGlobalSizeType(ktt.GlobalSizeType.CUDA)
+    d = tuner.AddKernelDefinition("directCoulombSum", "", ktt.DimensionVector(grid, grid, grid), ktt.DimensionVector())
+    k = tuner.CreateSimpleKernel("CoulombSum", d)
+    ro = ktt.ArgumentAccessType.ReadOnly
+    args = [tuner.AddArgumentVectorFloat(atoms.reshape(-1), ro)]
+    args += [tuner.AddArgumentVectorFloat(np.ascontiguousarray(atoms[:, c]), ro) for c in range(4)]
+    args += [tuner.AddArgumentScalarInt(n), tuner.AddArgumentScalarFloat(h), tuner.AddArgumentScalarInt(grid)]
+    grid_id = tuner.AddArgumentVectorFloat(np.zeros(grid ** 3, dtype=np.float32), ktt.ArgumentAccessType.WriteOnly)
+    args += [grid_id, tuner.AddArgumentSymbolInt(grid, symbolName="cGridSize"), tuner.AddArgumentLocalFloat(4096)]
+    tuner.SetArguments(d, args)
+    for name, value in (("WORK_GROUP_SIZE_X", 32), ("WORK_GROUP_SIZE_Y", 4), ("WORK_GROUP_SIZE_Z", 1),
+                        ("Z_ITERATIONS", 8), ("INNER_UNROLL_FACTOR", 2), ("USE_CONSTANT_MEMORY", 0), ("USE_SOA", 0),
+                        ("VECTOR_SIZE", 1)):
+        tuner.AddParameter(k, name, [value])
+    for dim, name in ((ktt.ModifierDimension.X, "WORK_GROUP_SIZE_X"), (ktt.ModifierDimension.Y, "WORK_GROUP_SIZE_Y")):
+        tuner.AddThreadModifier(k, [d], ktt.ModifierType.Local, dim, name, ktt.ModifierAction.Multiply)
+        tuner.AddThreadModifier(k, [d], ktt.ModifierType.Global, dim, name, ktt.ModifierAction.DivideCeil)
+    tuner.AddThreadModifier(k, [d], ktt.ModifierType.Global, ktt.ModifierDimension.Z, "Z_ITERATIONS",
+                            ktt.ModifierAction.DivideCeil)
+
+    def compute_reference(buffer):
+        np.frombuffer(buffer, dtype=np.float32)[:] = reference
+
+    tuner.SetReferenceComputation(grid_id, grid ** 3 * 4, compute_reference)
+    tuner.SetValidationMethod(ktt.ValidationMethod.SideBySideComparison, 0.01)
+    results = tuner.Tune(k)
+    assert len(results) == 1 and results[0].GetStatus() == ktt.ResultStatus.Ok, str(results[0].GetStatus())
