@@ -5,6 +5,7 @@
 // include/coulktt.h) instead of KTT's libktt.so.
 #pragma once
 
+#include <ktt/ComputeApiInitializer.h>
 #include <ktt/ComputeInterface.h>
 #include <ktt/Configuration.h>
 #include <ktt/ConfigurationSpace.h>

@@ -125,12 +125,21 @@ typedef struct coul_ctx coul_ctx;
 /* ---- context ------------------------------------------------------------ */
 COUL_API int coul_ctx_create(int device, coul_ctx** ctx);
 COUL_API int coul_ctx_destroy(coul_ctx* ctx);
+/* A context on the caller's own CUDA context (a CUcontext, passed as void*) instead of the device's
+   primary context: every later call of this context makes cu_context current on the calling thread.
+   `stream` (a CUstream of that context, or NULL for a stream of its own) is where calls are
+   enqueued.  The caller keeps ownership of both and destroys them after coul_ctx_destroy.  Replaces
+   KTT's CUDA engine set-up from a ComputeApiInitializer (Source/ComputeEngine/Cuda/CudaEngine.cpp:67-106,
+   Source/Api/ComputeApiInitializer.h:26). */
+COUL_API int coul_ctx_create_on(void* cu_context, void* stream, coul_ctx** ctx);
 /* Enqueue every later call of this context on the given cudaStream_t (passed as void*).  NULL is
    the legacy default stream (PyTorch's default stream), not a private one.  A new context starts
    on a non-blocking stream of its own, returned by coul_ctx_own_stream. */
 COUL_API int coul_ctx_set_stream(coul_ctx* ctx, void* stream);
 COUL_API void* coul_ctx_get_stream(coul_ctx* ctx);
 COUL_API void* coul_ctx_own_stream(coul_ctx* ctx);
+/* Index of the context's CUDA device. */
+COUL_API int coul_ctx_device(coul_ctx* ctx, int* device);
 /* Number of SMs and compute capability of the context's device. */
 COUL_API int coul_ctx_device_info(coul_ctx* ctx, int* sm_count, int* cc_major, int* cc_minor);
 

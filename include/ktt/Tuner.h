@@ -31,6 +31,7 @@
 #include <type_traits>
 #include <vector>
 
+#include <ktt/ComputeApiInitializer.h>
 #include <ktt/ComputeInterface.h>
 #include <ktt/Configuration.h>
 #include <ktt/ConfigurationSpace.h>
@@ -123,6 +124,10 @@ public:
     explicit Tuner(const PlatformIndex platform, const DeviceIndex device, const ComputeApi api);
     explicit Tuner(const PlatformIndex platform, const DeviceIndex device, const ComputeApi api,
         const uint32_t computeQueueCount);
+    // On the caller's CUDA context and streams (Tutorials/05ComputeApiInitializer); the queues get ids
+    // 0, 1, ... in the initializer's order, also returned in assignedQueueIds.
+    explicit Tuner(const ComputeApi api, const ComputeApiInitializer& initializer);
+    explicit Tuner(const ComputeApi api, const ComputeApiInitializer& initializer, std::vector<QueueId>& assignedQueueIds);
     ~Tuner();
 
     // ---- kernels --------------------------------------------------------------------------
@@ -323,6 +328,14 @@ public:
     std::vector<KernelResult> LoadResults(const std::string& filePath, const OutputFormat format, UserData& data) const;
 
     // ---- queues, device, compiler and logging ----------------------------------------------
+    // Queues of a tuner created from a ComputeApiInitializer: another of the caller's streams, or one
+    // removed again (the last one stays); without an initializer the tuner has queue 0 only.
+    QueueId AddComputeQueue(ComputeQueue queue);
+    void RemoveComputeQueue(const QueueId id);
+    // Compute and transfer actions complete before the call that started them returns, so these only
+    // wait for the device.
+    void WaitForComputeAction(const ComputeActionId id);
+    void WaitForTransferAction(const TransferActionId id);
     void SynchronizeQueue(const QueueId id);
     void SynchronizeQueues();
     void SynchronizeDevice();

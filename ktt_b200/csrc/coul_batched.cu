@@ -225,7 +225,7 @@ COUL_API int coul_batch_destroy(coul_batch* batch)
     if (batch == nullptr)
         return COUL_OK;
     if (batch->ctx)
-        cudaSetDevice(batch->ctx->device);
+        ctx_activate(batch->ctx);
     if (batch->ctx && batch->ctx->stream)
         cudaStreamSynchronize(batch->ctx->stream);
     batch_release(batch);

@@ -132,8 +132,36 @@ int cuda_error(cudaError_t e, const char* what)
     return set_error(COUL_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+// cuCtxSetCurrent from the driver, through the runtime's entry-point query (no link to libcuda).
+using CtxSetCurrentFn = int (*)(void*);
+
+CtxSetCurrentFn ctx_set_current_fn()
+{
+    static CtxSetCurrentFn fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult status{};
+        if (cudaGetDriverEntryPoint("cuCtxSetCurrent", &p, cudaEnableDefault, &status) != cudaSuccess ||
+            status != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            p = nullptr;
+        }
+        return reinterpret_cast<CtxSetCurrentFn>(p);
+    }();
+    return fn;
+}
+
 int ctx_activate(coul_ctx* ctx)
 {
+    if (ctx->user_context != nullptr) {
+        // the caller's context, made current on this thread; the runtime calls below then use it
+        const CtxSetCurrentFn set_current = ctx_set_current_fn();
+        if (set_current == nullptr)
+            return set_error(COUL_ERR_CUDA, "cuCtxSetCurrent is not available from the driver");
+        const int r = set_current(ctx->user_context);
+        if (r != 0)
+            return set_error(COUL_ERR_CUDA, "cuCtxSetCurrent failed with driver error " + std::to_string(r));
+        return COUL_OK;
+    }
     cudaError_t e = cudaSetDevice(ctx->device);
     if (e != cudaSuccess)
         return cuda_error(e, "cudaSetDevice");
@@ -274,6 +302,36 @@ COUL_API const char* coul_status_string(int status)
     }
 }
 
+namespace {
+
+// Device check and per-context resources, with the context's CUDA context already current.
+int ctx_init(coul_ctx* ctx, int device)
+{
+    cudaDeviceProp prop{};
+    cudaError_t e = cudaGetDeviceProperties(&prop, device);
+    if (e != cudaSuccess)
+        return cuda_error(e, "cudaGetDeviceProperties");
+    if (prop.major != 10 || prop.minor != 0)
+        return set_error(COUL_ERR_NO_DEVICE, std::string("libcoulktt is built for sm_100a only; device is ") +
+                                                 prop.name + " (sm_" + std::to_string(prop.major) +
+                                                 std::to_string(prop.minor) + ")");
+    ctx->device = device;
+    ctx->sm_count = prop.multiProcessorCount;
+    ctx->cc_major = prop.major;
+    ctx->cc_minor = prop.minor;
+    if ((e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreate(&ctx->ev_start)) != cudaSuccess || (e = cudaEventCreate(&ctx->ev_stop)) != cudaSuccess ||
+        (e = cudaMalloc(&ctx->d_status, sizeof(int))) != cudaSuccess ||
+        (e = cudaMemset(ctx->d_status, 0, sizeof(int))) != cudaSuccess)
+        return cuda_error(e, "context set-up");
+    if (ctx->stream == nullptr)
+        ctx->stream = ctx->own_stream;
+    (void)registry();
+    return COUL_OK;
+}
+
+}  // namespace
+
 COUL_API int coul_ctx_create(int device, coul_ctx** out)
 {
     if (out == nullptr)
@@ -286,32 +344,42 @@ COUL_API int coul_ctx_create(int device, coul_ctx** out)
                                                  (e != cudaSuccess ? cudaGetErrorString(e) : "count is 0"));
     if (device < 0 || device >= count)
         return set_error(COUL_ERR_NO_DEVICE, "device index out of range");
-    cudaDeviceProp prop{};
-    e = cudaGetDeviceProperties(&prop, device);
-    if (e != cudaSuccess)
-        return cuda_error(e, "cudaGetDeviceProperties");
-    if (prop.major != 10 || prop.minor != 0)
-        return set_error(COUL_ERR_NO_DEVICE, std::string("libcoulktt is built for sm_100a only; device is ") +
-                                                 prop.name + " (sm_" + std::to_string(prop.major) +
-                                                 std::to_string(prop.minor) + ")");
     e = cudaSetDevice(device);
     if (e != cudaSuccess)
         return cuda_error(e, "cudaSetDevice");
     auto* ctx = new coul_ctx();
-    ctx->device = device;
-    ctx->sm_count = prop.multiProcessorCount;
-    ctx->cc_major = prop.major;
-    ctx->cc_minor = prop.minor;
-    if ((e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking)) != cudaSuccess ||
-        (e = cudaEventCreate(&ctx->ev_start)) != cudaSuccess || (e = cudaEventCreate(&ctx->ev_stop)) != cudaSuccess ||
-        (e = cudaMalloc(&ctx->d_status, sizeof(int))) != cudaSuccess ||
-        (e = cudaMemset(ctx->d_status, 0, sizeof(int))) != cudaSuccess) {
-        const int rc = cuda_error(e, "context set-up");
+    const int rc = ctx_init(ctx, device);
+    if (rc) {
         coul_ctx_destroy(ctx);
         return rc;
     }
-    ctx->stream = ctx->own_stream;
-    (void)registry();
+    *out = ctx;
+    return COUL_OK;
+}
+
+COUL_API int coul_ctx_create_on(void* cu_context, void* stream, coul_ctx** out)
+{
+    if (out == nullptr || cu_context == nullptr)
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "NULL CUDA context or ctx output pointer");
+    *out = nullptr;
+    auto* ctx = new coul_ctx();
+    ctx->user_context = cu_context;
+    ctx->stream = static_cast<cudaStream_t>(stream);
+    int rc = ctx_activate(ctx);
+    int device = -1;
+    if (rc == COUL_OK) {
+        const cudaError_t e = cudaGetDevice(&device);  // the device of the current (the caller's) context
+        if (e != cudaSuccess)
+            rc = cuda_error(e, "cudaGetDevice");
+    }
+    if (rc == COUL_OK)
+        rc = ctx_init(ctx, device);
+    if (rc) {
+        if (device < 0)
+            ctx->user_context = nullptr;  // nothing was created in it
+        coul_ctx_destroy(ctx);
+        return rc;
+    }
     *out = ctx;
     return COUL_OK;
 }
@@ -320,7 +388,7 @@ COUL_API int coul_ctx_destroy(coul_ctx* ctx)
 {
     if (ctx == nullptr)
         return COUL_OK;
-    cudaSetDevice(ctx->device);
+    ctx_activate(ctx);
     if (ctx->stream)
         cudaStreamSynchronize(ctx->stream);
     if (ctx->d_atoms_cache)
@@ -352,6 +420,14 @@ COUL_API int coul_ctx_set_stream(coul_ctx* ctx, void* stream)
 COUL_API void* coul_ctx_get_stream(coul_ctx* ctx) { return ctx ? static_cast<void*>(ctx->stream) : nullptr; }
 
 COUL_API void* coul_ctx_own_stream(coul_ctx* ctx) { return ctx ? static_cast<void*>(ctx->own_stream) : nullptr; }
+
+COUL_API int coul_ctx_device(coul_ctx* ctx, int* device)
+{
+    if (ctx == nullptr || device == nullptr)
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "ctx or device is NULL");
+    *device = ctx->device;
+    return COUL_OK;
+}
 
 COUL_API int coul_ctx_device_info(coul_ctx* ctx, int* sm_count, int* cc_major, int* cc_minor)
 {

@@ -12,6 +12,7 @@
 
 struct coul_ctx {
     int device = 0;
+    void* user_context = nullptr;  // the caller's CUcontext (coul_ctx_create_on), else the primary context
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;  // the stream every call of this context is enqueued on
     cudaEvent_t ev_start = nullptr; // bracket the most recent timed call

@@ -148,7 +148,27 @@ Tuner::Tuner([[maybe_unused]] const PlatformIndex platform, const DeviceIndex de
     m_Core(std::make_unique<TunerCore>(device, api))
 {}
 
+Tuner::Tuner(const ComputeApi api, const ComputeApiInitializer& initializer) :
+    m_Core(std::make_unique<TunerCore>(0, api))
+{
+    std::vector<QueueId> ignored;
+    m_Core->AdoptContext(initializer, ignored);
+}
+
+Tuner::Tuner(const ComputeApi api, const ComputeApiInitializer& initializer, std::vector<QueueId>& assignedQueueIds) :
+    m_Core(std::make_unique<TunerCore>(0, api))
+{
+    m_Core->AdoptContext(initializer, assignedQueueIds);
+}
+
 Tuner::~Tuner() = default;
+
+ComputeApiInitializer::ComputeApiInitializer(ComputeContext context, const std::vector<ComputeQueue>& queues) :
+    m_Context(context), m_Queues(queues)
+{}
+
+ComputeContext ComputeApiInitializer::GetContext() const { return m_Context; }
+const std::vector<ComputeQueue>& ComputeApiInitializer::GetQueues() const { return m_Queues; }
 
 KernelDefinitionId Tuner::AddKernelDefinition(const std::string& name, const std::string& source, const DimensionVector& globalSize,
     const DimensionVector& localSize, const std::vector<std::string>& typeNames)
@@ -824,8 +844,27 @@ std::string Tuner::GetKernelDefinitionSource(const KernelDefinitionId id, const 
     return Guarded([&] { return m_Core->GetDefinitionSource(id, configuration); }, std::string());
 }
 
-void Tuner::SynchronizeQueue([[maybe_unused]] const QueueId id) { GuardedVoid([&] { m_Core->Synchronize(); }); }
-void Tuner::SynchronizeQueues() { GuardedVoid([&] { m_Core->Synchronize(); }); }
+QueueId Tuner::AddComputeQueue(ComputeQueue queue)
+{
+    return Guarded([&] { return m_Core->AddQueue(queue); }, InvalidQueueId);
+}
+
+void Tuner::RemoveComputeQueue(const QueueId id) { GuardedVoid([&] { m_Core->RemoveQueue(id); }); }
+void Tuner::WaitForComputeAction([[maybe_unused]] const ComputeActionId id) { GuardedVoid([&] { m_Core->Synchronize(); }); }
+void Tuner::WaitForTransferAction([[maybe_unused]] const TransferActionId id) { GuardedVoid([&] { m_Core->Synchronize(); }); }
+void Tuner::SynchronizeQueue(const QueueId id) { GuardedVoid([&] { m_Core->SynchronizeQueue(id); }); }
+
+void Tuner::SynchronizeQueues()
+{
+    GuardedVoid([&]
+    {
+        for (const auto id : m_Core->QueueIds())
+        {
+            m_Core->SynchronizeQueue(id);
+        }
+    });
+}
+
 void Tuner::SynchronizeDevice() { GuardedVoid([&] { m_Core->Synchronize(); }); }
 void Tuner::SetCompilerOptions(const std::string& options, [[maybe_unused]] const bool overrideDefault)
 {

@@ -104,24 +104,31 @@ public:
         }
     }
 
-    ComputeActionId RunKernelAsync(const KernelDefinitionId id, [[maybe_unused]] const QueueId queue) override
+    // the launch runs on the queue's stream; it completes before the call returns
+    ComputeActionId RunKernelAsync(const KernelDefinitionId id, const QueueId queue) override
     {
-        RunKernel(id);
+        m_Core.OnQueue(queue, [&] { RunKernel(id); });
         return m_NextAction++;
     }
 
-    ComputeActionId RunKernelAsync(const KernelDefinitionId id, [[maybe_unused]] const QueueId queue,
+    ComputeActionId RunKernelAsync(const KernelDefinitionId id, const QueueId queue,
         const DimensionVector& globalSize, const DimensionVector& localSize) override
     {
-        RunKernel(id, globalSize, localSize);
+        m_Core.OnQueue(queue, [&] { RunKernel(id, globalSize, localSize); });
         return m_NextAction++;
     }
 
     void WaitForComputeAction([[maybe_unused]] const ComputeActionId id) override { m_Core.Synchronize(); }
-    QueueId GetDefaultQueue() const override { return 0; }
-    std::vector<QueueId> GetAllQueues() const override { return {0}; }
-    void SynchronizeQueue([[maybe_unused]] const QueueId queue) override { m_Core.Synchronize(); }
-    void SynchronizeQueues() override { m_Core.Synchronize(); }
+    QueueId GetDefaultQueue() const override { return m_Core.QueueIds().front(); }
+    std::vector<QueueId> GetAllQueues() const override { return m_Core.QueueIds(); }
+    void SynchronizeQueue(const QueueId queue) override { m_Core.SynchronizeQueue(queue); }
+    void SynchronizeQueues() override
+    {
+        for (const auto queue : m_Core.QueueIds())
+        {
+            m_Core.SynchronizeQueue(queue);
+        }
+    }
     void SynchronizeDevice() override { m_Core.Synchronize(); }
 
     const DimensionVector& GetCurrentGlobalSize(const KernelDefinitionId id) const override { return SizeOf(m_Global, id); }
@@ -288,16 +295,159 @@ coul_ctx* TunerCore::Context()
 {
     if (m_Context == nullptr)
     {
-        const int rc = coul_ctx_create(static_cast<int>(m_Device), &m_Context);
+        const int rc = m_UserContext != nullptr
+            ? coul_ctx_create_on(m_UserContext, m_Queues.front().second, &m_Context)
+            : coul_ctx_create(static_cast<int>(m_Device), &m_Context);
 
         if (rc != COUL_OK)
         {
             m_Context = nullptr;
             throw RunFailure(ResultStatus::ComputationFailed, std::string("device initialisation failed: ") + coul_last_error());
         }
+
+        int device = 0;
+        CheckCoul(coul_ctx_device(m_Context, &device), "device index");
+        m_Device = static_cast<DeviceIndex>(device);
     }
 
     return m_Context;
+}
+
+// ---- queues: the caller's streams (KTT: CudaEngine.cpp:67-106 adopts the initializer's context and
+// streams; AddComputeQueue / RemoveComputeQueue, Tuner.h:851-863) --
+
+void TunerCore::AdoptContext(const ComputeApiInitializer& initializer, std::vector<QueueId>& assigned)
+{
+    if (initializer.GetContext() == nullptr || initializer.GetQueues().empty())
+    {
+        throw std::runtime_error("Compute API initializer needs a context and at least one queue");
+    }
+
+    m_UserContext = initializer.GetContext();
+    assigned.clear();
+
+    for (const auto queue : initializer.GetQueues())
+    {
+        assigned.push_back(AddQueue(queue));
+    }
+}
+
+QueueId TunerCore::AddQueue(ComputeQueue queue)
+{
+    if (m_UserContext == nullptr)
+    {
+        throw std::runtime_error("New queues can only be added to a tuner created with a compute API initializer");
+    }
+
+    if (queue == nullptr)
+    {
+        throw std::runtime_error("Queue must be a stream of the initializer's context");
+    }
+
+    for (const auto& [id, stream] : m_Queues)
+    {
+        if (stream == queue)
+        {
+            throw std::runtime_error("Queue was already added with id " + std::to_string(id));
+        }
+    }
+
+    const QueueId id = m_NextQueue++;
+    m_Queues.emplace_back(id, queue);
+    return id;
+}
+
+void TunerCore::RemoveQueue(const QueueId id)
+{
+    if (m_UserContext == nullptr)
+    {
+        throw std::runtime_error("Queues can only be removed from a tuner created with a compute API initializer");
+    }
+
+    const auto it = std::find_if(m_Queues.begin(), m_Queues.end(), [id](const auto& q) { return q.first == id; });
+
+    if (it == m_Queues.end())
+    {
+        throw std::runtime_error("Invalid queue id: " + std::to_string(id));
+    }
+
+    if (m_Queues.size() == 1)
+    {
+        throw std::runtime_error("The last queue of a tuner cannot be removed");
+    }
+
+    const bool current = m_Context != nullptr && coul_ctx_get_stream(m_Context) == it->second;
+
+    if (m_Context != nullptr)
+    {
+        CheckCoul(coul_synchronize(m_Context), "synchronize before a queue is removed");
+    }
+
+    m_Queues.erase(it);
+
+    if (current)
+    {
+        CheckCoul(coul_ctx_set_stream(m_Context, m_Queues.front().second), "queue switch");
+    }
+}
+
+std::vector<QueueId> TunerCore::QueueIds() const
+{
+    if (m_UserContext == nullptr)
+    {
+        return {0};
+    }
+
+    std::vector<QueueId> ids;
+
+    for (const auto& q : m_Queues)
+    {
+        ids.push_back(q.first);
+    }
+
+    return ids;
+}
+
+void TunerCore::OnQueue(const QueueId id, const std::function<void()>& work)
+{
+    if (m_UserContext == nullptr)
+    {
+        if (id != 0)
+        {
+            throw std::runtime_error("Invalid queue id: " + std::to_string(id) + " (this tuner has queue 0)");
+        }
+
+        work();
+        return;
+    }
+
+    const auto it = std::find_if(m_Queues.cbegin(), m_Queues.cend(), [id](const auto& q) { return q.first == id; });
+
+    if (it == m_Queues.cend())
+    {
+        throw std::runtime_error("Invalid queue id: " + std::to_string(id));
+    }
+
+    coul_ctx* ctx = Context();
+    void* previous = coul_ctx_get_stream(ctx);
+    CheckCoul(coul_ctx_set_stream(ctx, it->second), "queue switch");
+
+    try
+    {
+        work();
+    }
+    catch (...)
+    {
+        coul_ctx_set_stream(ctx, previous);
+        throw;
+    }
+
+    CheckCoul(coul_ctx_set_stream(ctx, previous), "queue switch");
+}
+
+void TunerCore::SynchronizeQueue(const QueueId id)
+{
+    OnQueue(id, [this] { Synchronize(); });
 }
 
 void TunerCore::Synchronize()

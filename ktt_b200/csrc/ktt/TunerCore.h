@@ -149,6 +149,14 @@ public:
     coul_ctx* Context();
     void Synchronize();
     DeviceInfo GetDeviceInfo();
+    // queues: ids of the caller's streams, or {0} for the tuner's own
+    void AdoptContext(const ComputeApiInitializer& initializer, std::vector<QueueId>& assigned);
+    QueueId AddQueue(ComputeQueue queue);
+    void RemoveQueue(const QueueId id);
+    std::vector<QueueId> QueueIds() const;
+    void SynchronizeQueue(const QueueId id);
+    // runs `work` with the context's calls enqueued on queue `id`
+    void OnQueue(const QueueId id, const std::function<void()>& work);
     std::vector<DeviceInfo> GetDeviceInfo(const PlatformIndex platform);
     std::vector<PlatformInfo> GetPlatformInfo();
     static DeviceInfo QueryDevice(const DeviceIndex index);
@@ -180,6 +188,9 @@ public:
 
 private:
     DeviceIndex m_Device;
+    ComputeContext m_UserContext = nullptr;                  // caller's CUcontext (ComputeApiInitializer)
+    std::vector<std::pair<QueueId, ComputeQueue>> m_Queues;  // caller's streams with their ids
+    QueueId m_NextQueue = 0;
     ComputeApi m_Api;
     coul_ctx* m_Context;
     GlobalSizeType m_GlobalSizeType;

@@ -455,9 +455,36 @@ PYBIND11_MODULE(pyktt, m)
     BindScalarUpdate<double>(ci, "UpdateScalarArgumentDouble");
 
     // ---- tuner (PythonTuner.cpp) ----
+    // The caller's CUDA context and streams as integers (CUcontext / CUstream handles, e.g. from ctypes).
+    py::class_<ktt::ComputeApiInitializer>(m, "ComputeApiInitializer")
+        .def(py::init([](const uintptr_t context, const std::vector<uintptr_t>& queues)
+            {
+                std::vector<ktt::ComputeQueue> q;
+
+                for (const auto queue : queues)
+                {
+                    q.push_back(reinterpret_cast<ktt::ComputeQueue>(queue));
+                }
+
+                return ktt::ComputeApiInitializer(reinterpret_cast<ktt::ComputeContext>(context), q);
+            }), py::arg("context"), py::arg("queues"))
+        .def("GetContext", [](const ktt::ComputeApiInitializer& i) { return reinterpret_cast<uintptr_t>(i.GetContext()); })
+        .def("GetQueues", [](const ktt::ComputeApiInitializer& i)
+            {
+                std::vector<uintptr_t> q;
+
+                for (const auto queue : i.GetQueues())
+                {
+                    q.push_back(reinterpret_cast<uintptr_t>(queue));
+                }
+
+                return q;
+            });
+
     py::class_<ktt::Tuner> tuner(m, "Tuner");
     tuner.def(py::init<const ktt::PlatformIndex, const ktt::DeviceIndex, const ktt::ComputeApi>())
         .def(py::init<const ktt::PlatformIndex, const ktt::DeviceIndex, const ktt::ComputeApi, const uint32_t>())
+        .def(py::init<const ktt::ComputeApi, const ktt::ComputeApiInitializer&>())
         .def("AddKernelDefinition", py::overload_cast<const std::string&, const std::string&, const ktt::DimensionVector&,
             const ktt::DimensionVector&, const std::vector<std::string>&>(&ktt::Tuner::AddKernelDefinition),
             py::arg("name"), py::arg("source"), py::arg("globalSize"), py::arg("localSize"),
@@ -610,6 +637,10 @@ PYBIND11_MODULE(pyktt, m)
         .def("SaveResults", &ktt::Tuner::SaveResults, py::arg("results"), py::arg("filePath"), py::arg("format"),
             py::arg("data") = ktt::UserData{})
         .def("LoadResults", py::overload_cast<const std::string&, const ktt::OutputFormat>(&ktt::Tuner::LoadResults, py::const_))
+        .def("AddComputeQueue", [](ktt::Tuner& t, const uintptr_t queue) { return t.AddComputeQueue(reinterpret_cast<ktt::ComputeQueue>(queue)); })
+        .def("RemoveComputeQueue", &ktt::Tuner::RemoveComputeQueue)
+        .def("WaitForComputeAction", &ktt::Tuner::WaitForComputeAction)
+        .def("WaitForTransferAction", &ktt::Tuner::WaitForTransferAction)
         .def("SynchronizeQueue", &ktt::Tuner::SynchronizeQueue)
         .def("SynchronizeQueues", &ktt::Tuner::SynchronizeQueues)
         .def("SynchronizeDevice", &ktt::Tuner::SynchronizeDevice)

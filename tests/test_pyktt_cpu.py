@@ -165,6 +165,24 @@ def test_local_symbol_arguments_and_profiled_definitions():
     tuner.SetArguments(d1, ["lm"])  # local memory goes last; the argument list is accepted
 
 
+def test_queues_of_a_tuner():
+    """Only a tuner made from a ComputeApiInitializer takes further queues; ids follow the
+    initializer's order, duplicates and the last queue are refused (logged, no exception).  The
+    handles here are never used: no call below creates the device context."""
+    plain = ktt.Tuner(0, 0, ktt.ComputeApi.CUDA)
+    assert plain.AddComputeQueue(0x1000) == ktt.InvalidQueueId
+    with pytest.raises(Exception):
+        ktt.Tuner(ktt.ComputeApi.CUDA, ktt.ComputeApiInitializer(0, [0x2000]))
+    init = ktt.ComputeApiInitializer(0xC000, [0x2000, 0x3000])
+    assert init.GetContext() == 0xC000 and init.GetQueues() == [0x2000, 0x3000]
+    tuner = ktt.Tuner(ktt.ComputeApi.CUDA, init)
+    assert tuner.AddComputeQueue(0x4000) == 2
+    assert tuner.AddComputeQueue(0x3000) == ktt.InvalidQueueId  # already a queue
+    tuner.RemoveComputeQueue(1)
+    tuner.RemoveComputeQueue(7)  # unknown id: logged
+    assert tuner.AddComputeQueue(0x5000) == 3
+
+
 def test_tuning_loader_from_python(tmp_path, recorded):
     path, _, best = recorded
     shutil.copy(os.path.join(GOLDEN, "ktt_scripts", "CoulombSum3dCudaScript.json"), tmp_path)

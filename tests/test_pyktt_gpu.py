@@ -115,3 +115,96 @@ def test_device_info_and_local_symbol_arguments():
     tuner.SetValidationMethod(ktt.ValidationMethod.SideBySideComparison, 0.01)
     results = tuner.Tune(k)
     assert len(results) == 1 and results[0].GetStatus() == ktt.ResultStatus.Ok, str(results[0].GetStatus())
+
+
+# Run in a child process: it creates and destroys a CUDA context of its own, which the other tests'
+# process-wide device state should not see.
+_INITIALIZER_PROGRAM = r'''
+import ctypes
+import numpy as np
+import oracle
+from ktt_b200 import errors
+from ktt_b200 import pyktt as ktt
+
+cu = ctypes.CDLL("libcuda.so.1")
+
+
+def ck(r, what):
+    if r != 0:
+        raise SystemExit(f"{what} failed with driver error {r}")
+
+
+ck(cu.cuInit(0), "cuInit")
+dev = ctypes.c_int()
+ck(cu.cuDeviceGet(ctypes.byref(dev), 0), "cuDeviceGet")
+ctx = ctypes.c_void_p()
+ck(cu.cuCtxCreate_v2(ctypes.byref(ctx), 0, dev), "cuCtxCreate")
+s1, s2 = ctypes.c_void_p(), ctypes.c_void_p()
+ck(cu.cuStreamCreate(ctypes.byref(s1), 0), "cuStreamCreate")
+ck(cu.cuStreamCreate(ctypes.byref(s2), 0), "cuStreamCreate")
+
+tuner = ktt.Tuner(ktt.ComputeApi.CUDA, ktt.ComputeApiInitializer(ctx.value, [s1.value]))
+assert tuner.AddComputeQueue(s2.value) == 1
+grid, n, h = 32, 80, 0.5
+rng = np.random.default_rng(9)
+atoms = np.empty((n, 4), dtype=np.float32)
+atoms[:, :3] = rng.uniform(0.0, grid * h, (n, 3))
+atoms[:, 3] = rng.uniform(-1.0, 1.0, n)
+reference = oracle.grid3d(atoms, h, (grid, grid, grid)).astype(np.float32).reshape(-1)
+tuner.SetGlobalSizeType(ktt.GlobalSizeType.CUDA)
+d = tuner.AddKernelDefinition("directCoulombSum", "", ktt.DimensionVector(grid, grid, grid), ktt.DimensionVector())
+k = tuner.CreateSimpleKernel("CoulombSum", d)
+ro = ktt.ArgumentAccessType.ReadOnly
+args = [tuner.AddArgumentVectorFloat(atoms.reshape(-1), ro)]
+args += [tuner.AddArgumentVectorFloat(np.ascontiguousarray(atoms[:, c]), ro) for c in range(4)]
+args += [tuner.AddArgumentScalarInt(n), tuner.AddArgumentScalarFloat(h), tuner.AddArgumentScalarInt(grid)]
+out_id = tuner.AddArgumentVectorFloat(np.zeros(grid ** 3, dtype=np.float32), ktt.ArgumentAccessType.WriteOnly)
+tuner.SetArguments(d, args + [out_id])
+for name, value in (("WORK_GROUP_SIZE_X", 32), ("WORK_GROUP_SIZE_Y", 4), ("Z_ITERATIONS", 8),
+                    ("INNER_UNROLL_FACTOR", 2), ("USE_SOA", 0)):
+    tuner.AddParameter(k, name, [value])
+for dim, name in ((ktt.ModifierDimension.X, "WORK_GROUP_SIZE_X"), (ktt.ModifierDimension.Y, "WORK_GROUP_SIZE_Y")):
+    tuner.AddThreadModifier(k, [d], ktt.ModifierType.Local, dim, name, ktt.ModifierAction.Multiply)
+    tuner.AddThreadModifier(k, [d], ktt.ModifierType.Global, dim, name, ktt.ModifierAction.DivideCeil)
+tuner.AddThreadModifier(k, [d], ktt.ModifierType.Global, ktt.ModifierDimension.Z, "Z_ITERATIONS",
+                        ktt.ModifierAction.DivideCeil)
+seen = []
+
+
+def launcher(ci):
+    seen.append(list(ci.GetAllQueues()))
+    ci.RunKernelAsync(d, 1)  # on the second of the caller's streams
+    ci.SynchronizeQueues()
+
+
+tuner.SetLauncher(k, launcher)
+out = np.zeros(grid ** 3, dtype=np.float32)
+config = tuner.CreateConfiguration(k, [("WORK_GROUP_SIZE_X", 32), ("WORK_GROUP_SIZE_Y", 4), ("Z_ITERATIONS", 8),
+                                       ("INNER_UNROLL_FACTOR", 2), ("USE_SOA", 0)])
+result = tuner.Run(k, config, [ktt.BufferOutputDescriptor(out_id, out)])
+assert result.GetStatus() == ktt.ResultStatus.Ok, str(result.GetStatus())
+assert seen == [[0, 1]], seen
+assert errors.report(out, reference)["rel_norm"] <= 1e-5
+tuner.SynchronizeQueue(1)
+tuner.RemoveComputeQueue(1)
+assert tuner.GetCurrentDeviceInfo().GetCudaComputeCapabilityMajor() == 10
+del tuner
+ck(cu.cuStreamDestroy_v2(s1), "cuStreamDestroy")
+ck(cu.cuStreamDestroy_v2(s2), "cuStreamDestroy")
+ck(cu.cuCtxDestroy_v2(ctx), "cuCtxDestroy")
+print("initializer ok")
+'''
+
+
+def test_compute_api_initializer_with_callers_context():
+    """Tutorials/05ComputeApiInitializer: a tuner on a CUDA context and streams the caller created
+    with the driver API; a launcher runs the kernel on the second stream (AddComputeQueue) and the
+    map matches the FP64 oracle."""
+    import os
+    import subprocess
+    import sys
+    repo = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, PYTHONPATH=repo + os.pathsep + os.environ.get("PYTHONPATH", ""))
+    r = subprocess.run([sys.executable, "-c", _INITIALIZER_PROGRAM], cwd=repo, env=env, capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0 and "initializer ok" in r.stdout, r.stdout[-2000:] + r.stderr[-2000:]
