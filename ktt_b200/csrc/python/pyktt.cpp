@@ -503,10 +503,32 @@ PYBIND11_MODULE(pyktt, m)
         .def("RemoveKernelDefinition", &ktt::Tuner::RemoveKernelDefinition)
         .def("SetArguments", &ktt::Tuner::SetArguments)
         .def("CreateSimpleKernel", &ktt::Tuner::CreateSimpleKernel)
-        .def("CreateCompositeKernel", &ktt::Tuner::CreateCompositeKernel, py::arg("name"), py::arg("definitionIds"),
-            py::arg("launcher") = nullptr)
+        // Python launchers receive the ComputeInterface by reference (a pointer on the C++ side; the
+        // interface cannot be copied), as KTT's module passes it (Source/Python/PythonTuner.cpp:80-88)
+        .def("CreateCompositeKernel", [](ktt::Tuner& t, const std::string& name, const std::vector<ktt::KernelDefinitionId>& ids,
+            std::function<void(ktt::ComputeInterface*)> launcher)
+            {
+                ktt::KernelLauncher wrapped;
+
+                if (launcher)
+                {
+                    wrapped = [launcher](ktt::ComputeInterface& ci) { launcher(&ci); };
+                }
+
+                return t.CreateCompositeKernel(name, ids, wrapped);
+            }, py::arg("name"), py::arg("definitionIds"), py::arg("launcher") = nullptr)
         .def("RemoveKernel", &ktt::Tuner::RemoveKernel)
-        .def("SetLauncher", &ktt::Tuner::SetLauncher)
+        .def("SetLauncher", [](ktt::Tuner& t, const ktt::KernelId id, std::function<void(ktt::ComputeInterface*)> launcher)
+            {
+                ktt::KernelLauncher wrapped;
+
+                if (launcher)
+                {
+                    wrapped = [launcher](ktt::ComputeInterface& ci) { launcher(&ci); };
+                }
+
+                t.SetLauncher(id, wrapped);
+            }, py::arg("id"), py::arg("launcher"))
         .def("AddParameter", [](ktt::Tuner& t, const ktt::KernelId id, const std::string& name, const std::vector<uint64_t>& values,
             const std::string& group) { t.AddParameter(id, name, values, group); },
             py::arg("id"), py::arg("name"), py::arg("values"), py::arg("group") = std::string())

@@ -183,6 +183,26 @@ def test_queues_of_a_tuner():
     assert tuner.AddComputeQueue(0x5000) == 3
 
 
+def test_python_launchers_get_the_compute_interface():
+    """SetLauncher and CreateCompositeKernel take Python launchers; they are handed the tuner's
+    ComputeInterface (queues, configuration) without a copy.  These launchers launch nothing, so
+    the runs need no device."""
+    tuner = ktt.Tuner(0, 0, ktt.ComputeApi.CUDA)
+    d = tuner.AddKernelDefinition("noop", "", ktt.DimensionVector(32), ktt.DimensionVector(32))
+    k = tuner.CreateSimpleKernel("k", d)
+    tuner.AddParameter(k, "P", [1, 2])
+    seen = []
+
+    def launcher(ci):
+        seen.append((list(ci.GetAllQueues()), ci.GetDefaultQueue(), ci.GetCurrentConfiguration().GetString()))
+
+    tuner.SetLauncher(k, launcher)
+    assert tuner.Run(k, tuner.CreateConfiguration(k, [("P", 2)]), []).GetStatus() == ktt.ResultStatus.Ok
+    c = tuner.CreateCompositeKernel("c", [d], launcher)
+    assert tuner.Run(c, tuner.CreateConfiguration(c, []), []).GetStatus() == ktt.ResultStatus.Ok
+    assert seen == [([0], 0, "P 2"), ([0], 0, "empty")]
+
+
 def test_tuning_loader_from_python(tmp_path, recorded):
     path, _, best = recorded
     shutil.copy(os.path.join(GOLDEN, "ktt_scripts", "CoulombSum3dCudaScript.json"), tmp_path)
