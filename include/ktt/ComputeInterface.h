@@ -55,6 +55,25 @@ public:
     virtual void CopyBuffer(const ArgumentId& destination, const ArgumentId& source, const size_t dataSize = 0) = 0;
     virtual void ClearBuffer(const ArgumentId& id) = 0;
     virtual bool HasBuffer(const ArgumentId& id) = 0;
+
+    // Transfers on a queue (Source/Api/ComputeInterface.h:216-310).  They complete before the call
+    // returns; the action ids exist for WaitForTransferAction, as in KTT.
+    virtual TransferActionId UploadBufferAsync(const ArgumentId& id, const QueueId queue) = 0;
+    virtual TransferActionId DownloadBufferAsync(const ArgumentId& id, const QueueId queue, void* destination,
+        const size_t dataSize = 0) = 0;
+    virtual TransferActionId UpdateBufferAsync(const ArgumentId& id, const QueueId queue, const void* data,
+        const size_t dataSize = 0) = 0;
+    virtual TransferActionId CopyBufferAsync(const ArgumentId& destination, const ArgumentId& source, const QueueId queue,
+        const size_t dataSize = 0) = 0;
+    virtual void WaitForTransferAction(const TransferActionId id) = 0;
+    // New size of a vector argument's device buffer owned by the tuner (user buffers cannot be resized),
+    // keeping the first min(old, new) bytes when preserveData.
+    virtual void ResizeBuffer(const ArgumentId& id, const size_t newDataSize, const bool preserveData) = 0;
+    // New size of a local-memory argument.
+    virtual void UpdateLocalArgument(const ArgumentId& id, const size_t dataSize) = 0;
+    // Unified-memory arguments are not offered by this build: the call reports an error.
+    virtual void GetUnifiedMemoryBufferHandle(const ArgumentId& id, UnifiedBufferMemory& memoryHandle) = 0;
+    virtual bool GetProfiling(const KernelId id) = 0;
 };
 
 } // namespace ktt

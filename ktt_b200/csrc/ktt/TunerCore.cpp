@@ -215,6 +215,58 @@ public:
         return argument.ownership == ArgumentOwnership::User || argument.device != nullptr;
     }
 
+    TransferActionId UploadBufferAsync(const ArgumentId& id, const QueueId queue) override
+    {
+        m_Core.OnQueue(queue, [&] { UploadBuffer(id); });
+        return m_NextTransfer++;
+    }
+
+    TransferActionId DownloadBufferAsync(const ArgumentId& id, const QueueId queue, void* destination,
+        const size_t dataSize) override
+    {
+        m_Core.OnQueue(queue, [&] { DownloadBuffer(id, destination, dataSize); });
+        return m_NextTransfer++;
+    }
+
+    TransferActionId UpdateBufferAsync(const ArgumentId& id, const QueueId queue, const void* data, const size_t dataSize) override
+    {
+        m_Core.OnQueue(queue, [&] { UpdateBuffer(id, data, dataSize); });
+        return m_NextTransfer++;
+    }
+
+    TransferActionId CopyBufferAsync(const ArgumentId& destination, const ArgumentId& source, const QueueId queue,
+        const size_t dataSize) override
+    {
+        m_Core.OnQueue(queue, [&] { CopyBuffer(destination, source, dataSize); });
+        return m_NextTransfer++;
+    }
+
+    void WaitForTransferAction([[maybe_unused]] const TransferActionId id) override { m_Core.Synchronize(); }
+
+    void ResizeBuffer(const ArgumentId& id, const size_t newDataSize, const bool preserveData) override
+    {
+        m_Core.ResizeArgument(m_Core.Argument(id), newDataSize, preserveData);
+    }
+
+    void UpdateLocalArgument(const ArgumentId& id, const size_t dataSize) override
+    {
+        ArgumentData& argument = m_Core.Argument(id);
+
+        if (argument.memoryType != ArgumentMemoryType::Local || dataSize == 0)
+        {
+            throw std::runtime_error("Argument " + id + " is not a local memory argument, or the size is zero");
+        }
+
+        argument.bytes = dataSize;
+    }
+
+    void GetUnifiedMemoryBufferHandle(const ArgumentId& id, [[maybe_unused]] UnifiedBufferMemory& memoryHandle) override
+    {
+        throw std::runtime_error("Argument " + id + " is not in unified memory (this build keeps arguments in device memory)");
+    }
+
+    bool GetProfiling([[maybe_unused]] const KernelId id) override { return m_Core.GetProfiling(); }
+
     std::vector<ComputationResult> Results() const
     {
         std::vector<ComputationResult> out;
@@ -237,6 +289,7 @@ private:
     std::map<KernelDefinitionId, ComputationResult> m_Results;
     std::vector<KernelDefinitionId> m_Order;
     ComputeActionId m_NextAction = 0;
+    TransferActionId m_NextTransfer = 0;
 
     static const DimensionVector& SizeOf(const std::map<KernelDefinitionId, DimensionVector>& sizes, const KernelDefinitionId id)
     {
@@ -834,6 +887,39 @@ void TunerCore::UploadArgument(ArgumentData& argument, const bool force)
         CheckCoul(coul_buffer_upload(ctx, argument.device, argument.HostData(), argument.bytes), "upload of argument " + argument.id);
         argument.deviceCurrent = true;
     }
+}
+
+// ComputeInterface::ResizeBuffer (KTT: Source/Api/ComputeInterface.h:312-318): the tuner-owned device
+// buffer and its host copy take the new size; preserved bytes are copied on the device.
+void TunerCore::ResizeArgument(ArgumentData& argument, const size_t bytes, const bool preserve)
+{
+    if (argument.memoryType != ArgumentMemoryType::Vector || argument.ownership != ArgumentOwnership::Owned || bytes == 0)
+    {
+        throw std::runtime_error("Only vector arguments whose data the tuner owns can be resized, to a non-zero size ("
+            + argument.id + ")");
+    }
+
+    UploadArgument(argument, false);
+    coul_ctx* ctx = Context();
+    void* resized = nullptr;
+    CheckCoul(coul_buffer_alloc(ctx, bytes, &resized), "buffer allocation for argument " + argument.id);
+
+    if (preserve)
+    {
+        CheckCoul(coul_buffer_copy(ctx, resized, argument.device, std::min(bytes, argument.bytes)), "resize of " + argument.id);
+    }
+    else
+    {
+        CheckCoul(coul_buffer_memset(ctx, resized, 0, bytes), "resize of " + argument.id);
+    }
+
+    CheckCoul(coul_synchronize(ctx), "resize of " + argument.id);
+    coul_buffer_free(ctx, argument.device);
+    argument.device = resized;
+    argument.deviceBytes = bytes;
+    argument.owned.resize(bytes, 0);
+    argument.bytes = bytes;
+    argument.deviceCurrent = true;
 }
 
 void TunerCore::DownloadArgument(ArgumentData& argument, void* destination, size_t bytes)

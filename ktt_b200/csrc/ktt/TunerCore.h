@@ -184,6 +184,7 @@ public:
     Nanoseconds LaunchDefinition(const KernelData& kernel, const KernelDefinitionId id, const KernelConfiguration& configuration,
         const DimensionVector& global, const DimensionVector& local);
     void UploadArgument(ArgumentData& argument, const bool force);
+    void ResizeArgument(ArgumentData& argument, const size_t bytes, const bool preserve);
     void DownloadArgument(ArgumentData& argument, void* destination, size_t bytes);
 
 private:

@@ -446,7 +446,26 @@ PYBIND11_MODULE(pyktt, m)
             })
         .def("CopyBuffer", &ktt::ComputeInterface::CopyBuffer)
         .def("ClearBuffer", &ktt::ComputeInterface::ClearBuffer)
-        .def("HasBuffer", &ktt::ComputeInterface::HasBuffer);
+        .def("HasBuffer", &ktt::ComputeInterface::HasBuffer)
+        .def("UploadBufferAsync", &ktt::ComputeInterface::UploadBufferAsync)
+        .def("DownloadBufferAsync", [](ktt::ComputeInterface& c, const ktt::ArgumentId& id, const ktt::QueueId queue,
+            py::buffer destination)
+            {
+                const py::buffer_info info = destination.request(true);
+                return c.DownloadBufferAsync(id, queue, info.ptr, static_cast<size_t>(info.size * info.itemsize));
+            })
+        .def("UpdateBufferAsync", [](ktt::ComputeInterface& c, const ktt::ArgumentId& id, const ktt::QueueId queue,
+            py::buffer data)
+            {
+                const py::buffer_info info = data.request();
+                return c.UpdateBufferAsync(id, queue, info.ptr, static_cast<size_t>(info.size * info.itemsize));
+            })
+        .def("CopyBufferAsync", &ktt::ComputeInterface::CopyBufferAsync, py::arg("destination"), py::arg("source"),
+            py::arg("queue"), py::arg("dataSize") = 0)
+        .def("WaitForTransferAction", &ktt::ComputeInterface::WaitForTransferAction)
+        .def("ResizeBuffer", &ktt::ComputeInterface::ResizeBuffer)
+        .def("UpdateLocalArgument", &ktt::ComputeInterface::UpdateLocalArgument)
+        .def("GetProfiling", &ktt::ComputeInterface::GetProfiling);
     BindScalarUpdate<int8_t>(ci, "UpdateScalarArgumentChar");
     BindScalarUpdate<int16_t>(ci, "UpdateScalarArgumentShort");
     BindScalarUpdate<int32_t>(ci, "UpdateScalarArgumentInt");

@@ -208,3 +208,38 @@ def test_compute_api_initializer_with_callers_context():
     r = subprocess.run([sys.executable, "-c", _INITIALIZER_PROGRAM], cwd=repo, env=env, capture_output=True, text=True,
                        timeout=300)
     assert r.returncode == 0 and "initializer ok" in r.stdout, r.stdout[-2000:] + r.stderr[-2000:]
+
+
+def test_launcher_transfers_resize_and_local_size():
+    """ComputeInterface's queue transfers, ResizeBuffer (data kept), UpdateLocalArgument and
+    GetProfiling from a Python launcher (Source/Api/ComputeInterface.h:202-349)."""
+    tuner = ktt.Tuner(0, 0, ktt.ComputeApi.CUDA)
+    d = tuner.AddKernelDefinition("noop", "", ktt.DimensionVector(32), ktt.DimensionVector(32))
+    k = tuner.CreateSimpleKernel("k", d)
+    rw = ktt.ArgumentAccessType.ReadWrite
+    a = tuner.AddArgumentVectorFloat(np.arange(16, dtype=np.float32), rw)
+    b = tuner.AddArgumentVectorFloat(np.zeros(16, dtype=np.float32), rw)
+    local = tuner.AddArgumentLocalFloat(256)
+    got = {}
+
+    def launcher(ci):
+        ci.UploadBufferAsync(a, 0)
+        ci.UploadBufferAsync(b, 0)
+        ci.WaitForTransferAction(ci.CopyBufferAsync(b, a, 0, 32))  # the first 8 floats
+        ci.UpdateBufferAsync(a, 0, np.full(16, 5.0, dtype=np.float32))
+        ci.ResizeBuffer(b, 128, True)  # 32 floats, the 16 old ones kept
+        out_b = np.full(32, -1.0, dtype=np.float32)
+        ci.DownloadBufferAsync(b, 0, out_b)
+        ci.SynchronizeQueues()
+        out_a = np.zeros(16, dtype=np.float32)
+        ci.DownloadBuffer(a, out_a)
+        ci.UpdateLocalArgument(local, 512)
+        got.update(a=out_a, b=out_b, profiling=ci.GetProfiling(k))
+
+    tuner.SetLauncher(k, launcher)
+    result = tuner.Run(k, tuner.CreateConfiguration(k, []), [])
+    assert result.GetStatus() == ktt.ResultStatus.Ok, str(result.GetStatus())
+    assert np.array_equal(got["b"][:8], np.arange(8, dtype=np.float32))
+    assert not got["b"][8:].any()
+    assert np.array_equal(got["a"], np.full(16, 5.0, dtype=np.float32))
+    assert got["profiling"] is False
