@@ -67,7 +67,7 @@ public:
         const size_t dataSize = 0) = 0;
     virtual void WaitForTransferAction(const TransferActionId id) = 0;
     // New size of a vector argument's device buffer owned by the tuner (user buffers cannot be resized),
-    // keeping the first min(old, new) bytes when preserveData.
+    // keeping the first min(old, new) bytes when preserveData; the other bytes are zero.
     virtual void ResizeBuffer(const ArgumentId& id, const size_t newDataSize, const bool preserveData) = 0;
     // New size of a local-memory argument.
     virtual void UpdateLocalArgument(const ArgumentId& id, const size_t dataSize) = 0;

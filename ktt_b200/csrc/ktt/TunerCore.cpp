@@ -904,13 +904,12 @@ void TunerCore::ResizeArgument(ArgumentData& argument, const size_t bytes, const
     void* resized = nullptr;
     CheckCoul(coul_buffer_alloc(ctx, bytes, &resized), "buffer allocation for argument " + argument.id);
 
+    // bytes not preserved read as zero
+    CheckCoul(coul_buffer_memset(ctx, resized, 0, bytes), "resize of " + argument.id);
+
     if (preserve)
     {
         CheckCoul(coul_buffer_copy(ctx, resized, argument.device, std::min(bytes, argument.bytes)), "resize of " + argument.id);
-    }
-    else
-    {
-        CheckCoul(coul_buffer_memset(ctx, resized, 0, bytes), "resize of " + argument.id);
     }
 
     CheckCoul(coul_synchronize(ctx), "resize of " + argument.id);
