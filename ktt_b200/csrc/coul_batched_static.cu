@@ -56,16 +56,13 @@ const StaticVariant* static_variants()
     return v;
 }
 
-// Per-device state found at the first call on that device: the device address of the scratch
-// array and the SM count (occupancy is looked up per block shape on each call).
-struct DeviceSetup {
-    bool ready = false;
-    unsigned char* scratch = nullptr;
-    int sm_count = 0;
-};
+// SM count per device, found at the first call on that device (occupancy is looked up per block
+// shape on each call).  The scratch array's device address is not cached: a module-scope
+// __device__ array has one instance per CUDA context that loads the module, so the address belongs
+// to the context current at the call (the device's primary context, or a caller-owned one).
+int g_sm_count[kMaxDevices];
 
 std::mutex g_mutex;
-DeviceSetup g_setup[kMaxDevices];
 MolDesc g_host_table[kStaticMaxMolecules];  // host staging, reused by every call (under g_mutex)
 int g_order[kStaticMaxMolecules];
 
@@ -120,20 +117,19 @@ extern "C" COUL_API int coul_batch_run_static(void* stream, const coul_molecule*
         return fail(COUL_ERR_NO_DEVICE, "coul_batch_run_static: device index beyond 63");
 
     std::lock_guard<std::mutex> lock(g_mutex);
-    DeviceSetup& setup = g_setup[device];
-    if (!setup.ready) {
-        // First call on this device (the current one): look up the device address of the static
-        // scratch array.  In host code the symbol itself is only a host-side stand-in.
-        void* ptr = nullptr;
-        if ((e = cudaGetSymbolAddress(&ptr, g_batch_scratch)) != cudaSuccess)
-            return cuda_error(e, "cudaGetSymbolAddress of the static batch scratch");
+    if (g_sm_count[device] == 0) {
         int sm = 0;
         if ((e = cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess)
             return cuda_error(e, "cudaDeviceGetAttribute");
-        setup.scratch = static_cast<unsigned char*>(ptr);
-        setup.sm_count = sm;
-        setup.ready = true;
+        g_sm_count[device] = sm;
     }
+    // The device address of the static scratch array in the context current on this thread (in
+    // host code the symbol itself is only a host-side stand-in).  A lookup, no allocation; the first
+    // lookup in a context loads this library's device code into it.
+    void* scratch_ptr = nullptr;
+    if ((e = cudaGetSymbolAddress(&scratch_ptr, g_batch_scratch)) != cudaSuccess)
+        return cuda_error(e, "cudaGetSymbolAddress of the static batch scratch");
+    unsigned char* scratch = static_cast<unsigned char*>(scratch_ptr);
 
     // Molecule table in decreasing order of pair count (same work list as coul_batch_create).
     for (int i = 0; i < n_molecules; ++i)
@@ -174,8 +170,8 @@ extern "C" COUL_API int coul_batch_run_static(void* stream, const coul_molecule*
         return COUL_OK;
 
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    unsigned long long* counter = reinterpret_cast<unsigned long long*>(setup.scratch);
-    MolDesc* table = reinterpret_cast<MolDesc*>(setup.scratch + kStaticTableOffset);
+    unsigned long long* counter = reinterpret_cast<unsigned long long*>(scratch);
+    MolDesc* table = reinterpret_cast<MolDesc*>(scratch + kStaticTableOffset);
     // The copy reads the pageable host table before it returns, so the table may be refilled by the
     // next call; the counter must start at zero.
     if ((e = cudaMemcpyAsync(table, g_host_table, sizeof(MolDesc) * n_molecules, cudaMemcpyHostToDevice, s)) !=
@@ -193,7 +189,7 @@ extern "C" COUL_API int coul_batch_run_static(void* stream, const coul_molecule*
         return fail(COUL_ERR_DEVICE_LIMITS, "coul_batch_run_static: kernel does not fit on an SM");
     BatchParams p{table, n_molecules, next, counter, accumulate ? 1 : 0, d_status};
     void* args[] = {&p};
-    e = cudaLaunchKernel(variant->kernel, dim3(static_cast<unsigned>(blocks_per_sm * setup.sm_count)),
+    e = cudaLaunchKernel(variant->kernel, dim3(static_cast<unsigned>(blocks_per_sm * g_sm_count[device])),
                          dim3(static_cast<unsigned>(tune->block_x), static_cast<unsigned>(tune->block_y), 1), args, smem,
                          s);
     if (e != cudaSuccess)

@@ -8,6 +8,9 @@ point (coul_batch_create + coul_batch_run) within the suite's tolerance.  It liv
 collected last, and passes both alone in a fresh process and after the other tests.
 """
 import ctypes
+import os
+import subprocess
+import sys
 
 import numpy as np
 import pytest
@@ -77,6 +80,97 @@ def test_static_entry_point_matches_allocating_entry_point_twice():
             rep = errors.report(g, w)
             assert rep["rel_norm"] <= TOL_NORM, rep
     ctx.close()
+
+
+# Child process: the static array has one instance per CUDA context, so calls made under the
+# device's primary context, then under a context the caller created with the driver API, then under
+# the primary context again must each find their own context's copy.  One molecule per call is
+# checked against the FP64 oracle.
+_CONTEXT_PROGRAM = r'''
+import ctypes
+import numpy as np
+import torch
+import ktt_b200
+import oracle
+from ktt_b200 import errors
+from ktt_b200._signatures import Molecule
+
+cu = ctypes.CDLL("libcuda.so.1")
+lib = ktt_b200.load_library()
+fn = lib.coul_batch_run_static
+fn.argtypes = [ctypes.c_void_p, ctypes.POINTER(Molecule), ctypes.c_int, ctypes.POINTER(ktt_b200._Tune),
+               ctypes.c_int, ctypes.c_void_p]
+fn.restype = ctypes.c_int
+
+
+def ck(r, what):
+    if r != 0:
+        raise SystemExit(f"{what} failed with driver error {r}")
+
+
+rng = np.random.default_rng(5)
+n, dims, h = 300, (40, 24, 20), 0.5
+atoms = np.empty((n, 4), dtype=np.float32)
+atoms[:, :3] = rng.uniform(0.0, 12.0, (n, 3))
+atoms[:, 3] = rng.uniform(-1.0, 1.0, n)
+want = oracle.grid3d(atoms, h, dims)
+tune = ktt_b200.Tune(block_x=32, block_y=4, z_iterations=8, x_points=2, unroll=2, rsqrt_soft=2).c()
+out_bytes = dims[0] * dims[1] * dims[2] * 4
+
+
+def run(d_atoms, d_out, stream):
+    m = (Molecule * 1)()
+    m[0].d_atoms, m[0].n_atoms, m[0].d_out = d_atoms, n, d_out
+    m[0].grid = ktt_b200._grid(dims, h, None)
+    rc = fn(ctypes.c_void_p(stream), m, 1, ctypes.byref(tune), 0, None)
+    assert rc == ktt_b200.COUL_OK, lib.coul_last_error()
+
+
+def primary_call():
+    a = torch.from_numpy(atoms).cuda()
+    o = torch.full((dims[2], dims[1], dims[0]), float("nan"), device="cuda")
+    run(a.data_ptr(), o.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    return o.cpu().numpy()
+
+
+def own_context_call():
+    dev = ctypes.c_int()
+    ck(cu.cuDeviceGet(ctypes.byref(dev), 0), "cuDeviceGet")
+    ctx = ctypes.c_void_p()
+    ck(cu.cuCtxCreate_v2(ctypes.byref(ctx), 0, dev), "cuCtxCreate")  # current on this thread
+    d_atoms, d_out = ctypes.c_uint64(), ctypes.c_uint64()
+    ck(cu.cuMemAlloc_v2(ctypes.byref(d_atoms), ctypes.c_size_t(atoms.nbytes)), "cuMemAlloc")
+    ck(cu.cuMemAlloc_v2(ctypes.byref(d_out), ctypes.c_size_t(out_bytes)), "cuMemAlloc")
+    ck(cu.cuMemcpyHtoD_v2(d_atoms, atoms.ctypes.data_as(ctypes.c_void_p), ctypes.c_size_t(atoms.nbytes)), "HtoD")
+    ck(cu.cuMemsetD32_v2(d_out, 0x7fc00000, ctypes.c_size_t(out_bytes // 4)), "cuMemsetD32")
+    run(d_atoms.value, d_out.value, 0)  # the legacy default stream of the current (own) context
+    ck(cu.cuCtxSynchronize(), "cuCtxSynchronize")
+    got = np.empty((dims[2], dims[1], dims[0]), dtype=np.float32)
+    ck(cu.cuMemcpyDtoH_v2(got.ctypes.data_as(ctypes.c_void_p), d_out, ctypes.c_size_t(out_bytes)), "DtoH")
+    ck(cu.cuMemFree_v2(d_atoms), "cuMemFree")
+    ck(cu.cuMemFree_v2(d_out), "cuMemFree")
+    ck(cu.cuCtxDestroy_v2(ctx), "cuCtxDestroy")
+    return got
+
+
+maps = [primary_call(), own_context_call()]
+torch.cuda.synchronize()  # back on the primary context
+maps.append(primary_call())
+for got in maps:
+    assert np.all(np.isfinite(got))
+    rep = errors.report(got, want)
+    assert rep["rel_norm"] <= 1e-5, rep
+print("contexts ok")
+'''
+
+
+def test_static_entry_point_under_callers_own_context():
+    repo = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, PYTHONPATH=repo + os.pathsep + os.environ.get("PYTHONPATH", ""))
+    r = subprocess.run([sys.executable, "-c", _CONTEXT_PROGRAM], cwd=repo, env=env, capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0 and "contexts ok" in r.stdout, r.stdout + r.stderr
 
 
 def test_static_entry_point_rejects_oversized_batch():
