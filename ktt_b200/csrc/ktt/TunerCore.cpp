@@ -2,6 +2,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <sstream>
@@ -164,7 +165,7 @@ public:
             throw std::runtime_error("Argument " + id + " is not a scalar");
         }
 
-        std::memcpy(argument.owned.data(), data, argument.bytes);
+        m_Core.OverrideScalar(id, data);
     }
 
     void UploadBuffer(const ArgumentId& id) override { m_Core.UploadArgument(m_Core.Argument(id), true); }
@@ -177,16 +178,7 @@ public:
     void UpdateBuffer(const ArgumentId& id, const void* data, const size_t dataSize) override
     {
         ArgumentData& argument = m_Core.Argument(id);
-        const size_t bytes = dataSize == 0 ? argument.bytes : std::min(dataSize, argument.bytes);
-
-        if (argument.ownership == ArgumentOwnership::User)
-        {
-            CheckCoul(coul_buffer_upload(m_Core.Context(), argument.userDevice, data, bytes), "UpdateBuffer");
-            return;
-        }
-
-        std::memcpy(argument.HostData(), data, bytes);
-        m_Core.UploadArgument(argument, true);
+        m_Core.UpdateArgumentDevice(argument, data, dataSize);
     }
 
     void CopyBuffer(const ArgumentId& destination, const ArgumentId& source, const size_t dataSize) override
@@ -195,7 +187,7 @@ public:
         ArgumentData& src = m_Core.Argument(source);
         m_Core.UploadArgument(dst, false);
         m_Core.UploadArgument(src, false);
-        const size_t bytes = dataSize == 0 ? std::min(dst.bytes, src.bytes) : dataSize;
+        const size_t bytes = dataSize == 0 ? std::min(TunerCore::DeviceBytes(dst), TunerCore::DeviceBytes(src)) : dataSize;
         void* d = dst.ownership == ArgumentOwnership::User ? dst.userDevice : dst.device;
         const void* s = src.ownership == ArgumentOwnership::User ? src.userDevice : src.device;
         CheckCoul(coul_buffer_copy(m_Core.Context(), d, s, bytes), "CopyBuffer");
@@ -206,7 +198,7 @@ public:
         ArgumentData& argument = m_Core.Argument(id);
         m_Core.UploadArgument(argument, false);
         void* d = argument.ownership == ArgumentOwnership::User ? argument.userDevice : argument.device;
-        CheckCoul(coul_buffer_memset(m_Core.Context(), d, 0, argument.bytes), "ClearBuffer");
+        CheckCoul(coul_buffer_memset(m_Core.Context(), d, 0, TunerCore::DeviceBytes(argument)), "ClearBuffer");
     }
 
     bool HasBuffer(const ArgumentId& id) override
@@ -250,14 +242,16 @@ public:
 
     void UpdateLocalArgument(const ArgumentId& id, const size_t dataSize) override
     {
-        ArgumentData& argument = m_Core.Argument(id);
+        const ArgumentData& argument = m_Core.Argument(id);
 
         if (argument.memoryType != ArgumentMemoryType::Local || dataSize == 0)
         {
             throw std::runtime_error("Argument " + id + " is not a local memory argument, or the size is zero");
         }
 
-        argument.bytes = dataSize;
+        // A per-run override in KTT (ComputeLayer.cpp:175-186) that sets the launch's dynamic shared
+        // memory; the built-in kernels size their own shared memory, so the stored argument is left
+        // as it is and nothing carries over to later runs.
     }
 
     void GetUnifiedMemoryBufferHandle(const ArgumentId& id, [[maybe_unused]] UnifiedBufferMemory& memoryHandle) override
@@ -312,9 +306,18 @@ TunerCore::TunerCore(const DeviceIndex device, const ComputeApi api) :
     m_ValidationMode(ValidationMode::OfflineTuning | ValidationMode::OnlineTuning), m_NextDefinition(0), m_NextKernel(0),
     m_NextArgument(0)
 {
-    if (api != ComputeApi::CUDA)
+    if (api == ComputeApi::Vulkan)
     {
-        throw std::runtime_error("This build runs the CUDA compute API only (B200, sm_100a)");
+        throw std::runtime_error("This build has no Vulkan engine; it runs the built-in CUDA kernels for sm_100a");
+    }
+
+    if (api == ComputeApi::OpenCL)
+    {
+        // KTT's OpenCL host programs for this path (Examples/CoulombSum2d/CoulombSum2d.cpp,
+        // Examples/CoulombSum3dIterative/CoulombSum3dIterative.cpp) run unchanged: their definitions
+        // are matched by kernel name and argument list to the same built-in kernels, with KTT's
+        // OpenCL global-size convention; the .cl sources are never compiled.
+        log::Info("ComputeApi::OpenCL requested: definitions run on the built-in CUDA kernels (sm_100a)");
     }
 }
 
@@ -374,6 +377,11 @@ void TunerCore::AdoptContext(const ComputeApiInitializer& initializer, std::vect
     if (initializer.GetContext() == nullptr || initializer.GetQueues().empty())
     {
         throw std::runtime_error("Compute API initializer needs a context and at least one queue");
+    }
+
+    if (m_Api != ComputeApi::CUDA)
+    {
+        throw std::runtime_error("Compute API initializer: only a CUDA context and CUDA streams can be adopted");
     }
 
     m_UserContext = initializer.GetContext();
@@ -869,14 +877,16 @@ void TunerCore::UploadArgument(ArgumentData& argument, const bool force)
 
     coul_ctx* ctx = Context();
 
-    if (argument.device == nullptr || argument.deviceBytes < argument.bytes)
+    // A fresh upload starts from the host data at its own size, so a buffer resized by an earlier
+    // run's launcher is re-created (KTT re-creates writable buffers per run).
+    if (argument.device != nullptr && (force || !argument.deviceCurrent) && argument.deviceBytes != argument.bytes)
     {
-        if (argument.device != nullptr)
-        {
-            coul_buffer_free(ctx, argument.device);
-            argument.device = nullptr;
-        }
+        coul_buffer_free(ctx, argument.device);
+        argument.device = nullptr;
+    }
 
+    if (argument.device == nullptr)
+    {
         CheckCoul(coul_buffer_alloc(ctx, argument.bytes, &argument.device), "buffer allocation for argument " + argument.id);
         argument.deviceBytes = argument.bytes;
         argument.deviceCurrent = false;
@@ -889,13 +899,36 @@ void TunerCore::UploadArgument(ArgumentData& argument, const bool force)
     }
 }
 
-// ComputeInterface::ResizeBuffer (KTT: Source/Api/ComputeInterface.h:312-318): the tuner-owned device
-// buffer and its host copy take the new size; preserved bytes are copied on the device.
+size_t TunerCore::DeviceBytes(const ArgumentData& argument)
+{
+    return argument.ownership != ArgumentOwnership::User && argument.device != nullptr ? argument.deviceBytes : argument.bytes;
+}
+
+// ComputeInterface::UpdateBuffer (KTT: CudaEngine.cpp:430-470, UpdateArgument): the device buffer takes
+// the data; the host copy is not touched, so a writable argument starts the next run from the
+// caller's data again.
+void TunerCore::UpdateArgumentDevice(ArgumentData& argument, const void* data, size_t bytes)
+{
+    if (argument.memoryType != ArgumentMemoryType::Vector)
+    {
+        throw std::runtime_error("Argument " + argument.id + " is not a vector");
+    }
+
+    UploadArgument(argument, false);
+    bytes = bytes == 0 ? DeviceBytes(argument) : std::min(bytes, DeviceBytes(argument));
+    void* target = argument.ownership == ArgumentOwnership::User ? argument.userDevice : argument.device;
+    CheckCoul(coul_buffer_upload(Context(), target, data, bytes), "UpdateBuffer of argument " + argument.id);
+}
+
+// ComputeInterface::ResizeBuffer (KTT: Source/Api/ComputeInterface.h:312-318, CudaEngine.cpp:558-569):
+// only the tuner-owned device buffer takes the new size (preserved bytes are copied on the device,
+// the rest reads as zero).  The host data keep their size; a writable argument is re-created from
+// them at the start of the next run, a cached read-only one keeps the resized buffer.
 void TunerCore::ResizeArgument(ArgumentData& argument, const size_t bytes, const bool preserve)
 {
-    if (argument.memoryType != ArgumentMemoryType::Vector || argument.ownership != ArgumentOwnership::Owned || bytes == 0)
+    if (argument.memoryType != ArgumentMemoryType::Vector || argument.ownership == ArgumentOwnership::User || bytes == 0)
     {
-        throw std::runtime_error("Only vector arguments whose data the tuner owns can be resized, to a non-zero size ("
+        throw std::runtime_error("Only vector arguments whose buffer the tuner manages can be resized, to a non-zero size ("
             + argument.id + ")");
     }
 
@@ -909,15 +942,13 @@ void TunerCore::ResizeArgument(ArgumentData& argument, const size_t bytes, const
 
     if (preserve)
     {
-        CheckCoul(coul_buffer_copy(ctx, resized, argument.device, std::min(bytes, argument.bytes)), "resize of " + argument.id);
+        CheckCoul(coul_buffer_copy(ctx, resized, argument.device, std::min(bytes, argument.deviceBytes)), "resize of " + argument.id);
     }
 
     CheckCoul(coul_synchronize(ctx), "resize of " + argument.id);
     coul_buffer_free(ctx, argument.device);
     argument.device = resized;
     argument.deviceBytes = bytes;
-    argument.owned.resize(bytes, 0);
-    argument.bytes = bytes;
     argument.deviceCurrent = true;
 }
 
@@ -928,10 +959,28 @@ void TunerCore::DownloadArgument(ArgumentData& argument, void* destination, size
         throw std::runtime_error("Argument " + argument.id + " is not a vector");
     }
 
-    bytes = bytes == 0 ? argument.bytes : std::min(bytes, argument.bytes);
     UploadArgument(argument, false);
+    bytes = bytes == 0 ? DeviceBytes(argument) : std::min(bytes, DeviceBytes(argument));
     const void* source = argument.ownership == ArgumentOwnership::User ? argument.userDevice : argument.device;
     CheckCoul(coul_buffer_download(Context(), destination, source, bytes), "download of argument " + argument.id);
+}
+
+void TunerCore::OverrideScalar(const ArgumentId& id, const void* data)
+{
+    const ArgumentData& argument = Argument(id);
+    const auto* bytes = static_cast<const uint8_t*>(data);
+    m_ScalarOverrides[id] = std::vector<uint8_t>(bytes, bytes + argument.bytes);
+}
+
+void TunerCore::ClearOverrides()
+{
+    m_ScalarOverrides.clear();
+}
+
+const void* TunerCore::ScalarData(const ArgumentData& argument) const
+{
+    auto it = m_ScalarOverrides.find(argument.id);
+    return it != m_ScalarOverrides.end() ? it->second.data() : argument.owned.data();
 }
 
 std::vector<ArgumentId> TunerCore::KernelArguments(const KernelData& kernel) const
@@ -1078,7 +1127,7 @@ Nanoseconds TunerCore::LaunchDefinition(const KernelData& kernel, const KernelDe
                 + " must be a scalar");
         }
 
-        const void* p = argument.owned.data();
+        const void* p = ScalarData(argument);
 
         switch (argument.dataType)
         {
@@ -1141,12 +1190,46 @@ Nanoseconds TunerCore::LaunchDefinition(const KernelData& kernel, const KernelDe
     const bool threeD = definition.globalSize.GetSizeZ() > 1 || global.GetSizeZ() > 1;
     int rc = COUL_OK;
 
-    if (definition.name == "directCoulombSum" && args.size() == 9 && threeD)
+    // The buffers a launch reads and writes must hold what the scalars describe; checked on the
+    // host so that a mismatched host program ends with a failed result instead of a device fault.
+    auto require = [&](const size_t i, const double bytes, const char* what)
+    {
+        if (bytes < 0.0 || static_cast<double>(DeviceBytes(Argument(args.at(i)))) < bytes)
+        {
+            throw RunFailure(ResultStatus::ComputationFailed, definition.name + ": argument " + std::to_string(i) + " ("
+                + what + ") is smaller than the sizes given by the scalar arguments");
+        }
+    };
+    auto requireAtoms = [&](const int64_t n)
+    {
+        if (parameter("USE_SOA", 0) == 0)
+        {
+            require(0, 16.0 * static_cast<double>(n), "atoms");
+        }
+        else
+        {
+            for (size_t i = 1; i <= 4; ++i)
+            {
+                require(i, 4.0 * static_cast<double>(n), "atom array");
+            }
+        }
+    };
+
+    // The nine-argument directCoulombSum is either KTT's 3D kernel, whose eighth argument is the
+    // (cubic) grid size (Examples/CoulombSum3d/CoulombSum3d.cu), or one slice of a 3D map, whose
+    // eighth argument is the slice index and which its launcher runs with a global z size of 1
+    // (Examples/CoulombSum3dIterative/CoulombSum3dIterative.cpp:146-184, .cl:36-41).
+    const bool sliceOf3d = definition.name == "directCoulombSum" && args.size() == 9
+        && (!threeD || (global.GetSizeZ() == 1 && static_cast<int64_t>(scalar(7)) != static_cast<int64_t>(definition.globalSize.GetSizeX())));
+
+    if (definition.name == "directCoulombSum" && args.size() == 9 && !sliceOf3d)
     {
         // Examples/CoulombSum3d/CoulombSum3d.cu: (atomInfo, X, Y, Z, W, numberOfAtoms, gridSpacing, gridSize, energyGrid)
         const int64_t n = static_cast<int64_t>(scalar(5));
         const int g = static_cast<int>(scalar(7));
         coul_grid grid{g, g, g, static_cast<float>(scalar(6)), {0.0f, 0.0f, 0.0f}};
+        requireAtoms(n);
+        require(8, 4.0 * g * g * static_cast<double>(g), "energy grid");
         tune.z_iterations = static_cast<int>(parameter("Z_ITERATIONS", 1));
         tune.x_points = static_cast<int>(parameter("X_POINTS", parameter("VECTOR_SIZE", 1)));
 
@@ -1167,6 +1250,8 @@ Nanoseconds TunerCore::LaunchDefinition(const KernelData& kernel, const KernelDe
         const int nx = static_cast<int>(definition.globalSize.GetSizeX());
         const int ny = static_cast<int>(definition.globalSize.GetSizeY());
         const int64_t zIndex = args.size() == 9 ? static_cast<int64_t>(scalar(7)) : 0;
+        requireAtoms(n);
+        require(args.size() - 1, 4.0 * (static_cast<double>(zIndex) + 1.0) * nx * static_cast<double>(ny), "energy grid");
         float* out = vector(args.size() - 1) + zIndex * static_cast<int64_t>(nx) * ny;
         tune.z_iterations = static_cast<int>(parameter("Y_ITERATIONS", 2));
         tune.x_points = static_cast<int>(parameter("X_POINTS", parameter("OUTER_UNROLL_FACTOR", 1)));
@@ -1178,6 +1263,8 @@ Nanoseconds TunerCore::LaunchDefinition(const KernelData& kernel, const KernelDe
         // Examples/CoulombSum3d/CoulombSum3dReference.cu: (atomInfo, numberOfAtoms, gridSpacing, gridSize, energyGrid)
         const int g = static_cast<int>(scalar(3));
         coul_grid grid{g, g, g, static_cast<float>(scalar(2)), {0.0f, 0.0f, 0.0f}};
+        require(0, 16.0 * scalar(1), "atoms");
+        require(4, 4.0 * g * g * static_cast<double>(g), "energy grid");
         rc = coul_forward_3d_reference(ctx, vector(0), static_cast<int64_t>(scalar(1)), &grid, 1, vector(4));
     }
     else if (definition.name == "directCoulombSumReference" && args.size() == 4 && threeD)
@@ -1185,6 +1272,8 @@ Nanoseconds TunerCore::LaunchDefinition(const KernelData& kernel, const KernelDe
         // Examples/CoulombSum3dIterative/CoulombSum3dIterativeReference.cl: 3D map, sizes from the global size
         coul_grid grid{static_cast<int>(definition.globalSize.GetSizeX()), static_cast<int>(definition.globalSize.GetSizeY()),
             static_cast<int>(definition.globalSize.GetSizeZ()), static_cast<float>(scalar(2)), {0.0f, 0.0f, 0.0f}};
+        require(0, 16.0 * scalar(1), "atoms");
+        require(3, 4.0 * grid.nx * static_cast<double>(grid.ny) * grid.nz, "energy grid");
         rc = coul_forward_3d_reference(ctx, vector(0), static_cast<int64_t>(scalar(1)), &grid, 1, vector(3));
     }
     else if (definition.name == "directCoulombSumReference" && args.size() == 4)
@@ -1194,6 +1283,8 @@ Nanoseconds TunerCore::LaunchDefinition(const KernelData& kernel, const KernelDe
         coul_tune_default(&reference);
         reference.z_iterations = 2;
         reference.x_points = 1;
+        require(0, 16.0 * scalar(1), "atoms");
+        require(3, 4.0 * static_cast<double>(definition.globalSize.GetSizeX()) * definition.globalSize.GetSizeY(), "energy grid");
         rc = coul_forward_2d(ctx, vector(0), static_cast<int64_t>(scalar(1)), static_cast<float>(scalar(2)),
             static_cast<int>(definition.globalSize.GetSizeX()), static_cast<int>(definition.globalSize.GetSizeY()), &reference, 0,
             vector(3));
@@ -1662,6 +1753,13 @@ KernelResult TunerCore::Run(const KernelId id, const KernelConfiguration& config
     {
         if (kernel.launcher)
         {
+            // overrides a launcher sets hold for this execution only
+            struct DropOverrides
+            {
+                TunerCore& core;
+                ~DropOverrides() { core.ClearOverrides(); }
+            } drop{*this};
+            ClearOverrides();
             ComputeLayer layer(*this, kernel, configuration, mode);
             kernel.launcher(layer);
             return layer.Results();
@@ -1813,6 +1911,31 @@ void TunerCore::SetSearcher(const KernelId id, std::unique_ptr<Searcher> searche
     Kernel(id).searcher = std::move(searcher);
 }
 
+// Operator cap on the configurations one Tune call runs, on top of the program's own stop
+// condition: KTT_B200_CONFIGURATION_LIMIT=N (a positive integer; unset, empty or 0 = no cap).  It
+// lets a KTT host program whose search space and stop condition are fixed in its source run with
+// a bounded budget.  No counterpart in KTT.
+uint64_t TunerCore::ConfigurationLimitFromEnvironment()
+{
+    const char* value = std::getenv("KTT_B200_CONFIGURATION_LIMIT");
+
+    if (value == nullptr || *value == '\0')
+    {
+        return 0;
+    }
+
+    char* end = nullptr;
+    const unsigned long long n = std::strtoull(value, &end, 10);
+
+    if (end == value || *end != '\0')
+    {
+        log::Warning(std::string("KTT_B200_CONFIGURATION_LIMIT is not a number, ignored: ") + value);
+        return 0;
+    }
+
+    return static_cast<uint64_t>(n);
+}
+
 std::vector<KernelResult> TunerCore::Tune(const KernelId id, std::unique_ptr<StopCondition> stop)
 {
     // The offline tuning loop of Source/TuningRunner/TuningRunner.cpp:17-82.
@@ -1834,9 +1957,16 @@ std::vector<KernelResult> TunerCore::Tune(const KernelId id, std::unique_ptr<Sto
 
     std::vector<KernelResult> results;
     Nanoseconds searcherOverhead = 0;
+    const uint64_t limit = ConfigurationLimitFromEnvironment();
 
     while (!space.IsExhausted())
     {
+        if (limit != 0 && results.size() >= limit)
+        {
+            log::Info("Tuning stopped after " + std::to_string(limit) + " configurations (KTT_B200_CONFIGURATION_LIMIT)");
+            break;
+        }
+
         const KernelConfiguration configuration = kernel.searcher->GetCurrentConfiguration();
         KernelResult result = Run(id, configuration, {}, KernelRunMode::OfflineTuning);
         result.SetSearcherOverhead(searcherOverhead);

@@ -186,6 +186,15 @@ public:
     void UploadArgument(ArgumentData& argument, const bool force);
     void ResizeArgument(ArgumentData& argument, const size_t bytes, const bool preserve);
     void DownloadArgument(ArgumentData& argument, void* destination, size_t bytes);
+    // Writes the argument's device buffer only; its host data stays as the caller gave it.
+    void UpdateArgumentDevice(ArgumentData& argument, const void* data, size_t bytes);
+    // Size of the buffer a launch sees (a resized device buffer keeps its new size until the run ends).
+    static size_t DeviceBytes(const ArgumentData& argument);
+    // Per-run overrides set from a launcher (KTT: ComputeLayer.cpp:160-190, AddArgumentOverride):
+    // they apply to the launches of the current run and are dropped when it ends.
+    void OverrideScalar(const ArgumentId& id, const void* data);
+    void ClearOverrides();
+    const void* ScalarData(const ArgumentData& argument) const;
 
 private:
     DeviceIndex m_Device;
@@ -215,8 +224,10 @@ private:
     std::vector<std::string> m_ProfilingCounters;  // empty: the default list
     std::set<std::string> m_UnsupportedCounters;   // reported once each
     bool m_ProfilingFailureReported = false;
+    std::map<ArgumentId, std::vector<uint8_t>> m_ScalarOverrides;  // the current run's only
 
     void ResetWritableArguments(const KernelData& kernel);
+    static uint64_t ConfigurationLimitFromEnvironment();
     std::unique_ptr<KernelProfilingData> ProfileExecution(const KernelData& kernel,
         const std::function<std::vector<ComputationResult>()>& execute);
     bool ValidateOutputs(const KernelData& kernel, const KernelConfiguration& configuration, KernelResult& result);

@@ -99,7 +99,8 @@ def compile_cubin(source: str, name: str, defines: dict | None) -> bytes:
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ktt-root", default=os.environ.get("KTT_ROOT", "/root/reference"))
+    ap.add_argument("--ktt-root", default=os.environ.get("KTT_ROOT"), required="KTT_ROOT" not in os.environ,
+                    help="KTT source tree (default: $KTT_ROOT)")
     ap.add_argument("--out", default=os.path.join(HERE, "_ref", "kernels"))
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)

@@ -2,7 +2,7 @@
 
 Run from the repository root, in a container where the KTT tree is mounted:
 
-    python tests/golden/make_golden.py [--ktt-root /root/reference]
+    python tests/golden/make_golden.py --ktt-root KTT_TREE   (or KTT_ROOT=KTT_TREE in the environment)
 
 It writes, next to this script:
 
@@ -143,7 +143,7 @@ def scripts(ktt_root: str) -> None:
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ktt-root", default="/root/reference")
+    ap.add_argument("--ktt-root", default=os.environ.get("KTT_ROOT"), required="KTT_ROOT" not in os.environ)
     args = ap.parse_args()
     kat(args.ktt_root)
     space_2080(args.ktt_root)

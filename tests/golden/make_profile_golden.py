@@ -2,7 +2,7 @@
 
 Run from the repository root where the KTT 2.1.0 tree is mounted (no GPU, no pyktt needed):
 
-    python tests/golden/make_profile_golden.py [--ktt-root /root/reference]
+    python tests/golden/make_profile_golden.py --ktt-root KTT_TREE   (or KTT_ROOT=KTT_TREE in the environment)
 
 It imports ``Scripts/ProfileBasedSearcher.py`` from the KTT tree with a stand-in ``pyktt`` module
 (only its class bodies refer to pyktt) and evaluates its functions on the recorded 2080 Ti counters
@@ -60,7 +60,7 @@ class _FixedRandom:
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ktt-root", default="/root/reference")
+    ap.add_argument("--ktt-root", default=os.environ.get("KTT_ROOT"), required="KTT_ROOT" not in os.environ)
     args = ap.parse_args()
     mod = _load_searcher_module(args.ktt_root)
     meta = json.load(open(os.path.join(args.ktt_root, "Examples", "CoulombSum3d", "Models",

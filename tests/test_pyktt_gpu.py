@@ -243,3 +243,78 @@ def test_launcher_transfers_resize_and_local_size():
     assert not got["b"][8:].any()
     assert np.array_equal(got["a"], np.full(16, 5.0, dtype=np.float32))
     assert got["profiling"] is False
+
+
+def test_launcher_updates_hold_for_one_run_only():
+    """KTT's launcher-side updates are per run (Source/KernelRunner/ComputeLayer.cpp:160-190:
+    UpdateScalarArgument / UpdateLocalArgument add argument overrides dropped with the run;
+    CudaEngine.cpp:430-470, 558-569: UpdateBuffer and ResizeBuffer change the device buffer only,
+    and writable buffers are re-created from the host data by the next run).  The first run's
+    launcher sets the atom count to 0, overwrites one buffer, resizes another and changes a local
+    size; the second run's launcher changes nothing and must see the original values."""
+    grid, n, h = 32, 96, 0.5
+    rng = np.random.default_rng(17)
+    atoms = np.empty((n, 4), dtype=np.float32)
+    atoms[:, :3] = rng.uniform(0.0, grid * h, (n, 3))
+    atoms[:, 3] = rng.uniform(-1.0, 1.0, n)
+    reference = oracle.grid3d(atoms, h, (grid, grid, grid)).reshape(-1)
+
+    tuner = ktt.Tuner(0, 0, ktt.ComputeApi.CUDA)
+    tuner.SetGlobalSizeType(ktt.GlobalSizeType.CUDA)
+    d = tuner.AddKernelDefinition("directCoulombSum", "", ktt.DimensionVector(grid, grid, grid), ktt.DimensionVector())
+    side = tuner.AddKernelDefinition("noop", "", ktt.DimensionVector(32), ktt.DimensionVector(32))
+    ro, rw = ktt.ArgumentAccessType.ReadOnly, ktt.ArgumentAccessType.ReadWrite
+    args = [tuner.AddArgumentVectorFloat(atoms.reshape(-1), ro)]
+    args += [tuner.AddArgumentVectorFloat(np.ascontiguousarray(atoms[:, c]), ro) for c in range(4)]
+    n_id = tuner.AddArgumentScalarInt(n)
+    args += [n_id, tuner.AddArgumentScalarFloat(h), tuner.AddArgumentScalarInt(grid)]
+    map_id = tuner.AddArgumentVectorFloat(np.zeros(grid ** 3, dtype=np.float32), ktt.ArgumentAccessType.WriteOnly)
+    tuner.SetArguments(d, args + [map_id])
+    aux = tuner.AddArgumentVectorFloat(np.arange(16, dtype=np.float32), rw)
+    grown = tuner.AddArgumentVectorFloat(np.arange(16, dtype=np.float32) + 100.0, rw)
+    local = tuner.AddArgumentLocalFloat(256)
+    tuner.SetArguments(side, [aux, grown, local])
+    state = {"update": True}
+    seen = []
+
+    def launcher(ci):
+        if state["update"]:
+            ci.UpdateScalarArgumentInt(n_id, 0)
+            ci.UpdateBuffer(aux, np.full(16, 5.0, dtype=np.float32))
+            ci.ResizeBuffer(grown, 128, True)
+            ci.UpdateLocalArgument(local, 512)
+        ci.RunKernel(d)
+        got_map = np.empty(grid ** 3, dtype=np.float32)
+        ci.DownloadBuffer(map_id, got_map)
+        got_aux = np.zeros(16, dtype=np.float32)
+        ci.DownloadBuffer(aux, got_aux)
+        got_grown = np.full(32, -1.0, dtype=np.float32)
+        ci.DownloadBuffer(grown, got_grown)
+        seen.append((got_map, got_aux, got_grown))
+
+    k = tuner.CreateCompositeKernel("CoulombSumWithSideBuffers", [d, side], launcher)
+    for name, value in (("WORK_GROUP_SIZE_X", 32), ("WORK_GROUP_SIZE_Y", 4), ("Z_ITERATIONS", 8),
+                        ("INNER_UNROLL_FACTOR", 2), ("USE_SOA", 0)):
+        tuner.AddParameter(k, name, [value])
+    for dim, name in ((ktt.ModifierDimension.X, "WORK_GROUP_SIZE_X"), (ktt.ModifierDimension.Y, "WORK_GROUP_SIZE_Y")):
+        tuner.AddThreadModifier(k, [d], ktt.ModifierType.Local, dim, name, ktt.ModifierAction.Multiply)
+        tuner.AddThreadModifier(k, [d], ktt.ModifierType.Global, dim, name, ktt.ModifierAction.DivideCeil)
+    tuner.AddThreadModifier(k, [d], ktt.ModifierType.Global, ktt.ModifierDimension.Z, "Z_ITERATIONS",
+                            ktt.ModifierAction.DivideCeil)
+    config = tuner.CreateConfiguration(k, [("WORK_GROUP_SIZE_X", 32), ("WORK_GROUP_SIZE_Y", 4), ("Z_ITERATIONS", 8),
+                                           ("INNER_UNROLL_FACTOR", 2), ("USE_SOA", 0)])
+    for update in (True, False):
+        state["update"] = update
+        result = tuner.Run(k, config, [])
+        assert result.GetStatus() == ktt.ResultStatus.Ok, str(result.GetStatus())
+
+    (map1, aux1, grown1), (map2, aux2, grown2) = seen
+    # first run: no atoms, the updated buffer, the resized buffer (old values kept, the rest zero)
+    assert not map1.any()
+    assert np.array_equal(aux1, np.full(16, 5.0, dtype=np.float32))
+    assert np.array_equal(grown1[:16], np.arange(16, dtype=np.float32) + 100.0) and not grown1[16:].any()
+    # second run: the original atom count, buffer contents and buffer size
+    assert errors.report(map2, reference)["rel_norm"] <= 1e-5
+    assert np.array_equal(aux2, np.arange(16, dtype=np.float32))
+    assert np.array_equal(grown2[:16], np.arange(16, dtype=np.float32) + 100.0)
+    assert np.all(grown2[16:] == -1.0)
