@@ -239,13 +239,26 @@ __device__ __forceinline__ float2 rsqrt_fma_x2(float2 x)
 // issue slot for two pairs.  The reciprocal square roots go to the MUFU unit one lane at a time,
 // or, for a static share of the lane pairs, to the FMA pipe (rsqrt_fma_x2).
 // ------------------------------------------------------------------------------------------
-// Static split between the MUFU unit and the FMA pipe: lane pair p (of the x_points * z_iterations / 2
-// pairs a thread evaluates per atom) uses the FMA pipe when (p % 8) < SOFT -- a share of SOFT / 8 for
-// 8 or 16 pairs, min(SOFT, n) / n for n < 8 pairs.
-template <int SOFT>
+// Static split between the MUFU unit and the FMA pipe.  A thread evaluates NP = x_points *
+// ceil(z_iterations / 2) lane pairs per atom.  The atoms are taken in groups of soft_group(NP) =
+// max(1, 8 / NP) consecutive atoms, which together hold 8 (or, for NP >= 8, NP) pair slots; slot
+// s = (atom's phase in the group) * NP + p for NP < 8, s = p % 8 otherwise, and a slot takes the
+// FMA pipe when s < SOFT.  The share is SOFT / 8 at every tile size.  From kSoftAlternate on
+// (SOFT = kSoftAlternate + k) two such groups alternate between k and k + 1 soft slots, a share of
+// (2k + 1) / 16.  soft_phases is the number of consecutive atoms one whole pattern spans.
+constexpr int kSoftAlternate = 10;
+constexpr int soft_group(int np) { return np >= 8 ? 1 : 8 / np; }
+constexpr int soft_phases(int soft, int np)
+{
+    return soft == 0 ? 1 : (soft >= kSoftAlternate ? 2 : 1) * soft_group(np);
+}
+
+template <int SOFT, int NP, int PHASE>
 __device__ __forceinline__ constexpr bool pair_is_soft(int p)
 {
-    return (p & 7) < SOFT;
+    constexpr int G = soft_group(NP);
+    constexpr int base = SOFT >= kSoftAlternate ? SOFT - kSoftAlternate + PHASE / G : SOFT;
+    return (NP >= 8 ? (p & 7) : (PHASE % G) * NP + p) < base;
 }
 
 __device__ __forceinline__ float2 rsqrt_mufu_x2(float2 r2)
@@ -253,8 +266,55 @@ __device__ __forceinline__ float2 rsqrt_mufu_x2(float2 r2)
     return make_float2(rsqrt_mufu(r2.x), rsqrt_mufu(r2.y));
 }
 
+// One lane pair: acc += q / sqrt(r2) lane-wise, the rsqrt on the FMA pipe when SOFT_PAIR (the charge
+// then comes pre-scaled by kSoftRsqrtScale in qs2).  HALF_PAIR: only the .x lane holds a point (an
+// odd number of points along the blocked axis); it is evaluated alone, so no rsqrt is spent on a
+// point that is never stored.
+template <bool SOFT_PAIR, bool HALF_PAIR>
+__device__ __forceinline__ void pair_update(float2 r2, float2 q2, float2 qs2, float2& acc)
+{
+    if constexpr (HALF_PAIR) {
+        if constexpr (SOFT_PAIR)
+            acc.x = fmaf(qs2.x, rsqrt_fma(r2.x), acc.x);
+        else
+            acc.x = fmaf(q2.x, rsqrt_mufu(r2.x), acc.x);
+    } else {
+        if constexpr (SOFT_PAIR)
+            acc = __ffma2_rn(qs2, rsqrt_fma_x2(r2), acc);
+        else
+            acc = __ffma2_rn(q2, rsqrt_mufu_x2(r2), acc);
+    }
+}
+
+// Unrolled k (x point), i (lane pair of the blocked axis) loops with the soft/MUFU choice and the
+// half pair resolved at compile time.  r2 per pair from the per-k term pk and the per-i term pi:
+//   SQUARE_I (3D):  r2 = pi^2 + pk   (pi = dz of the two points, pk = dx^2 + dy^2)
+//   else (2D):      r2 = pk^2 + pi   (pk = dx, pi = dy^2 + dz^2 of the two rows)
+template <bool SQUARE_I, int XP, int ZH, int SOFT, int PHASE, bool HALF, int K = 0, int I = 0>
+__device__ __forceinline__ void pair_rows(const float (&pk)[XP], const float2 (&pi)[ZH], float2 q2, float2 qs2,
+                                          float2 (&acc)[XP][ZH])
+{
+    if constexpr (K < XP) {
+        if constexpr (I < ZH) {
+            constexpr bool soft = SOFT != 0 && pair_is_soft<SOFT, XP * ZH, PHASE>(K * ZH + I);
+            constexpr bool half = HALF && I == ZH - 1;
+            if constexpr (half) {
+                const float r2 = SQUARE_I ? fmaf(pi[I].x, pi[I].x, pk[K]) : fmaf(pk[K], pk[K], pi[I].x);
+                pair_update<soft, true>(make_float2(r2, 0.0f), q2, qs2, acc[K][I]);
+            } else {
+                const float2 r2 = SQUARE_I ? __ffma2_rn(pi[I], pi[I], splat(pk[K]))
+                                           : __ffma2_rn(splat(pk[K]), splat(pk[K]), pi[I]);
+                pair_update<soft, false>(r2, q2, qs2, acc[K][I]);
+            }
+            pair_rows<SQUARE_I, XP, ZH, SOFT, PHASE, HALF, K, I + 1>(pk, pi, q2, qs2, acc);
+        } else {
+            pair_rows<SQUARE_I, XP, ZH, SOFT, PHASE, HALF, K + 1, 0>(pk, pi, q2, qs2, acc);
+        }
+    }
+}
+
 // 3D: thread owns points (gx[k], gy, gz[i].x / gz[i].y); acc[k][i] += q / |r - a| lane-wise.
-template <int XP, int ZH, int SOFT>
+template <int XP, int ZH, int SOFT, int PHASE, bool HALF>
 __device__ __forceinline__ void pair_block_3d(const float (&gx)[XP], float gy, const float2 (&gz)[ZH], float4 a,
                                               float2 (&acc)[XP][ZH])
 {
@@ -271,37 +331,12 @@ __device__ __forceinline__ void pair_block_3d(const float (&gx)[XP], float gy, c
 #pragma unroll
     for (int i = 0; i < ZH; ++i)
         dz[i] = __fadd2_rn(gz[i], naz);
-    const float2 q2 = splat(a.w);
-    if constexpr (SOFT == 0) {
-#pragma unroll
-        for (int k = 0; k < XP; ++k) {
-            const float2 w = splat(dxy[k]);
-#pragma unroll
-            for (int i = 0; i < ZH; ++i) {
-                const float2 r2 = __ffma2_rn(dz[i], dz[i], w);
-                acc[k][i] = __ffma2_rn(q2, rsqrt_mufu_x2(r2), acc[k][i]);
-            }
-        }
-    } else {
-        const float2 qs2 = splat(a.w * kSoftRsqrtScale);
-#pragma unroll
-        for (int k = 0; k < XP; ++k) {
-            const float2 w = splat(dxy[k]);
-#pragma unroll
-            for (int i = 0; i < ZH; ++i) {
-                const float2 r2 = __ffma2_rn(dz[i], dz[i], w);
-                if (pair_is_soft<SOFT>(k * ZH + i))
-                    acc[k][i] = __ffma2_rn(qs2, rsqrt_fma_x2(r2), acc[k][i]);
-                else
-                    acc[k][i] = __ffma2_rn(q2, rsqrt_mufu_x2(r2), acc[k][i]);
-            }
-        }
-    }
+    pair_rows<true, XP, ZH, SOFT, PHASE, HALF>(dxy, dz, splat(a.w), splat(a.w * kSoftRsqrtScale), acc);
 }
 
 // 2D slice (KTT's 2D convention): thread owns points (gx[k], gy[i].x / gy[i].y) of one slice, the
 // atom's .z holds the squared z distance c; acc[k][i] += q / sqrt(dx^2 + dy^2 + c) lane-wise.
-template <int XP, int YH, int SOFT>
+template <int XP, int YH, int SOFT, int PHASE, bool HALF>
 __device__ __forceinline__ void pair_block_2d(const float (&gx)[XP], const float2 (&gy)[YH], float4 a,
                                               float2 (&acc)[XP][YH])
 {
@@ -317,32 +352,7 @@ __device__ __forceinline__ void pair_block_2d(const float (&gx)[XP], const float
 #pragma unroll
     for (int k = 0; k < XP; ++k)
         dx[k] = gx[k] - a.x;
-    const float2 q2 = splat(a.w);
-    if constexpr (SOFT == 0) {
-#pragma unroll
-        for (int k = 0; k < XP; ++k) {
-            const float2 u = splat(dx[k]);
-#pragma unroll
-            for (int i = 0; i < YH; ++i) {
-                const float2 r2 = __ffma2_rn(u, u, dyc[i]);
-                acc[k][i] = __ffma2_rn(q2, rsqrt_mufu_x2(r2), acc[k][i]);
-            }
-        }
-    } else {
-        const float2 qs2 = splat(a.w * kSoftRsqrtScale);
-#pragma unroll
-        for (int k = 0; k < XP; ++k) {
-            const float2 u = splat(dx[k]);
-#pragma unroll
-            for (int i = 0; i < YH; ++i) {
-                const float2 r2 = __ffma2_rn(u, u, dyc[i]);
-                if (pair_is_soft<SOFT>(k * YH + i))
-                    acc[k][i] = __ffma2_rn(qs2, rsqrt_fma_x2(r2), acc[k][i]);
-                else
-                    acc[k][i] = __ffma2_rn(q2, rsqrt_mufu_x2(r2), acc[k][i]);
-            }
-        }
-    }
+    pair_rows<false, XP, YH, SOFT, PHASE, HALF>(dx, dyc, splat(a.w), splat(a.w * kSoftRsqrtScale), acc);
 }
 
 // Knuth's two-sum: s + e == a + b exactly (round-to-nearest, no contraction of additions).

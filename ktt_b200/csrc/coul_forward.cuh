@@ -36,20 +36,26 @@ struct FwdLaunch {
     int split;      // atom-split form: CTAs per cluster sharing one point tile (0 / 1 = one CTA per tile)
 };
 
-// rsqrt_soft values from kSoftAlternate on: consecutive atoms alternate between k and k + 1 of every
-// 8 lane pairs on the FMA pipe, k = SOFT - kSoftAlternate, a share of (2k + 1) / 16 for 8-pair tiles.
-constexpr int kSoftAlternate = 10;
-constexpr int soft_even(int soft) { return soft >= kSoftAlternate ? soft - kSoftAlternate : soft; }
-constexpr int soft_odd(int soft) { return soft >= kSoftAlternate ? soft - kSoftAlternate + 1 : soft; }
-
-template <int MODE, int XP, int ZH, int SOFT>
+template <int MODE, int XP, int ZH, int SOFT, int PHASE, bool HALF>
 __device__ __forceinline__ void eval_atom(const float (&gx)[XP], float gy, const float2 (&gb)[ZH], float4 a,
                                           float2 (&dst)[XP][ZH])
 {
     if constexpr (MODE == kModeGrid3d)
-        pair_block_3d<XP, ZH, SOFT>(gx, gy, gb, a, dst);
+        pair_block_3d<XP, ZH, SOFT, PHASE, HALF>(gx, gy, gb, a, dst);
     else
-        pair_block_2d<XP, ZH, SOFT>(gx, gb, a, dst);
+        pair_block_2d<XP, ZH, SOFT, PHASE, HALF>(gx, gb, a, dst);
+}
+
+// The atoms j0 .. j0 + P - 1 of one pattern of the FMA-pipe share (P = soft_phases), each with its
+// phase in the pattern.
+template <int MODE, int XP, int ZH, int SOFT, bool HALF, int PHASE, int P, class AtomAt>
+__device__ __forceinline__ void eval_group(const float (&gx)[XP], float gy, const float2 (&gb)[ZH], const AtomAt& at,
+                                           const int j0, float2 (&dst)[XP][ZH])
+{
+    if constexpr (PHASE < P) {
+        eval_atom<MODE, XP, ZH, SOFT, PHASE, HALF>(gx, gy, gb, at(j0 + PHASE), dst);
+        eval_group<MODE, XP, ZH, SOFT, HALF, PHASE + 1, P>(gx, gy, gb, at, j0, dst);
+    }
 }
 
 __device__ __forceinline__ float lane(const float2& v, int l) { return l == 0 ? v.x : v.y; }
@@ -128,9 +134,11 @@ __device__ __forceinline__ bool tile_accumulate(const FwdParams& p, const int x0
 #pragma unroll
     for (int k = 0; k < XP; ++k)
         gx[k] = fmaf(static_cast<float>(x0 + k), p.h, p.ox);
-    // Blocked-axis points in lane pairs: (z0 + 2i, z0 + 2i + 1) in 3D, rows in 2D.  With ZI == 1
-    // the second lane evaluates the next point, which is never stored.
+    // Blocked-axis points in lane pairs: (z0 + 2i, z0 + 2i + 1) in 3D, rows in 2D.  With an odd ZI
+    // the last pair holds one point (HALF), evaluated on its own.
     constexpr int ZH = (ZI + 1) / 2;
+    constexpr bool HALF = (ZI & 1) != 0;
+    constexpr int P = soft_phases(SOFT, XP * ZH);  // atoms per whole pattern of the FMA-pipe share
     float2 gb[ZH];
     float gy;
     if constexpr (MODE == kModeGrid3d) {
@@ -196,18 +204,17 @@ __device__ __forceinline__ bool tile_accumulate(const FwdParams& p, const int x0
         (void)full;
         (void)gstage;
         const int n = static_cast<int>(p.n_atoms);
-        if constexpr (SOFT >= kSoftAlternate) {
+        if constexpr (P > 1) {
+            auto at = [](int j) { return c_atoms[j]; };
             int j = 0;
-            for (; j + 1 < n; j += 2) {
-                eval_atom<MODE, XP, ZH, soft_even(SOFT)>(gx, gy, gb, c_atoms[j], acc);
-                eval_atom<MODE, XP, ZH, soft_odd(SOFT)>(gx, gy, gb, c_atoms[j + 1], acc);
-            }
-            if (j < n)
-                eval_atom<MODE, XP, ZH, soft_even(SOFT)>(gx, gy, gb, c_atoms[j], acc);
+            for (; j + P <= n; j += P)
+                eval_group<MODE, XP, ZH, SOFT, HALF, 0, P>(gx, gy, gb, at, j, acc);
+            for (; j < n; ++j)  // the last, partial pattern
+                eval_atom<MODE, XP, ZH, SOFT, 0, HALF>(gx, gy, gb, c_atoms[j], acc);
         } else {
 #pragma unroll UNR
             for (int j = 0; j < n; ++j)
-                eval_atom<MODE, XP, ZH, SOFT>(gx, gy, gb, c_atoms[j], acc);
+                eval_atom<MODE, XP, ZH, SOFT, 0, HALF>(gx, gy, gb, c_atoms[j], acc);
         }
     } else {
         const int nthreads = blockDim.x * blockDim.y;
@@ -299,34 +306,19 @@ __device__ __forceinline__ bool tile_accumulate(const FwdParams& p, const int x0
                     return make_float4(f[j], f[kTileAtoms + j], f[2 * kTileAtoms + j], f[3 * kTileAtoms + j]);
                 }
             };
-            // the stage is padded to kTileAtoms (an even count), so the alternating form pairs atoms
-            constexpr int kPairUnroll = UNR > 1 ? UNR / 2 : 1;
+            // the stage is padded to kTileAtoms, a multiple of every pattern length P (at most 16)
+            static_assert(kSubTile % 16 == 0, "sub-tiles hold whole patterns of the FMA-pipe share");
+            constexpr int kGroupUnroll = UNR > P ? UNR / P : 1;
             if constexpr (PREC == kPrecFp32) {
-                if constexpr (SOFT >= kSoftAlternate) {
-#pragma unroll kPairUnroll
-                    for (int j = 0; j < kTileAtoms; j += 2) {
-                        eval_atom<MODE, XP, ZH, soft_even(SOFT)>(gx, gy, gb, atom_at(j), acc);
-                        eval_atom<MODE, XP, ZH, soft_odd(SOFT)>(gx, gy, gb, atom_at(j + 1), acc);
-                    }
-                } else {
-#pragma unroll UNR
-                    for (int j = 0; j < kTileAtoms; ++j)
-                        eval_atom<MODE, XP, ZH, SOFT>(gx, gy, gb, atom_at(j), acc);
-                }
+#pragma unroll kGroupUnroll
+                for (int j = 0; j < kTileAtoms; j += P)
+                    eval_group<MODE, XP, ZH, SOFT, HALF, 0, P>(gx, gy, gb, atom_at, j, acc);
             } else {
                 for (int j0 = 0; j0 < kTileAtoms; j0 += kSubTile) {
                     clear_part();
-                    if constexpr (SOFT >= kSoftAlternate) {
-#pragma unroll kPairUnroll
-                        for (int j = 0; j < kSubTile; j += 2) {
-                            eval_atom<MODE, XP, ZH, soft_even(SOFT)>(gx, gy, gb, atom_at(j0 + j), part);
-                            eval_atom<MODE, XP, ZH, soft_odd(SOFT)>(gx, gy, gb, atom_at(j0 + j + 1), part);
-                        }
-                    } else {
-#pragma unroll UNR
-                        for (int j = 0; j < kSubTile; ++j)
-                            eval_atom<MODE, XP, ZH, SOFT>(gx, gy, gb, atom_at(j0 + j), part);
-                    }
+#pragma unroll kGroupUnroll
+                    for (int j = 0; j < kSubTile; j += P)
+                        eval_group<MODE, XP, ZH, SOFT, HALF, 0, P>(gx, gy, gb, atom_at, j0 + j, part);
                     merge();
                 }
             }
