@@ -53,6 +53,17 @@ def _chosen_tune():
     return ktt_b200.Tune(), "built-in default"
 
 
+def _soft_share(tune) -> float:
+    """Share of the pairs whose rsqrt runs on the FMA pipe (coul_tune.rsqrt_soft), for the thread
+    tile's x_points * z_iterations / 2 lane pairs."""
+    pairs = max(1, tune.x_points * tune.z_iterations // 2)
+    soft = tune.rsqrt_soft
+    if soft >= 10:
+        k = soft - 10
+        return (2 * k + 1) / 16.0 if pairs >= 8 else (min(k, pairs) + min(k + 1, pairs)) / (2.0 * pairs)
+    return soft / 8.0 if pairs >= 8 else min(soft, pairs) / pairs
+
+
 class ClockSampler:
     """nvidia-smi clock / throttle-reason sampling during the timed region."""
 
@@ -234,7 +245,9 @@ def run_ours(args) -> None:
         ms = [a.elapsed_time(b) for a, b in evs]
         return max_over_ranks(sum(ms)), ms
 
-    rsqrt_rate, ffma_rate = ctx.pipe_rates()
+    rates = ctx.pipe_rates_ex()
+    rsqrt_rate = rates["rsqrt_per_s"]
+    ffma_rate = max(rates["ffma_per_s"], rates["ffma2_lanes_per_s"])
 
     with ClockSampler(dev.index) as clocks:
         total_ms, step_ms = timed_steps(chosen, args.steps, args.warmup)
@@ -277,15 +290,39 @@ def run_ours(args) -> None:
     r_pipe = (rsqrt_rate + (ffma_rate - 2 * rsqrt_rate) / (2 + SOFT_FP32_OPS)) / 1e9
     r_comb = rsqrt_rate * (fm - 1 + s) / (2 + s) / 1e9
     peak = max(r_pipe, r_comb)
+    # The same two formulas on datasheet lane counts (sm_100: 128 FP32 lanes and 16 MUFU results per
+    # SM per clock) at the SM clock sampled during the timed steps (the maximum clock if unsampled).
+    sm_hz = 1e6 * (clk["sm_mhz"] if clk else rates["max_sm_clock_khz"] / 1e3)
+    m_ds = 16.0 * rates["sm_count"] * sm_hz
+    f_ds = 128.0 * rates["sm_count"] * sm_hz
+    r_pipe_ds = (m_ds + (f_ds - 2 * m_ds) / (2 + SOFT_FP32_OPS)) / 1e9
+    r_comb_ds = m_ds * (f_ds / m_ds - 1 + s) / (2 + s) / 1e9
+    peak_ds = max(r_pipe_ds, r_comb_ds)
+    # Issue model of the chosen form: a MUFU instruction costs c issue slots, measured from the MUFU
+    # rate left with six FMAs beside each rsqrt (128 thread-instructions per SM per clock:
+    # rate_mix * (c + 6) = 128 S f); per pair the packed FP32 work takes one slot, an FMA-pipe rsqrt
+    # SOFT_ISSUE_SLOTS / 2 + 1 slots (half of the packed instructions, all of the integer ones).
+    issue_rate = 128.0 * rates["sm_count"] * sm_hz
+    c_mufu = max(1.0, issue_rate / rates["rsqrt_mix6_per_s"] - 6.0)
+    phi = 1.0 - _soft_share(chosen)
+    soft_slots = 5.0
+    r_issue = min(rsqrt_rate / phi if phi > 0 else float("inf"),
+                  issue_rate / (1.0 + phi * c_mufu + (1.0 - phi) * soft_slots)) / 1e9
     traffic = _load_traffic()
     roofline = {
         "bound": "mufu+fma", "achieved": achieved, "peak": peak, "unit": UNIT, "frac": achieved / peak,
         "traffic": traffic.get("bytes_per_launch") if traffic else None,
-        "peak_source": "measured in this run: MUFU rsqrt and FP32 FMA throughput microkernels; "
-                       "peak = max(R_pipe, R_comb)",
+        "peak_source": "measured in this run: MUFU rsqrt and FP32 FMA (the larger of scalar FFMA and packed "
+                       "FFMA2) throughput microkernels; peak = max(R_pipe, R_comb)",
         "peak_pipe": r_pipe, "peak_comb": r_comb, "frac_comb": achieved / r_comb,
         "peak_mufu_only": r_mufu, "frac_mufu_only": achieved / r_mufu,
-        "rsqrt_per_s": rsqrt_rate, "ffma_per_s": ffma_rate, "soft_rsqrt_issue_slots": s,
+        "peak_datasheet": peak_ds, "frac_datasheet": achieved / peak_ds,
+        "datasheet_source": f"128 FP32 lanes + 16 MUFU/clk/SM x {rates['sm_count']} SMs x {sm_hz / 1e6:.0f} MHz, "
+                            "max(R_pipe, R_comb)",
+        "peak_issue_model": r_issue, "frac_issue_model": achieved / r_issue,
+        "mufu_issue_slots": c_mufu, "mufu_share": phi,
+        "rsqrt_per_s": rsqrt_rate, "ffma_per_s": rates["ffma_per_s"], "ffma2_lanes_per_s": rates["ffma2_lanes_per_s"],
+        "rsqrt_mix6_per_s": rates["rsqrt_mix6_per_s"], "soft_rsqrt_issue_slots": s,
         "soft_rsqrt_fp32_ops": SOFT_FP32_OPS,
         "plain_achieved": plain_value / world, "plain_frac": plain_value / world / peak,
     }

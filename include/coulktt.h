@@ -224,6 +224,17 @@ COUL_API int coul_forward_3d_soa(coul_ctx* ctx, const float* d_x, const float* d
 COUL_API int coul_forward_3d_reference(coul_ctx* ctx, const float* d_atoms, int64_t n_atoms,
                                        const coul_grid* grid, int accumulate, float* d_out);
 /*
+ * The same map evaluated in FP64 on the GPU, for validating configurations while tuning (KTT's
+ * Coulomb examples validate against a reference kernel, Examples/CoulombSum3d/CoulombSum3d.cpp:
+ * 221-227; KTT registers CPU reference computations through Tuner::SetReferenceComputation,
+ * Source/Tuner.h:610).  One point per thread; the FP32 grid coordinates (as the tiled kernels form
+ * them) and atoms widened to double, then differences, squares, square root and division in FP64,
+ * accumulated in FP64; d_out holds nx * ny * nz doubles (assigned).  Slow (no MUFU, no register
+ * blocking): a checker, not a product form.
+ */
+COUL_API int coul_forward_3d_reference_fp64(coul_ctx* ctx, const float* d_atoms, int64_t n_atoms,
+                                            const coul_grid* grid, double* d_out);
+/*
  * 2D slice in KTT's 2D argument convention: d_atoms holds (x, y, dz2, q) with
  * dz2 the squared z distance of the atom to the slice.  out[j*nx + i] over an
  * nx * ny slice with spacing h and zero origin.  tune->z_iterations is the
@@ -338,9 +349,11 @@ COUL_API int coul_batch_info(const coul_batch* batch, int64_t* work_items, int* 
  *   - at most 1024 molecules per call (larger batches are rejected with COUL_ERR_INVALID_ARGUMENT);
  *   - tile shapes (z_iterations/x_points/unroll/precision/rsqrt_soft, any block up to 256 threads):
  *     8/2/2/0/2, 8/2/1/0/0, 16/1/1/0/2; others return COUL_ERR_UNSUPPORTED;
- *   - the first call on a device looks up the device address of the static array
- *     (cudaGetSymbolAddress) with that device current; make that first call before any stream
- *     capture;
+ *   - the array exists once per CUDA context that loads the library (the device's primary context,
+ *     or a context of the caller's own, current on the calling thread); every call looks up its
+ *     device address in the current context (cudaGetSymbolAddress, a lookup that allocates
+ *     nothing).  The first call in a context also loads the library's device code into it: make
+ *     that first call before any stream capture;
  *   - every call shares the one array and leaves its table behind; calls whose kernels overlap on
  *     the GPU (different streams without ordering) race on it and give wrong maps.
  * Returns after enqueueing (the molecule table is copied from host memory before it returns).
@@ -358,6 +371,28 @@ COUL_API int coul_batch_run_static(void* stream, const coul_molecule* molecules,
  * Source/ComputeEngine/Cuda/Cupti/CuptiMetricInterface.cpp:621-660.)
  */
 COUL_API int coul_measure_pipe_rates(coul_ctx* ctx, double* rsqrt_per_s, double* ffma_per_s);
+
+/* The same microkernels and three more, reported separately (no counterpart in the reference):
+ *   rsqrt_per_s        MUFU rsqrt.approx.f32 results per second;
+ *   ffma_per_s         FP32 FMAs per second issued as scalar FFMA;
+ *   ffma2_lanes_per_s  FP32 FMAs per second issued as packed FFMA2 (two per instruction), the form
+ *                      the pair kernels use; coul_measure_pipe_rates reports the larger of the two;
+ *   dfma_per_s         FP64 FMAs per second;
+ *   rsqrt_mix6_per_s   MUFU rsqrts per second when six independent FP32 FMAs issue beside each one
+ *                      (with one issue slot per MUFU instruction this would equal rsqrt_per_s; the
+ *                      drop measures what a MUFU instruction costs in issue slots);
+ *   sm_count, max_sm_clock_khz  the device's SM count and its maximum SM clock, for the datasheet
+ *                      lane rates (128 FP32 lanes and 16 MUFU results per SM per clock on sm_100). */
+typedef struct coul_pipe_rates {
+    double rsqrt_per_s;
+    double ffma_per_s;
+    double ffma2_lanes_per_s;
+    double dfma_per_s;
+    double rsqrt_mix6_per_s;
+    int sm_count;
+    int max_sm_clock_khz;
+} coul_pipe_rates;
+COUL_API int coul_measure_pipe_rates_ex(coul_ctx* ctx, coul_pipe_rates* out);
 
 /* ---- hardware counters ----------------------------------------------------------- */
 /*

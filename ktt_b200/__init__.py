@@ -48,6 +48,13 @@ class _Tune(ctypes.Structure):
                 ("precision", ctypes.c_int), ("rsqrt_soft", ctypes.c_int), ("atom_split", ctypes.c_int)]
 
 
+class _PipeRates(ctypes.Structure):
+    _fields_ = [("rsqrt_per_s", ctypes.c_double), ("ffma_per_s", ctypes.c_double),
+                ("ffma2_lanes_per_s", ctypes.c_double), ("dfma_per_s", ctypes.c_double),
+                ("rsqrt_mix6_per_s", ctypes.c_double), ("sm_count", ctypes.c_int),
+                ("max_sm_clock_khz", ctypes.c_int)]
+
+
 class _Grid(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int), ("spacing", ctypes.c_float),
                 ("origin", ctypes.c_float * 3)]
@@ -123,11 +130,13 @@ def load_library():
         "coul_forward_3d_slab": [vp, vp, i64, G, ci, ci, T, ci, vp],
         "coul_forward_3d_soa": [vp, vp, vp, vp, vp, i64, G, T, ci, vp],
         "coul_forward_3d_reference": [vp, vp, i64, G, ci, vp],
+        "coul_forward_3d_reference_fp64": [vp, vp, i64, G, vp],
         "coul_forward_2d": [vp, vp, i64, cf, ci, ci, T, ci, vp],
         "coul_slice_atoms": [vp, vp, i64, cf, vp],
         "coul_forward_3d_host": [vp, vp, i64, G, T, vp],
         "coul_probe_bounded_wait": [vp, ci, ctypes.c_uint64],
         "coul_measure_pipe_rates": [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)],
+        "coul_measure_pipe_rates_ex": [vp, ctypes.POINTER(_PipeRates)],
     }
     for name, args in sig.items():
         fn = getattr(lib, name)
@@ -237,10 +246,18 @@ class CoulombContext:
         return int(self._lib.coul_probe_bounded_wait(self._ctx, 1 if arrive else 0, int(budget_ns)))
 
     def pipe_rates(self) -> tuple[float, float]:
-        """(MUFU rsqrt/s, FP32 FMA/s) of the whole GPU, measured now by throughput microkernels."""
+        """(MUFU rsqrt/s, FP32 FMA/s) of the whole GPU, measured now by throughput microkernels (the
+        FMA rate is the larger of the scalar and the packed-FFMA2 rate)."""
         m, f = ctypes.c_double(), ctypes.c_double()
         _check(self._lib.coul_measure_pipe_rates(self._ctx, ctypes.byref(m), ctypes.byref(f)))
         return m.value, f.value
+
+    def pipe_rates_ex(self) -> dict:
+        """All pipe rates of coul_measure_pipe_rates_ex (per second, whole GPU) with the SM count and
+        the maximum SM clock."""
+        r = _PipeRates()
+        _check(self._lib.coul_measure_pipe_rates_ex(self._ctx, ctypes.byref(r)))
+        return {name: getattr(r, name) for name, _ in _PipeRates._fields_}
 
     def synchronize(self) -> None:
         _check(self._lib.coul_synchronize(self._ctx))
@@ -315,6 +332,22 @@ class CoulombContext:
         g = _grid(dims, spacing, origin)
         _check(self._lib.coul_forward_3d_reference(self._ctx, _ptr(atoms), atoms.shape[0], ctypes.byref(g),
                                                    1 if accumulate else 0, _ptr(out)))
+        return out
+
+    def forward_3d_reference_fp64(self, atoms, dims, spacing, origin=None, out=None):
+        """The map in FP64 (float64 tensor of shape (nz, ny, nx)), one point per thread: the
+        validation kernel of coul_forward_3d_reference_fp64."""
+        import torch
+        self._check_atoms(atoms)
+        nx, ny, nz = (int(d) for d in dims)
+        if out is None:
+            out = torch.empty((nz, ny, nx), dtype=torch.float64, device=atoms.device)
+        elif out.dtype != torch.float64 or not out.is_contiguous() or out.numel() != nx * ny * nz:
+            raise ValueError("out must be a contiguous float64 tensor of nx * ny * nz elements")
+        self._bind_stream()
+        g = _grid(dims, spacing, origin)
+        _check(self._lib.coul_forward_3d_reference_fp64(self._ctx, _ptr(atoms), atoms.shape[0], ctypes.byref(g),
+                                                        _ptr(out)))
         return out
 
     def forward_2d(self, atoms_xy_dz2_q, spacing, nx, ny, tune: Tune | None = None, out=None,

@@ -12,9 +12,13 @@ parameters with thread modifiers and constraints -- with the B200 parameters add
 RSQRT_SOFT) and a constraint that keeps the search inside the compiled variants; the batched map is
 the tuner's "coulombBatch" definition.  KTT's searchers pick the configurations (MCMC by default,
 Examples' ConfigurationCount budget), every configuration is validated by the tuner against a
-reference computation (the FP64-merge map, SideBySide within 1e-5 of the largest value), and the
-fastest valid configuration is written to ktt_b200/tuned/b200_map3d.json or b200_batch.json with
---save (the files bench.py and ktt_b200.Batch read).
+reference computation registered through Tuner::SetReferenceComputation (Source/Tuner.h:610;
+SideBySide within 1e-5 of the largest value), and the fastest valid configuration is written to
+ktt_b200/tuned/b200_map3d.json or b200_batch.json with --save (the files bench.py and
+ktt_b200.Batch read).  The reference computation is the caller's (tune_map3d / tune_batch take an
+FP64 map function, e.g. a CPU restatement of KTT's reference computation); without one it is the
+library's FP64 reference kernel (coul_forward_3d_reference_fp64: one point per thread, FP64
+differences, square root and division), which shares no arithmetic with the tuned kernels.
 """
 from __future__ import annotations
 
@@ -116,11 +120,35 @@ def _summary(results, work):
     return best, trials
 
 
+REFERENCE_KERNEL = "FP64 reference kernel (coul_forward_3d_reference_fp64)"
+
+
+def _fp64_maps(problems, reference):
+    """FP64 maps of (atoms, dims, spacing, origin) problems: reference(atoms, spacing, dims, origin) when
+    given, else the FP64 reference kernel on the GPU."""
+    if reference is not None:
+        return [np.asarray(reference(a, h, dims, origin), dtype=np.float64) for a, dims, h, origin in problems]
+    import torch
+
+    import ktt_b200
+    ctx = ktt_b200.CoulombContext(0)
+    try:
+        maps = []
+        for a, dims, h, origin in problems:
+            v = ctx.forward_3d_reference_fp64(torch.from_numpy(a).cuda(), dims, h, origin)
+            maps.append(v.cpu().numpy())
+        return maps
+    finally:
+        ctx.close()
+
+
 def tune_map3d(grid: int = 256, atoms: int = 65536, searcher: str = "mcmc", budget: int = 60,
                dry_run: bool = False, profile: bool = False, results_path: str = "", model: str = "",
-               seed: int | None = None) -> dict:
+               seed: int | None = None, reference=None, reference_name: str = "") -> dict:
     """Searches the single-map tile space on the uniform workload (grid^3 points at 0.5 A, `atoms` atoms
-    uniform in the cube the grid spans).  dry_run: only build the space and report its size."""
+    uniform in the cube the grid spans).  dry_run: only build the space and report its size.
+    reference(atoms, spacing, dims, origin) -> FP64 map of shape (nz, ny, nx) is the reference
+    computation every configuration is validated against (default: the FP64 reference kernel)."""
     import ktt_b200
     from ktt_b200 import pyktt as ktt
     from ktt_b200 import workloads
@@ -142,12 +170,7 @@ def tune_map3d(grid: int = 256, atoms: int = 65536, searcher: str = "mcmc", budg
     arg_ids.append(grid_id)
     tuner.SetArguments(definition, arg_ids)
 
-    import torch
-    ctx = ktt_b200.CoulombContext(0)
-    reference = ctx.forward_3d(torch.from_numpy(w.atoms).cuda(), w.dims, h,
-                               tune=ktt_b200.Tune(z_iterations=8, x_points=2, precision=ktt_b200.PREC_FP64_MERGE))
-    ref = reference.cpu().numpy().reshape(-1)
-    ctx.close()
+    ref = _fp64_maps([(w.atoms, w.dims, h, None)], reference)[0].reshape(-1)
 
     def compute_reference(buffer):
         np.frombuffer(buffer, dtype=np.float32)[:] = ref
@@ -160,7 +183,9 @@ def tune_map3d(grid: int = 256, atoms: int = 65536, searcher: str = "mcmc", budg
     out = {
         "workload": f"{g}^3 grid, h={h} A, {n} atoms uniform in the {g * h:g} A cube",
         "device": tuner.GetCurrentDeviceInfo().GetName(),
-        "selection": "fastest configuration whose map stays within 1e-5 of the largest value of the FP64-merge map",
+        "selection": "fastest configuration whose map stays within 1e-5 of the largest value of the FP64 reference "
+                     "map at every point",
+        "reference": reference_name or (REFERENCE_KERNEL if reference is None else "caller's FP64 reference computation"),
         "source": f"ktt_b200.autotune map3d: {searcher} searcher, {len(results)} of "
                   f"{tuner.GetConfigurationsCount(kernel)} configurations, kernel time from the tuner's event pair",
         "gpairs_per_s": round(best["gpairs_per_s"], 1),
@@ -172,11 +197,10 @@ def tune_map3d(grid: int = 256, atoms: int = 65536, searcher: str = "mcmc", budg
 
 def tune_batch(molecules: int = 512, seed: int = 4, searcher: str = "mcmc", budget: int = 40,
                dry_run: bool = False, profile: bool = False, results_path: str = "", model: str = "",
-               search_seed: int | None = None) -> dict:
+               search_seed: int | None = None, reference=None, reference_name: str = "") -> dict:
     """Searches the batched-map tile space (the coulombBatch definition) on the uneven molecule batch
-    (`molecules` molecules of 200-20000 atoms, log-uniform, from `seed`)."""
-    import torch
-
+    (`molecules` molecules of 200-20000 atoms, log-uniform, from `seed`); reference as in tune_map3d,
+    applied to every molecule."""
     import ktt_b200
     from ktt_b200 import pyktt as ktt
     from ktt_b200 import workloads
@@ -205,14 +229,11 @@ def tune_batch(molecules: int = 512, seed: int = 4, searcher: str = "mcmc", budg
     ids += [maps_id, tuner.AddArgumentVectorLong(map_off, ro), tuner.AddArgumentScalarInt(len(mols))]
     tuner.SetArguments(definition, ids)
 
-    ctx = ktt_b200.CoulombContext(0)
     ref = np.zeros(int(map_off[-1]), dtype=np.float32)
-    fp64 = ktt_b200.Tune(z_iterations=8, x_points=2, precision=ktt_b200.PREC_FP64_MERGE)
+    maps = _fp64_maps([(m.atoms, m.dims, m.spacing, m.origin) for m in mols], reference)
     for i, m in enumerate(mols):
-        v = ctx.forward_3d(torch.from_numpy(m.atoms).cuda(), m.dims, m.spacing, m.origin, tune=fp64)
         size = m.dims[0] * m.dims[1] * m.dims[2]
-        ref[map_off[i]:map_off[i] + size] = v.cpu().numpy().reshape(-1)
-    ctx.close()
+        ref[map_off[i]:map_off[i] + size] = maps[i].reshape(-1)
 
     def compute_reference(buffer):
         np.frombuffer(buffer, dtype=np.float32)[:] = ref
@@ -228,6 +249,7 @@ def tune_batch(molecules: int = 512, seed: int = 4, searcher: str = "mcmc", budg
         "workload": f"{len(mols)} molecules, seed {seed}, margin 8 A per side",
         "source": f"ktt_b200.autotune batch: {searcher} searcher, {len(results)} of "
                   f"{tuner.GetConfigurationsCount(kernel)} configurations of the coulombBatch definition",
+        "reference": reference_name or (REFERENCE_KERNEL if reference is None else "caller's FP64 reference computation"),
         "trials": trials,
     }
 

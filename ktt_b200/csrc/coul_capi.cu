@@ -75,6 +75,45 @@ __global__ void reference_kernel(const float4* __restrict__ atoms, int64_t n, in
     out[o] = accumulate ? out[o] + e : e;
 }
 
+// FP64 evaluation of the same sum, one point per thread, for validation: grid coordinates formed
+// as the tiled kernels form them (one FP32 fma), then widened; every difference, square, the square
+// root and the division in FP64 (correctly rounded), accumulated in FP64.  Atoms pass through shared
+// memory in tiles of kRefTile by plain loads.  No register blocking and no MUFU: independent of the
+// tiled kernels' arithmetic, so it can validate them during tuning.
+constexpr int kRefTile = 256;
+
+__global__ void __launch_bounds__(256) reference_fp64_kernel(const float4* __restrict__ atoms, int64_t n, int nx,
+                                                             int ny, int nz, float h, float ox, float oy, float oz,
+                                                             double* __restrict__ out)
+{
+    __shared__ float4 tile[kRefTile];
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z;
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    const int nthreads = blockDim.x * blockDim.y;
+    const double gx = static_cast<double>(fmaf(static_cast<float>(x), h, ox));
+    const double gy = static_cast<double>(fmaf(static_cast<float>(y), h, oy));
+    const double gz = static_cast<double>(fmaf(static_cast<float>(z), h, oz));
+    double e = 0.0;
+    for (int64_t base = 0; base < n; base += kRefTile) {
+        const int cnt = static_cast<int>(n - base < kRefTile ? n - base : kRefTile);
+        __syncthreads();
+        for (int j = tid; j < cnt; j += nthreads)
+            tile[j] = atoms[base + j];
+        __syncthreads();
+        for (int j = 0; j < cnt; ++j) {
+            const float4 a = tile[j];
+            const double dx = gx - static_cast<double>(a.x);
+            const double dy = gy - static_cast<double>(a.y);
+            const double dz = gz - static_cast<double>(a.z);
+            e += static_cast<double>(a.w) / sqrt(dx * dx + dy * dy + dz * dz);
+        }
+    }
+    if (x < nx && y < ny && z < nz)
+        out[(static_cast<int64_t>(z) * ny + y) * nx + x] = e;
+}
+
 // (x, y, z, q) -> (x, y, (z_slice - z)^2, q): KTT's 2D convention, computed on the device
 // (the iterative example does it on the host per slice: CoulombSum3dIterative.cpp:160-179).
 __global__ void slice_atoms_kernel(const float4* __restrict__ in, int64_t n, float zs, float4* __restrict__ out)
@@ -661,6 +700,33 @@ COUL_API int coul_forward_3d_reference(coul_ctx* ctx, const float* d_atoms, int6
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess)
         return cuda_error(e, "reference launch");
+    return ctx_end_timing(ctx);
+}
+
+COUL_API int coul_forward_3d_reference_fp64(coul_ctx* ctx, const float* d_atoms, int64_t n_atoms,
+                                            const coul_grid* grid, double* d_out)
+{
+    if (ctx == nullptr)
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    int rc = validate_grid(grid);
+    if (rc)
+        return rc;
+    if (n_atoms < 0 || d_out == nullptr || (n_atoms > 0 && (d_atoms == nullptr || !aligned16(d_atoms))))
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "bad atoms or output");
+    if (grid->nz > 65535)
+        return set_error(COUL_ERR_DEVICE_LIMITS, "nz above 65535");
+    if ((rc = ctx_activate(ctx)))
+        return rc;
+    const dim3 block(16, 16, 1);
+    const dim3 g((grid->nx + 15) / 16, (grid->ny + 15) / 16, grid->nz);
+    if ((rc = ctx_begin_timing(ctx)))
+        return rc;
+    reference_fp64_kernel<<<g, block, 0, ctx->stream>>>(reinterpret_cast<const float4*>(d_atoms), n_atoms, grid->nx,
+                                                        grid->ny, grid->nz, grid->spacing, grid->origin[0],
+                                                        grid->origin[1], grid->origin[2], d_out);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess)
+        return cuda_error(e, "FP64 reference launch");
     return ctx_end_timing(ctx);
 }
 

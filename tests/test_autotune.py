@@ -2,11 +2,15 @@
 
 CPU: both tile spaces build through the tuner (parameters, KTT's thread modifiers, the block-size
 constraint and the compiled-variant constraint) and every configuration the space keeps is one the
-library accepts.  GPU: a short MCMC / random search on small workloads validates every configuration
-against the FP64-merge map and returns a configuration whose map is then checked against the oracle.
+library accepts.  GPU: a short MCMC / random search on small workloads with the FP64 oracle registered
+as the tuner's reference computation (Tuner::SetReferenceComputation) validates every configuration
+against it and returns a configuration whose map is then checked against the oracle again; the
+library's FP64 reference kernel (the default reference computation) agrees with the oracle.  Opt-in
+(KTT_AUTOTUNE_OUT=path): the full 256^3 x 65,536 search validated against the oracle, written to path.
 """
 import itertools
 import json
+import os
 import subprocess
 import sys
 
@@ -51,13 +55,29 @@ def test_cli_dry_run():
     assert json.loads(out.strip().splitlines()[-1])["configurations"] > 0
 
 
+class _Spy:
+    """The oracle as a reference computation, counting its calls."""
+
+    def __init__(self):
+        import oracle
+        self.fn = oracle.grid3d
+        self.calls = 0
+
+    def __call__(self, atoms, spacing, dims, origin):
+        self.calls += 1
+        return self.fn(atoms, spacing, dims, origin)
+
+
 @pytest.mark.gpu
 def test_map3d_search_short():
     import torch
 
     import oracle
     from ktt_b200 import workloads
-    result = autotune.tune_map3d(grid=64, atoms=2048, searcher="mcmc", budget=8)
+    spy = _Spy()
+    result = autotune.tune_map3d(grid=64, atoms=2048, searcher="mcmc", budget=8, reference=spy,
+                                 reference_name="FP64 oracle (oracle/coulomb_oracle.c)")
+    assert spy.calls == 1 and result["reference"] == "FP64 oracle (oracle/coulomb_oracle.c)"
     valid = [t for t in result["trials"] if t["gpairs_per_s"] is not None]
     assert len(result["trials"]) == 8 and len(valid) == 8
     tune = ktt_b200.Tune(**result["tune"])
@@ -74,7 +94,45 @@ def test_map3d_search_short():
 
 @pytest.mark.gpu
 def test_batch_search_short():
-    result = autotune.tune_batch(molecules=12, seed=7, searcher="random", budget=6)
+    spy = _Spy()
+    result = autotune.tune_batch(molecules=12, seed=7, searcher="random", budget=6, reference=spy)
+    assert spy.calls == 12
     assert len(result["trials"]) == 6
     assert all(t["status"] == "Ok" for t in result["trials"]), result["trials"]
     assert ktt_b200.batch_tune_supported(ktt_b200.Tune(**result["batched"]))
+
+
+@pytest.mark.gpu
+def test_fp64_reference_kernel_matches_the_oracle():
+    import torch
+
+    import oracle
+    from ktt_b200 import workloads
+    w = workloads.uniform_map(n_atoms=1500, n=40, box=20.0)
+    dims = (40, 36, 28)
+    origin = (-1.5, 0.25, 2.0)
+    ref = oracle.grid3d(w.atoms, w.spacing, dims, origin)
+    ctx = ktt_b200.CoulombContext(0)
+    try:
+        got = ctx.forward_3d_reference_fp64(torch.from_numpy(w.atoms).cuda(), dims, w.spacing, origin).cpu().numpy()
+    finally:
+        ctx.close()
+    assert got.shape == ref.shape
+    assert np.max(np.abs(got - ref)) <= 1e-12 * np.max(np.abs(ref))
+    # the default reference computation of the autotuner is this kernel
+    maps = autotune._fp64_maps([(w.atoms, dims, w.spacing, origin)], None)
+    assert np.max(np.abs(maps[0] - ref)) <= 1e-12 * np.max(np.abs(ref))
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not os.environ.get("KTT_AUTOTUNE_OUT"), reason="the full search is opt-in")
+def test_full_map3d_search_validated_against_the_oracle():
+    """The search behind ktt_b200/tuned/b200_map3d.json: 256^3 x 65,536 atoms, MCMC, every configuration
+    validated against the FP64 oracle's full map (about 100 s on 16 host cores, once)."""
+    result = autotune.tune_map3d(grid=256, atoms=65536, searcher="mcmc",
+                                 budget=int(os.environ.get("KTT_AUTOTUNE_BUDGET", "150")), reference=_Spy(),
+                                 reference_name="FP64 oracle (oracle/coulomb_oracle.c), full map")
+    with open(os.environ["KTT_AUTOTUNE_OUT"], "w") as f:
+        json.dump(result, f, indent=1)
+        f.write("\n")
+    assert ktt_b200.tune_supported(ktt_b200.Tune(**result["tune"]))
