@@ -44,13 +44,39 @@ SOFT_ISSUE_SLOTS = 8  # FMA-pipe rsqrt: 2 integer + 6 FP32 instructions
 SOFT_FP32_OPS = 6     # of which FP32 operations on the FMA pipe
 
 
+# The FP64-pair form's tile (the fastest of the compiled FP64-pair shapes on this map) and its cost.
+EXACT_TUNE = dict(block_x=64, block_y=1, z_iterations=8, x_points=4, unroll=1, precision=3)
+EXACT_FP64_OPS = 6
+
+
 def _chosen_tune():
+    """The headline form: the autotuner's fastest configuration among the forms that pass the gate
+    (ktt_b200/tuned/b200_map3d.json)."""
     import ktt_b200
     path = os.path.join(REPO, "ktt_b200", "tuned", "b200_map3d.json")
     if os.path.exists(path):
         with open(path) as f:
             return ktt_b200.Tune(**json.load(f)["tune"]), os.path.relpath(path, REPO)
-    return ktt_b200.Tune(), "built-in default"
+    return ktt_b200.Tune(z_iterations=8, x_points=2, precision=2, rsqrt_soft=2), "built-in default"
+
+
+def _fast_fp32_tune():
+    """The fastest FP32-accumulation configuration the autotuner recorded (the same file's fast_fp32
+    entry), else the headline tile with FP32 accumulation."""
+    import ktt_b200
+    path = os.path.join(REPO, "ktt_b200", "tuned", "b200_map3d.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        if "fast_fp32" in d:
+            return ktt_b200.Tune(**d["fast_fp32"]["tune"])
+    t, _ = _chosen_tune()
+    t.precision = ktt_b200.PREC_FP32
+    return t if ktt_b200.tune_supported(t) else ktt_b200.Tune(z_iterations=8, x_points=2, unroll=2, rsqrt_soft=2)
+
+
+def _dtype(tune) -> str:
+    return {0: "f32", 1: "f32 pairs, compensated f32 sums", 2: "f32 pairs, f64 merge", 3: "f64 pairs"}[tune.precision]
 
 
 def _soft_share(tune) -> float:
@@ -172,6 +198,90 @@ def _load_traffic() -> dict | None:
     return None
 
 
+def _ktt_kernel_live(w, atoms, out, flush, steps: int, check_map) -> dict | None:
+    """KTT's own CUDA kernels timed in this run on the same map, beside the product (a comparison, not
+    the reference arm): Examples/CoulombSum3d/CoulombSum3d.cu at the best configuration of its
+    210-configuration space on B200 (profiles/ktt_kernel_space_b200.json) and
+    CoulombSum3dReference.cu, each compiled from the KTT tree the way KTT compiles them (NVRTC,
+    "#define" prefix, -use_fast_math; `make -C oracle refkernels`) and launched through the CUDA driver
+    with KTT's geometry (CoulombSum3d.cpp:70-72, 145-181).  Both kernels accumulate (+=), so the map
+    is cleared before every launch, outside the event pair.  None when the kernels were not built."""
+    import ctypes
+
+    import torch
+    kdir = os.path.join(REPO, "oracle", "_ref", "kernels")
+    rec = os.path.join(REPO, "profiles", "ktt_kernel_space_b200.json")
+    if not (os.path.exists(os.path.join(kdir, "manifest.json")) and os.path.exists(rec)):
+        return None
+    from cuda.bindings import driver as cu
+
+    def ok(res):
+        err = res[0] if isinstance(res, tuple) else res
+        if err != cu.CUresult.CUDA_SUCCESS:
+            raise RuntimeError(f"CUDA driver call failed: {err}")
+        return res[1] if isinstance(res, tuple) and len(res) > 1 else None
+
+    with open(os.path.join(kdir, "manifest.json")) as f:
+        manifest = json.load(f)["kernels"]
+    with open(rec) as f:
+        best = json.load(f)["best"]
+
+    def function(fname, name):
+        mod = ok(cu.cuModuleLoad(os.path.join(kdir, fname).encode()))
+        return ok(cu.cuModuleGetFunction(mod, manifest.get(fname, {}).get("function", name).encode())), mod
+
+    g = w.dims[0]
+    n = w.atoms.shape[0]
+    cols = [atoms[:, c].contiguous() for c in range(4)]
+    stream = torch.cuda.current_stream()
+    cs = cu.CUstream(stream.cuda_stream)
+    wx, wy, z = best["WORK_GROUP_SIZE_X"], best["WORK_GROUP_SIZE_Y"], best["Z_ITERATIONS"]
+    tuned_fn, tuned_mod = function(f"coulomb3d_z{z}_u{best['INNER_UNROLL_FACTOR']}_soa{best['USE_SOA']}.cubin",
+                                   "directCoulombSum")
+    ref_fn, ref_mod = function("coulomb3d_reference.cubin", "directCoulombSumReference")
+    tuned_args = ((atoms.data_ptr(), *(c.data_ptr() for c in cols), n, float(w.spacing), g, out.data_ptr()),
+                  (ctypes.c_void_p,) * 5 + (ctypes.c_int, ctypes.c_float, ctypes.c_int, ctypes.c_void_p))
+    ref_args = ((atoms.data_ptr(), n, float(w.spacing), g, out.data_ptr()),
+                (ctypes.c_void_p, ctypes.c_int, ctypes.c_float, ctypes.c_int, ctypes.c_void_p))
+
+    def launch(which):
+        if which == "tuned":
+            ok(cu.cuLaunchKernel(tuned_fn, -(-g // wx), -(-g // wy), -(-g // z), wx, wy, 1, 0, cs, tuned_args, 0))
+        else:
+            ok(cu.cuLaunchKernel(ref_fn, g // 16, g // 16, g, 16, 16, 1, 0, cs, ref_args, 0))
+
+    result = {}
+    for which in ("tuned", "reference"):
+        out.zero_()
+        launch(which)  # warm-up
+        ms = []
+        for _ in range(steps):
+            flush.zero_()
+            out.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            launch(which)
+            b.record(stream)
+            ms.append((a, b))
+        torch.cuda.synchronize()
+        t = [x.elapsed_time(y) for x, y in ms]
+        diff = float((out - check_map).abs().max() / check_map.abs().max())
+        result[which] = {"value": w.pairs / (1e-3 * sum(t) / len(t)) / 1e9, "ms_per_launch": sum(t) / len(t),
+                         "max_diff_vs_product_map_rel": diff}
+    ok(cu.cuModuleUnload(tuned_mod))
+    ok(cu.cuModuleUnload(ref_mod))
+    return {"value": result["tuned"]["value"], "unit": UNIT,
+            "config": {k: best[k] for k in ("WORK_GROUP_SIZE_X", "WORK_GROUP_SIZE_Y", "Z_ITERATIONS",
+                                            "INNER_UNROLL_FACTOR", "USE_SOA")},
+            "ms_per_launch": result["tuned"]["ms_per_launch"],
+            "max_diff_vs_product_map_rel": result["tuned"]["max_diff_vs_product_map_rel"],
+            "reference_kernel": {"value": result["reference"]["value"], "unit": UNIT,
+                                 "ms_per_launch": result["reference"]["ms_per_launch"]},
+            "source": "measured in this run: KTT's CoulombSum3d.cu (best configuration of its space on B200) and "
+                      "CoulombSum3dReference.cu, compiled from the KTT tree as KTT compiles them, same map, "
+                      "CUDA events, L2 flushed between launches"}
+
+
 def _ktt_kernel_recorded() -> dict | None:
     """KTT's own CUDA kernel on this map, best of its 210-configuration space, as recorded on B200."""
     path = os.path.join(REPO, "profiles", "ktt_kernel_space_b200.json")
@@ -224,6 +334,8 @@ def run_ours(args) -> None:
                           x_points=chosen.x_points, unroll=chosen.unroll)
     if not ktt_b200.tune_supported(plain):
         plain = ktt_b200.Tune()
+    fast = _fast_fp32_tune()
+    exact = ktt_b200.Tune(**EXACT_TUNE)
 
     def timed_steps(tune, steps, warmup):
         for _ in range(warmup):
@@ -255,9 +367,16 @@ def run_ours(args) -> None:
     value = world * pairs * args.steps / (total_ms * 1e-3) / 1e9
     chosen_map = out.clone()
 
-    plain_ms, _ = timed_steps(plain, max(2, args.steps // 2), 1)
-    plain_value = world * pairs * max(2, args.steps // 2) / (plain_ms * 1e-3) / 1e9
+    side_steps = max(2, args.steps // 2)
+    plain_ms, _ = timed_steps(plain, side_steps, 1)
+    plain_value = world * pairs * side_steps / (plain_ms * 1e-3) / 1e9
     plain_map = out.clone()
+    fast_ms, _ = timed_steps(fast, side_steps, 1)
+    fast_value = world * pairs * side_steps / (fast_ms * 1e-3) / 1e9
+    fast_map = out.clone()
+    exact_ms, exact_step_ms = timed_steps(exact, side_steps, 1)
+    exact_value = world * pairs * side_steps / (exact_ms * 1e-3) / 1e9
+    exact_map = out.clone()
 
     # end to end through the host-buffer C ABI call, pinned host memory
     h_atoms = torch.from_numpy(w.atoms).pin_memory()
@@ -327,16 +446,37 @@ def run_ours(args) -> None:
         "plain_achieved": plain_value / world, "plain_frac": plain_value / world / peak,
     }
 
+    # The FP64-pair form is bound by the FP64 pipe: six FP64 operations per pair (r^2, the Newton step's
+    # four, the accumulation), from the FP64 FMA rate measured in this run.
+    exact_achieved = pairs / (1e-3 * sum(exact_step_ms) / len(exact_step_ms)) / 1e9
+    exact_peak = rates["dfma_per_s"] / EXACT_FP64_OPS / 1e9
+    exact_roofline = {"bound": "fp64", "achieved": exact_achieved, "peak": exact_peak, "unit": UNIT,
+                      "frac": exact_achieved / exact_peak, "dfma_per_s": rates["dfma_per_s"],
+                      "fp64_ops_per_pair": EXACT_FP64_OPS,
+                      "peak_source": "measured in this run: FP64 FMA throughput microkernel / 6"}
+
+    live = None
+    if rank == 0 and world == 1 and not args.no_ktt_kernel:
+        try:
+            live = _ktt_kernel_live(w, atoms, out, flush, side_steps, exact_map)
+        except Exception as exc:  # the comparison leg must not end the benchmark
+            live = {"unavailable": f"{type(exc).__name__}: {exc}"}
+
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32" if chosen.precision == ktt_b200.PREC_FP32 else "f32 pairs, f64 merge",
+        "dtype": _dtype(chosen),
         "data": "synthetic (seeded)",
         "config": {"workload": WORKLOAD, "pairs_per_step_per_gpu": pairs, "tune": chosen.as_dict(),
                    "tune_source": chosen_src, "l2": "flushed between timed steps (256 MiB write)",
                    "parallelism": f"replicas x{world} (each rank its own map)"},
-        "plain": {"value": plain_value, "unit": UNIT, "tune": plain.as_dict()},
-        "ktt_kernel": _ktt_kernel_recorded(),
+        "plain": {"value": plain_value, "unit": UNIT, "tune": plain.as_dict(), "dtype": _dtype(plain),
+                  "what": "KTT's kernel form: FP32, every rsqrt on MUFU"},
+        "fast_fp32": {"value": fast_value, "unit": UNIT, "tune": fast.as_dict(), "dtype": _dtype(fast),
+                      "what": "FP32 accumulation with the FMA-pipe rsqrt share (fastest form; fails the pointwise gate)"},
+        "exact": {"value": exact_value, "unit": UNIT, "tune": exact.as_dict(), "dtype": _dtype(exact),
+                  "what": "FP64 pairs: pointwise within the strict floor", "roofline": exact_roofline},
+        "ktt_kernel": live if live else _ktt_kernel_recorded(),
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(w.atoms.nbytes),
                 "d2h_bytes_per_step": int(nx * ny * nz * 4), "api": "coul_forward_3d_host (pinned host buffers)"},
         "gpu_launches": args.steps,
@@ -365,9 +505,14 @@ def run_ours(args) -> None:
         if kat:
             line["cpu_baseline"]["reference_generator"] = kat
         line["accuracy"] = {
-            "chosen": errors.report(chosen_map.cpu().numpy().reshape(-1)[idx], ref, sumabs=sabs),
-            "plain": errors.report(plain_map.cpu().numpy().reshape(-1)[idx], ref, sumabs=sabs),
-            "points": len(idx), "tolerance_rel_norm": 1e-5,
+            "chosen": errors.gate(chosen_map.cpu().numpy().reshape(-1)[idx], ref, sumabs=sabs),
+            "plain": errors.gate(plain_map.cpu().numpy().reshape(-1)[idx], ref, sumabs=sabs),
+            "fast_fp32": errors.gate(fast_map.cpu().numpy().reshape(-1)[idx], ref, sumabs=sabs),
+            "exact": errors.gate(exact_map.cpu().numpy().reshape(-1)[idx], ref, sumabs=sabs),
+            "points": len(idx), "tolerance": errors.TOLERANCE,
+            "gate": f"max |dV| / max |V*| <= {errors.TOLERANCE:g} and max |dV| / max(|V*|, floor) <= "
+                    f"{errors.TOLERANCE:g}, floor = {errors.GATE_FLOOR_RMS:g} rms(V*); strict floor "
+                    f"{errors.STRICT_FLOOR_RMS:g} rms(V*) reported as rel_point_strict",
         }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -405,6 +550,7 @@ def main() -> None:
     # the 1,024-point calibration underestimates the threaded rate about 2x, so 30 gives ~15 s of work
     ap.add_argument("--cpu-seconds", type=float, default=30.0, help="size of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ktt-kernel", action="store_true", help="skip the live comparison with KTT's own kernels")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -77,11 +77,15 @@ enum {
     COUL_ATOMS_CONSTANT = 1    /* chunks of 4096 atoms copied into __constant__ memory */
 };
 
-/* Accumulation form.  All forms evaluate each pair in FP32. */
+/* Precision form.  The first three evaluate each pair in FP32 and differ in how they accumulate;
+   the fourth evaluates each pair in FP64. */
 enum {
     COUL_PREC_FP32 = 0,        /* one FP32 accumulator per point (KTT's kernel) */
     COUL_PREC_COMPENSATED = 1, /* FP32 partial per atom sub-tile, merged by two-sum into (sum, error) */
-    COUL_PREC_FP64_MERGE = 2   /* FP32 partial per atom sub-tile, merged into an FP64 accumulator */
+    COUL_PREC_FP64_MERGE = 2,  /* FP32 partial per atom sub-tile, merged into an FP64 accumulator */
+    COUL_PREC_FP64_PAIRS = 3   /* every pair in FP64: exact differences, FP64 r^2, MUFU rsqrt estimate
+                                  refined by one FP64 Newton step (about 2^-40), FP64 accumulation; the
+                                  map's error is then its FP32 store.  3D maps, rsqrt_soft 0 only */
 };
 
 /*
@@ -98,14 +102,15 @@ typedef struct coul_tune {
     int unroll;       /* unroll of the atom loop; 0 and 1 mean none [INNER_UNROLL_FACTOR] */
     int atom_source;  /* COUL_ATOMS_*                          [USE_CONSTANT_MEMORY] */
     int precision;    /* COUL_PREC_* */
-    int rsqrt_soft;   /* how many of every 8 point pairs a thread evaluates per atom take their
-                         reciprocal square root on the FMA pipe (Newton iterations) instead of the
-                         MUFU unit (0 = all MUFU).  A thread evaluates x_points * z_iterations points
-                         per atom in pairs; with n pairs, pair p is on the FMA pipe when (p % 8) <
-                         rsqrt_soft, so the share is rsqrt_soft / 8 for n = 8 or 16 and
-                         min(rsqrt_soft, n) / n below 8 pairs (e.g. 1 x 8 points: 2 -> 2 of 4).
-                         10 + k (k = 0..7): consecutive atoms alternate between k and k + 1 of every
-                         8 pairs, a share of (2k + 1) / 16 for 8-pair tiles */
+    int rsqrt_soft;   /* share of the reciprocal square roots taken on the FMA pipe (Newton
+                         iterations) instead of the MUFU unit, in eighths (0 = all MUFU).  A thread
+                         evaluates x_points * z_iterations points per atom in n lane pairs; within one
+                         stage of 256 atoms each pair keeps one form for every atom.  With n >= 8, pair
+                         p is on the FMA pipe when (p % 8) < rsqrt_soft; with n < 8 the stages take
+                         turns in 8 / n phases and pair p of a stage in phase g is on the FMA pipe
+                         when g * n + p < rsqrt_soft.  Either way the share is rsqrt_soft / 8.
+                         10 + k (k = 0..7): successive patterns alternate between k and k + 1 eighths,
+                         a share of (2k + 1) / 16 */
     int atom_split;   /* 0 or 1: one CTA per point tile; 2..16: a thread-block cluster of that many
                          CTAs shares each point tile, each streaming 1/atom_split of the atoms, the
                          partial sums reduced over distributed shared memory (for slices and small

@@ -34,6 +34,7 @@ ATOMS_CONSTANT = 1
 PREC_FP32 = 0
 PREC_COMPENSATED = 1
 PREC_FP64_MERGE = 2
+PREC_FP64_PAIRS = 3
 
 
 class CoulombError(RuntimeError):

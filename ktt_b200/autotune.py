@@ -58,14 +58,17 @@ def _tune_from(values, names):
     import ktt_b200
     v = dict(zip(names, values))
     return ktt_b200.Tune(block_x=v["WORK_GROUP_SIZE_X"], block_y=v["WORK_GROUP_SIZE_Y"], z_iterations=v["Z_ITERATIONS"],
-                         x_points=v["X_POINTS"], unroll=_unroll(v["INNER_UNROLL_FACTOR"]), rsqrt_soft=v["RSQRT_SOFT"])
+                         x_points=v["X_POINTS"], unroll=_unroll(v["INNER_UNROLL_FACTOR"]), rsqrt_soft=v["RSQRT_SOFT"],
+                         precision=v.get("PRECISION", 0))
 
 
-def _add_space(ktt, tuner, kernel, definition, space, supported):
+def _add_space(ktt, tuner, kernel, definition, space, supported, precisions=(0,)):
+    """The space's parameters, PRECISION (the accumulation forms searched), KTT's thread modifiers and
+    the constraints."""
+    space = dict(space, PRECISION=list(precisions))
     names = list(space)
     for name, values in space.items():
         tuner.AddParameter(kernel, name, values)
-    tuner.AddParameter(kernel, "PRECISION", [0])
     # KTT's thread modifiers of the 3D example (the launch sizes recorded in the results)
     for dim, name in ((ktt.ModifierDimension.X, "WORK_GROUP_SIZE_X"), (ktt.ModifierDimension.Y, "WORK_GROUP_SIZE_Y")):
         tuner.AddThreadModifier(kernel, [definition], ktt.ModifierType.Local, dim, name, ktt.ModifierAction.Multiply)
@@ -144,7 +147,7 @@ def _fp64_maps(problems, reference):
 
 def tune_map3d(grid: int = 256, atoms: int = 65536, searcher: str = "mcmc", budget: int = 60,
                dry_run: bool = False, profile: bool = False, results_path: str = "", model: str = "",
-               seed: int | None = None, reference=None, reference_name: str = "") -> dict:
+               seed: int | None = None, reference=None, reference_name: str = "", precisions=(0,)) -> dict:
     """Searches the single-map tile space on the uniform workload (grid^3 points at 0.5 A, `atoms` atoms
     uniform in the cube the grid spans).  dry_run: only build the space and report its size.
     reference(atoms, spacing, dims, origin) -> FP64 map of shape (nz, ny, nx) is the reference
@@ -158,7 +161,7 @@ def tune_map3d(grid: int = 256, atoms: int = 65536, searcher: str = "mcmc", budg
     tuner.SetGlobalSizeType(ktt.GlobalSizeType.CUDA)
     definition = tuner.AddKernelDefinition("directCoulombSum", "", ktt.DimensionVector(g, g, g), ktt.DimensionVector())
     kernel = tuner.CreateSimpleKernel("CoulombSum", definition)
-    _add_space(ktt, tuner, kernel, definition, MAP3D_SPACE, ktt_b200.tune_supported)
+    _add_space(ktt, tuner, kernel, definition, MAP3D_SPACE, ktt_b200.tune_supported, precisions)
     if dry_run:
         return {"configurations": tuner.GetConfigurationsCount(kernel)}
 
@@ -189,7 +192,9 @@ def tune_map3d(grid: int = 256, atoms: int = 65536, searcher: str = "mcmc", budg
         "source": f"ktt_b200.autotune map3d: {searcher} searcher, {len(results)} of "
                   f"{tuner.GetConfigurationsCount(kernel)} configurations, kernel time from the tuner's event pair",
         "gpairs_per_s": round(best["gpairs_per_s"], 1),
-        "tune": _tune_from([best["config"][k] for k in MAP3D_SPACE], list(MAP3D_SPACE)).as_dict(),
+        "precisions": list(precisions),
+        "tune": _tune_from([best["config"][k] for k in list(MAP3D_SPACE) + ["PRECISION"]],
+                           list(MAP3D_SPACE) + ["PRECISION"]).as_dict(),
         "trials": trials,
     }
     return out
@@ -209,7 +214,7 @@ def tune_batch(molecules: int = 512, seed: int = 4, searcher: str = "mcmc", budg
     tuner.SetGlobalSizeType(ktt.GlobalSizeType.CUDA)
     definition = tuner.AddKernelDefinition("coulombBatch", "", ktt.DimensionVector(1, 1, 2), ktt.DimensionVector())
     kernel = tuner.CreateSimpleKernel("CoulombBatch", definition)
-    _add_space(ktt, tuner, kernel, definition, BATCH_SPACE, ktt_b200.batch_tune_supported)
+    _add_space(ktt, tuner, kernel, definition, BATCH_SPACE, ktt_b200.batch_tune_supported, (0,))
     if dry_run:
         return {"configurations": tuner.GetConfigurationsCount(kernel)}
 
@@ -244,7 +249,8 @@ def tune_batch(molecules: int = 512, seed: int = 4, searcher: str = "mcmc", budg
     pairs = float(sum(m.pairs for m in mols))
     best, trials = _summary(results, pairs)
     return {
-        "batched": _tune_from([best["config"][k] for k in BATCH_SPACE], list(BATCH_SPACE)).as_dict(),
+        "batched": _tune_from([best["config"][k] for k in list(BATCH_SPACE) + ["PRECISION"]],
+                              list(BATCH_SPACE) + ["PRECISION"]).as_dict(),
         "batched_gpairs_per_s": round(best["gpairs_per_s"], 1),
         "workload": f"{len(mols)} molecules, seed {seed}, margin 8 A per side",
         "source": f"ktt_b200.autotune batch: {searcher} searcher, {len(results)} of "
@@ -268,6 +274,7 @@ def main() -> None:
     ap.add_argument("--molecules", type=int, default=512)
     ap.add_argument("--seed", type=int, default=4)
     ap.add_argument("--dry-run", action="store_true", help="report the configuration space only")
+    ap.add_argument("--precisions", default="0", help="accumulation forms to search (map3d), e.g. 1,2")
     ap.add_argument("--save", action="store_true", help="write ktt_b200/tuned/b200_<target>.json")
     ap.add_argument("--out", default="", help="write the result to this file instead")
     args = ap.parse_args()
@@ -277,7 +284,8 @@ def main() -> None:
     ktt.Tuner.SetLoggingLevel(ktt.LoggingLevel.Warning)
     if args.target == "map3d":
         result = tune_map3d(args.grid, args.atoms, args.searcher, args.budget, args.dry_run, args.profile,
-                            args.results, args.model, args.search_seed)
+                            args.results, args.model, args.search_seed,
+                            precisions=tuple(int(p) for p in args.precisions.split(",")))
     else:
         result = tune_batch(args.molecules, args.seed, args.searcher, args.budget, args.dry_run, args.profile,
                             args.results, args.model, args.search_seed)

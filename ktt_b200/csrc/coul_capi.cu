@@ -38,6 +38,8 @@ std::vector<VariantEntry>& registry()
         register_fwd_3d_precise(v);
         register_fwd_3d_soft(v);
         register_fwd_3d_soft_precise(v);
+        register_fwd_3d_soft_fp64m(v);
+        register_fwd_3d_fp64(v);
         register_fwd_2d(v);
         register_fwd_split(v);
     });
@@ -238,7 +240,7 @@ int validate_tune(const coul_tune* t, int mode, int soa, const VariantEntry** ou
                                                      std::to_string(kMaxThreads) + " threads");
     if (t->atom_source != COUL_ATOMS_SHARED_TMA && t->atom_source != COUL_ATOMS_CONSTANT)
         return set_error(COUL_ERR_INVALID_ARGUMENT, "unknown atom_source");
-    if (t->precision < COUL_PREC_FP32 || t->precision > COUL_PREC_FP64_MERGE)
+    if (t->precision < COUL_PREC_FP32 || t->precision > COUL_PREC_FP64_PAIRS)
         return set_error(COUL_ERR_INVALID_ARGUMENT, "unknown precision");
     if (t->rsqrt_soft < 0 || (t->rsqrt_soft > 8 && t->rsqrt_soft < kSoftAlternate) || t->rsqrt_soft > kSoftAlternate + 7)
         return set_error(COUL_ERR_INVALID_ARGUMENT, "rsqrt_soft must be in 0..8 or 10..17");

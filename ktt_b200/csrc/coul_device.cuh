@@ -21,6 +21,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 namespace coul {
 
 constexpr int kTileAtoms = 256;       // atoms per shared-memory stage
@@ -240,17 +242,34 @@ __device__ __forceinline__ float2 rsqrt_fma_x2(float2 x)
 // or, for a static share of the lane pairs, to the FMA pipe (rsqrt_fma_x2).
 // ------------------------------------------------------------------------------------------
 // Static split between the MUFU unit and the FMA pipe.  A thread evaluates NP = x_points *
-// ceil(z_iterations / 2) lane pairs per atom.  The atoms are taken in groups of soft_group(NP) =
-// max(1, 8 / NP) consecutive atoms, which together hold 8 (or, for NP >= 8, NP) pair slots; slot
-// s = (atom's phase in the group) * NP + p for NP < 8, s = p % 8 otherwise, and a slot takes the
-// FMA pipe when s < SOFT.  The share is SOFT / 8 at every tile size.  From kSoftAlternate on
-// (SOFT = kSoftAlternate + k) two such groups alternate between k and k + 1 soft slots, a share of
-// (2k + 1) / 16.  soft_phases is the number of consecutive atoms one whole pattern spans.
+// ceil(z_iterations / 2) lane pairs per atom.  Within one stage of the atom stream (kTileAtoms atoms)
+// every lane pair keeps one form for all atoms, so the form's bias scales that point's partial sum
+// and cannot correlate with a pattern in the charges.  The stages take turns in a pattern of
+// soft_group(NP) = max(1, 8 / NP) phases, which together hold 8 (or, for NP >= 8, NP) pair slots;
+// slot s = (stage phase) * NP + p for NP < 8, s = p % 8 otherwise, and a slot takes the FMA pipe
+// when s < SOFT.  The share is SOFT / 8 at every tile size.  From kSoftAlternate on
+// (SOFT = kSoftAlternate + k) two such patterns alternate between k and k + 1 soft slots, a share
+// of (2k + 1) / 16.  soft_phases is the number of stage phases of one whole pattern.
 constexpr int kSoftAlternate = 10;
 constexpr int soft_group(int np) { return np >= 8 ? 1 : 8 / np; }
 constexpr int soft_phases(int soft, int np)
 {
     return soft == 0 ? 1 : (soft >= kSoftAlternate ? 2 : 1) * soft_group(np);
+}
+
+// Calls f(std::integral_constant<int, phase>) for a run-time phase in [0, P): the stage loop is
+// instantiated once per phase so that the soft/MUFU choice stays a compile-time one per pair.
+template <int P, int G = 0, class F>
+__device__ __forceinline__ void with_phase(const int phase, F&& f)
+{
+    if constexpr (G + 1 < P) {
+        if (phase == G)
+            f(std::integral_constant<int, G>{});
+        else
+            with_phase<P, G + 1>(phase, f);
+    } else {
+        f(std::integral_constant<int, G>{});
+    }
 }
 
 template <int SOFT, int NP, int PHASE>
@@ -353,6 +372,50 @@ __device__ __forceinline__ void pair_block_2d(const float (&gx)[XP], const float
     for (int k = 0; k < XP; ++k)
         dx[k] = gx[k] - a.x;
     pair_rows<false, XP, YH, SOFT, PHASE, HALF>(dx, dyc, splat(a.w), splat(a.w * kSoftRsqrtScale), acc);
+}
+
+// ------------------------------------------------------------------------------------------
+// FP64 pairs (COUL_PREC_FP64_PAIRS): the atom's FP32 coordinates and charge widened to double, every
+// difference exact in FP64, r^2 by FP64 fma, the reciprocal square root from the MUFU approximation
+// rsqrt.approx.ftz.f64 (relative error below 2^-20) refined by one Newton step in FP64
+// (y <- y + y (1 - r^2 y^2) / 2, relative error about 1.5 * 2^-40), accumulated in FP64.  Six FP64
+// operations and one MUFU instruction per pair; the FP64 pipe bounds it.
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ double rsqrt_mufu_f64(double x)
+{
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    return y;
+}
+
+template <int XP, int ZI>
+__device__ __forceinline__ void pair_block_3d_f64(const double (&gx)[XP], double gy, const double (&gz)[ZI], float4 a,
+                                                  double (&acc)[XP][ZI])
+{
+    const double dy = gy - static_cast<double>(a.y);
+    const double dy2 = dy * dy;
+    const double q = static_cast<double>(a.w);
+    double dxy[XP];
+#pragma unroll
+    for (int k = 0; k < XP; ++k) {
+        const double dx = gx[k] - static_cast<double>(a.x);
+        dxy[k] = fma(dx, dx, dy2);
+    }
+    double dz[ZI];
+#pragma unroll
+    for (int m = 0; m < ZI; ++m)
+        dz[m] = gz[m] - static_cast<double>(a.z);
+#pragma unroll
+    for (int k = 0; k < XP; ++k) {
+#pragma unroll
+        for (int m = 0; m < ZI; ++m) {
+            const double r2 = fma(dz[m], dz[m], dxy[k]);
+            double y = rsqrt_mufu_f64(r2);
+            const double e = fma(-r2, y * y, 1.0);
+            y = fma(y * e, 0.5, y);
+            acc[k][m] = fma(q, y, acc[k][m]);
+        }
+    }
 }
 
 // Knuth's two-sum: s + e == a + b exactly (round-to-nearest, no contraction of additions).

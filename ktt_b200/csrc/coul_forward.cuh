@@ -21,7 +21,7 @@
 namespace coul {
 
 enum : int { kSrcShared = 0, kSrcConstant = 1 };
-enum : int { kPrecFp32 = 0, kPrecCompensated = 1, kPrecFp64Merge = 2 };
+enum : int { kPrecFp32 = 0, kPrecCompensated = 1, kPrecFp64Merge = 2, kPrecFp64Pairs = 3 };
 
 // Per translation unit: the constant-memory atom chunk.  Only the TU that instantiates the
 // constant-memory variants uses it; it has internal linkage so no relocatable device code is needed.
@@ -46,17 +46,6 @@ __device__ __forceinline__ void eval_atom(const float (&gx)[XP], float gy, const
         pair_block_2d<XP, ZH, SOFT, PHASE, HALF>(gx, gb, a, dst);
 }
 
-// The atoms j0 .. j0 + P - 1 of one pattern of the FMA-pipe share (P = soft_phases), each with its
-// phase in the pattern.
-template <int MODE, int XP, int ZH, int SOFT, bool HALF, int PHASE, int P, class AtomAt>
-__device__ __forceinline__ void eval_group(const float (&gx)[XP], float gy, const float2 (&gb)[ZH], const AtomAt& at,
-                                           const int j0, float2 (&dst)[XP][ZH])
-{
-    if constexpr (PHASE < P) {
-        eval_atom<MODE, XP, ZH, SOFT, PHASE, HALF>(gx, gy, gb, at(j0 + PHASE), dst);
-        eval_group<MODE, XP, ZH, SOFT, HALF, PHASE + 1, P>(gx, gy, gb, at, j0, dst);
-    }
-}
 
 __device__ __forceinline__ float lane(const float2& v, int l) { return l == 0 ? v.x : v.y; }
 
@@ -125,7 +114,7 @@ __device__ __forceinline__ void ring_init(uint64_t* full, const int tid)
 template <int ZI, int XP, int UNR, int SRC, int SOA, int PREC, int SOFT, int MODE>
 __device__ __forceinline__ bool tile_accumulate(const FwdParams& p, const int x0, const int yrow, const int z0,
                                                 unsigned char* tiles, uint64_t* full, uint32_t& gstage,
-                                                float (&val)[XP][ZI])
+                                                float (&val)[XP][ZI], const uint32_t phase_base = 0)
 {
     static_assert(XP == 1 || XP == 2 || XP == 4 || XP == 8, "XP must be 1, 2, 4 or 8");
     static_assert(kTileAtoms % kSubTile == 0, "sub-tiles must divide the stage");
@@ -138,7 +127,7 @@ __device__ __forceinline__ bool tile_accumulate(const FwdParams& p, const int x0
     // the last pair holds one point (HALF), evaluated on its own.
     constexpr int ZH = (ZI + 1) / 2;
     constexpr bool HALF = (ZI & 1) != 0;
-    constexpr int P = soft_phases(SOFT, XP * ZH);  // atoms per whole pattern of the FMA-pipe share
+    constexpr int P = soft_phases(SOFT, XP * ZH);  // stage phases of the FMA-pipe share's pattern
     float2 gb[ZH];
     float gy;
     if constexpr (MODE == kModeGrid3d) {
@@ -159,6 +148,21 @@ __device__ __forceinline__ bool tile_accumulate(const FwdParams& p, const int x0
     float2 part[XP][ZH];
     float2 cmp[XP][ZH];
     double acc64[XP][2 * ZH];
+    // FP64 pairs: the point coordinates widened once (3D only)
+    static_assert(PREC != kPrecFp64Pairs || (MODE == kModeGrid3d && SOFT == 0 && SRC == kSrcShared),
+                  "FP64 pairs: 3D maps, MUFU estimate, shared-memory atoms");
+    double gxd[XP], gzd[ZI], accd[XP][ZI];
+    const double gyd = static_cast<double>(gy);
+#pragma unroll
+    for (int k = 0; k < XP; ++k)
+        gxd[k] = static_cast<double>(gx[k]);
+#pragma unroll
+    for (int m = 0; m < ZI; ++m) {
+        gzd[m] = static_cast<double>(lane(gb[m / 2], m & 1));
+#pragma unroll
+        for (int k = 0; k < XP; ++k)
+            accd[k][m] = 0.0;
+    }
 #pragma unroll
     for (int k = 0; k < XP; ++k)
 #pragma unroll
@@ -204,17 +208,15 @@ __device__ __forceinline__ bool tile_accumulate(const FwdParams& p, const int x0
         (void)full;
         (void)gstage;
         const int n = static_cast<int>(p.n_atoms);
-        if constexpr (P > 1) {
-            auto at = [](int j) { return c_atoms[j]; };
-            int j = 0;
-            for (; j + P <= n; j += P)
-                eval_group<MODE, XP, ZH, SOFT, HALF, 0, P>(gx, gy, gb, at, j, acc);
-            for (; j < n; ++j)  // the last, partial pattern
-                eval_atom<MODE, XP, ZH, SOFT, 0, HALF>(gx, gy, gb, c_atoms[j], acc);
-        } else {
+        // the chunk in blocks of kTileAtoms atoms, each block one phase of the FMA-pipe share
+        for (int j0 = 0; j0 < n; j0 += kTileAtoms) {
+            const int j1 = j0 + kTileAtoms < n ? j0 + kTileAtoms : n;
+            with_phase<P>((j0 / kTileAtoms) % P, [&](auto phase) {
+                constexpr int G = decltype(phase)::value;
 #pragma unroll UNR
-            for (int j = 0; j < n; ++j)
-                eval_atom<MODE, XP, ZH, SOFT, 0, HALF>(gx, gy, gb, c_atoms[j], acc);
+                for (int j = j0; j < j1; ++j)
+                    eval_atom<MODE, XP, ZH, SOFT, G, HALF>(gx, gy, gb, c_atoms[j], acc);
+            });
         }
     } else {
         const int nthreads = blockDim.x * blockDim.y;
@@ -306,21 +308,29 @@ __device__ __forceinline__ bool tile_accumulate(const FwdParams& p, const int x0
                     return make_float4(f[j], f[kTileAtoms + j], f[2 * kTileAtoms + j], f[3 * kTileAtoms + j]);
                 }
             };
-            // the stage is padded to kTileAtoms, a multiple of every pattern length P (at most 16)
-            static_assert(kSubTile % 16 == 0, "sub-tiles hold whole patterns of the FMA-pipe share");
-            constexpr int kGroupUnroll = UNR > P ? UNR / P : 1;
-            if constexpr (PREC == kPrecFp32) {
-#pragma unroll kGroupUnroll
-                for (int j = 0; j < kTileAtoms; j += P)
-                    eval_group<MODE, XP, ZH, SOFT, HALF, 0, P>(gx, gy, gb, atom_at, j, acc);
+            // the stage is padded to kTileAtoms atoms; the whole stage is one phase of the FMA-pipe
+            // share's pattern
+            if constexpr (PREC == kPrecFp64Pairs) {
+#pragma unroll UNR
+                for (int j = 0; j < kTileAtoms; ++j)
+                    pair_block_3d_f64<XP, ZI>(gxd, gyd, gzd, atom_at(j), accd);
             } else {
-                for (int j0 = 0; j0 < kTileAtoms; j0 += kSubTile) {
-                    clear_part();
-#pragma unroll kGroupUnroll
-                    for (int j = 0; j < kSubTile; j += P)
-                        eval_group<MODE, XP, ZH, SOFT, HALF, 0, P>(gx, gy, gb, atom_at, j0 + j, part);
-                    merge();
-                }
+                with_phase<P>(static_cast<int>((phase_base + static_cast<uint32_t>(s)) % P), [&](auto phase) {
+                    constexpr int G = decltype(phase)::value;
+                    if constexpr (PREC == kPrecFp32) {
+#pragma unroll UNR
+                        for (int j = 0; j < kTileAtoms; ++j)
+                            eval_atom<MODE, XP, ZH, SOFT, G, HALF>(gx, gy, gb, atom_at(j), acc);
+                    } else {
+                        for (int j0 = 0; j0 < kTileAtoms; j0 += kSubTile) {
+                            clear_part();
+#pragma unroll UNR
+                            for (int j = 0; j < kSubTile; ++j)
+                                eval_atom<MODE, XP, ZH, SOFT, G, HALF>(gx, gy, gb, atom_at(j0 + j), part);
+                            merge();
+                        }
+                    }
+                });
             }
             // Everyone is done with this buffer; order the generic-proxy accesses before the next
             // TMA write into it, then refill.
@@ -338,6 +348,8 @@ __device__ __forceinline__ bool tile_accumulate(const FwdParams& p, const int x0
         for (int m = 0; m < ZI; ++m) {
             if constexpr (PREC == kPrecFp32)
                 val[k][m] = lane(acc[k][m / 2], m & 1);
+            else if constexpr (PREC == kPrecFp64Pairs)
+                val[k][m] = static_cast<float>(accd[k][m]);
             else if constexpr (PREC == kPrecCompensated)
                 val[k][m] = lane(acc[k][m / 2], m & 1) + lane(cmp[k][m / 2], m & 1);
             else
@@ -346,6 +358,7 @@ __device__ __forceinline__ bool tile_accumulate(const FwdParams& p, const int x0
     (void)part;
     (void)cmp;
     (void)acc64;
+    (void)accd;
     return true;
 }
 
@@ -445,8 +458,10 @@ __global__ void __launch_bounds__(kMaxThreads) split_kernel(const FwdParams p, c
     ring_init(full, tid);
     uint32_t gstage = 0;
     float val[XP][ZI];
+    // each rank starts at its own phase of the FMA-pipe share, so that a cluster whose ranks stream
+    // one stage each still splits the rsqrts SOFT/8 between the pipes
     (void)tile_accumulate<ZI, XP, UNR, kSrcShared, 0, kPrecFp32, SOFT, MODE>(q, x0, yrow, z0, smem_raw, full, gstage,
-                                                                            val);
+                                                                            val, r);
     // A CTA whose ring wait expired has set the status word; the cluster still meets at both
     // barriers so no CTA waits on one that left.
 #pragma unroll
@@ -607,6 +622,8 @@ void register_fwd_3d_const(std::vector<VariantEntry>& v);
 void register_fwd_3d_precise(std::vector<VariantEntry>& v);
 void register_fwd_3d_soft(std::vector<VariantEntry>& v);
 void register_fwd_3d_soft_precise(std::vector<VariantEntry>& v);
+void register_fwd_3d_soft_fp64m(std::vector<VariantEntry>& v);
+void register_fwd_3d_fp64(std::vector<VariantEntry>& v);
 void register_fwd_2d(std::vector<VariantEntry>& v);
 void register_fwd_split(std::vector<VariantEntry>& v);
 

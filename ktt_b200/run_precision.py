@@ -1,14 +1,16 @@
-"""Precision stress: the three accumulation forms on a cancellation-heavy map.
+"""Precision stress: the precision forms on a cancellation-heavy map (or the uniform map).
 
-    python -m ktt_b200.run_precision [--subset 0.01] [--repeat 3] [--n 256] [--per-cluster 1024]
+    python -m ktt_b200.run_precision [--map clustered|uniform] [--subset 0.01] [--repeat 3]
 
-65,536 atoms in 64 Gaussian clusters (sigma 2 A, centres uniform in the 128 A cube), charges +1/-1
-alternating within each cluster plus N(0, 0.01), total charge exactly zero; 256^3 grid at 0.5 A.
-Each form (FP32 accumulation, compensated two-sum, FP64 merge; MUFU-only and with 2/8 of the rsqrts
-on the FMA pipe) is timed on the device (best of --repeat) and compared with the FP64 oracle on a
-seeded subset of grid points.  Prints one JSON line per form: device time, pair rate, max abs error,
-max error / max |V| (rel_norm), rms error / rms V (rel_rms), and max error / sum_j |q_j| / r_ij
-(rel_cond, the error in units of the sum's condition).
+clustered: 65,536 atoms in 64 Gaussian clusters (sigma 2 A, centres uniform in the 128 A cube),
+charges +1/-1 alternating within each cluster plus N(0, 0.01), total charge exactly zero; uniform:
+the benchmark's map (65,536 atoms uniform in the 128 A cube, q ~ U[-1, 1]); 256^3 grid at 0.5 A.
+Each form (FP32 accumulation, compensated two-sum, FP64 merge -- MUFU-only and with part of the
+rsqrts on the FMA pipe -- and FP64 pairs) is timed on the device (best of --repeat) and compared with
+the FP64 oracle on a seeded subset of grid points.  Prints one JSON line per form: device time, pair
+rate, max abs error, max error / max |V| (rel_norm), rms error / rms V (rel_rms), the pointwise
+error max |dV| / max(|V|, floor) at the two stated floors 0.1 rms(V) and 1e-3 rms(V), and max error /
+sum_j |q_j| / r_ij (rel_cond, the error in units of the sum's condition).
 """
 from __future__ import annotations
 
@@ -24,11 +26,13 @@ FORMS = (
     ("compensated_soft2", dict(precision=1, rsqrt_soft=2)),
     ("fp64_merge", dict(precision=2, rsqrt_soft=0)),
     ("fp64_merge_soft2", dict(precision=2, rsqrt_soft=2)),
+    ("fp64_pairs", dict(precision=3, rsqrt_soft=0)),
 )
 
 
 def main() -> None:
     ap = argparse.ArgumentParser()
+    ap.add_argument("--map", choices=["clustered", "uniform"], default="clustered")
     ap.add_argument("--subset", type=float, default=0.01)
     ap.add_argument("--repeat", type=int, default=3)
     ap.add_argument("--n", type=int, default=256)
@@ -43,7 +47,10 @@ def main() -> None:
     import oracle
     from ktt_b200 import errors, workloads
 
-    case = workloads.clustered_map(n=args.n, per_cluster=args.per_cluster, box=args.n * 0.5)
+    if args.map == "clustered":
+        case = workloads.clustered_map(n=args.n, per_cluster=args.per_cluster, box=args.n * 0.5)
+    else:
+        case = workloads.uniform_map(n=args.n, box=args.n * 0.5)
     dims, h = case.dims, case.spacing
     total = dims[0] * dims[1] * dims[2]
     idx = workloads.subset_indices(total, args.subset)
@@ -55,7 +62,8 @@ def main() -> None:
     base = {"dims": list(dims), "atoms": int(case.atoms.shape[0]), "subset_points": int(idx.size),
             "ref_max_abs": float(np.max(np.abs(ref))), "ref_rms": float(np.sqrt(np.mean(ref * ref))),
             "sumabs_median": float(np.median(sumabs))}
-    print(json.dumps({"workload": "clustered 64 x 1024, net charge 0", **base}), flush=True)
+    label = "clustered 64 x 1024, net charge 0" if args.map == "clustered" else "uniform, q ~ U[-1, 1]"
+    print(json.dumps({"workload": label, **base}), flush=True)
     for name, fields in FORMS:
         tune = ktt_b200.Tune(block_x=32, block_y=4, z_iterations=args.z_iterations, x_points=args.x_points,
                              **fields)
@@ -68,6 +76,8 @@ def main() -> None:
         rep = errors.report(got, ref, sumabs)
         d = got - ref
         rep["rel_rms"] = float(np.sqrt(np.mean(d * d)) / np.sqrt(np.mean(ref * ref)))
+        rep["rel_point_floor_0.1rms"] = errors.report(got, ref, floor=0.1 * base["ref_rms"])["rel_point"]
+        rep["rel_point_floor_1e-3rms"] = errors.report(got, ref, floor=1e-3 * base["ref_rms"])["rel_point"]
         print(json.dumps({"form": name, "tune": tune.as_dict(), "ms": min(ms),
                           "gpairs_per_s": pairs / (min(ms) * 1e-3) / 1e9, **rep}), flush=True)
     ctx.close()

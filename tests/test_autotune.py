@@ -21,7 +21,8 @@ import ktt_b200
 from ktt_b200 import autotune
 
 
-def _kept(space, supported):
+def _kept(space, supported, precisions=(0,)):
+    space = dict(space, PRECISION=list(precisions))
     names = list(space)
     kept = 0
     for values in itertools.product(*space.values()):
@@ -34,6 +35,10 @@ def _kept(space, supported):
 def test_map3d_space_is_the_compiled_variants():
     n = autotune.tune_map3d(grid=64, atoms=64, dry_run=True)["configurations"]
     assert n == _kept(autotune.MAP3D_SPACE, ktt_b200.tune_supported)
+    assert n >= 100
+    # the precise forms' space (compensated and FP64 merge)
+    n = autotune.tune_map3d(grid=64, atoms=64, dry_run=True, precisions=(1, 2))["configurations"]
+    assert n == _kept(autotune.MAP3D_SPACE, ktt_b200.tune_supported, (1, 2))
     assert n >= 100
 
 
@@ -129,9 +134,11 @@ def test_fp64_reference_kernel_matches_the_oracle():
 def test_full_map3d_search_validated_against_the_oracle():
     """The search behind ktt_b200/tuned/b200_map3d.json: 256^3 x 65,536 atoms, MCMC, every configuration
     validated against the FP64 oracle's full map (about 100 s on 16 host cores, once)."""
+    precisions = tuple(int(p) for p in os.environ.get("KTT_AUTOTUNE_PRECISIONS", "1,2").split(","))
     result = autotune.tune_map3d(grid=256, atoms=65536, searcher="mcmc",
                                  budget=int(os.environ.get("KTT_AUTOTUNE_BUDGET", "150")), reference=_Spy(),
-                                 reference_name="FP64 oracle (oracle/coulomb_oracle.c), full map")
+                                 reference_name="FP64 oracle (oracle/coulomb_oracle.c), full map",
+                                 precisions=precisions)
     with open(os.environ["KTT_AUTOTUNE_OUT"], "w") as f:
         json.dump(result, f, indent=1)
         f.write("\n")
