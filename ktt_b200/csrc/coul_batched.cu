@@ -168,30 +168,10 @@ COUL_API int coul_batch_create(coul_ctx* ctx, const coul_molecule* molecules, in
 
     std::vector<MolDesc> descs;
     int64_t next = 0;
-    const int64_t span_x = static_cast<int64_t>(tune->block_x) * tune->x_points;
     for (const int i : b->order) {
-        const coul_molecule& m = molecules[i];
         MolDesc d{};
-        d.atoms = reinterpret_cast<const float4*>(m.d_atoms);
-        d.n_atoms = m.n_atoms;
-        d.out = m.d_out;
-        d.nx = m.grid.nx;
-        d.ny = m.grid.ny;
-        d.nz = m.grid.nz;
-        d.h = m.grid.spacing;
-        d.ox = m.grid.origin[0];
-        d.oy = m.grid.origin[1];
-        d.oz = m.grid.origin[2];
-        d.tiles_x = static_cast<int>((m.grid.nx + span_x - 1) / span_x);
-        d.tiles_y = (m.grid.ny + tune->block_y - 1) / tune->block_y;
-        const int tiles_z = (m.grid.nz + tune->z_iterations - 1) / tune->z_iterations;
-        const int xp = tune->x_points;
-        d.vec_ok = (xp > 1 && m.grid.nx % xp == 0 &&
-                    (reinterpret_cast<uintptr_t>(m.d_out) % (sizeof(float) * (xp >= 4 ? 4 : xp))) == 0)
-                       ? 1
-                       : 0;
         d.tile_begin = next;
-        next += static_cast<int64_t>(d.tiles_x) * d.tiles_y * tiles_z;
+        next += fill_mol_desc(d, molecules[i], b->tune);
         b->total_pairs += pairs(i);
         descs.push_back(d);
     }

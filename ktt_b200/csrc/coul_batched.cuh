@@ -2,6 +2,7 @@
 #pragma once
 
 #include "coul_forward.cuh"
+#include "coul_internal.h"
 
 namespace coul {
 
@@ -12,9 +13,54 @@ struct MolDesc {
     int64_t tile_begin;  // first work item of this molecule
     int nx, ny, nz;
     int tiles_x, tiles_y;
+    int tx;              // threads of a CTA along x for this molecule's tiles (the rest along y)
     int vec_ok;
     float h, ox, oy, oz;
 };
+
+// Tile geometry of one molecule: its CTA threads are arranged as tx x (threads / tx), tx the power
+// of two dividing the thread count whose tile pads the grid's x-y plane least (ties: the block's
+// own x size).  The arrangement only moves points between threads; every point is computed the
+// same way.  Returns the molecule's work items.
+inline int64_t fill_mol_desc(MolDesc& d, const coul_molecule& m, const coul_tune& t)
+{
+    const int threads = t.block_x * t.block_y;
+    int best_tx = t.block_x;
+    int64_t best_area = -1;
+    for (int tx = 1; tx <= threads; tx *= 2) {
+        if (threads % tx)
+            continue;
+        const int64_t sx = static_cast<int64_t>(tx) * t.x_points;
+        const int64_t sy = threads / tx;
+        const int64_t area = (m.grid.nx + sx - 1) / sx * sx * ((m.grid.ny + sy - 1) / sy * sy);
+        if (best_area < 0 || area < best_area || (area == best_area && tx == t.block_x)) {
+            best_area = area;
+            best_tx = tx;
+        }
+    }
+    d.atoms = reinterpret_cast<const float4*>(m.d_atoms);
+    d.n_atoms = m.n_atoms;
+    d.out = m.d_out;
+    d.nx = m.grid.nx;
+    d.ny = m.grid.ny;
+    d.nz = m.grid.nz;
+    d.h = m.grid.spacing;
+    d.ox = m.grid.origin[0];
+    d.oy = m.grid.origin[1];
+    d.oz = m.grid.origin[2];
+    d.tx = best_tx;
+    const int64_t span_x = static_cast<int64_t>(best_tx) * t.x_points;
+    const int ty = threads / best_tx;
+    d.tiles_x = static_cast<int>((m.grid.nx + span_x - 1) / span_x);
+    d.tiles_y = (m.grid.ny + ty - 1) / ty;
+    const int tiles_z = (m.grid.nz + t.z_iterations - 1) / t.z_iterations;
+    const int xp = t.x_points;
+    d.vec_ok = (xp > 1 && m.grid.nx % xp == 0 &&
+                (reinterpret_cast<uintptr_t>(m.d_out) % (sizeof(float) * (xp >= 4 ? 4 : xp))) == 0)
+                   ? 1
+                   : 0;
+    return static_cast<int64_t>(d.tiles_x) * d.tiles_y * tiles_z;
+}
 
 struct BatchParams {
     const MolDesc* mols;
@@ -75,11 +121,13 @@ __global__ void __launch_bounds__(kMaxThreads) batched_kernel(const BatchParams 
         p.out = m.out;
         p.accumulate = b.accumulate;
         p.status = b.status;
-        const int x0 = (tile_x * blockDim.x + threadIdx.x) * XP;
-        const int yrow = tile_y * blockDim.y + threadIdx.y;
+        const int ty = static_cast<int>(blockDim.x * blockDim.y) / m.tx;
+        const int x0 = (tile_x * m.tx + tid % m.tx) * XP;
+        const int yrow = tile_y * ty + tid / m.tx;
         const int z0 = tile_z * ZI;
-        if (!tile_pass<ZI, XP, UNR, kSrcShared, 0, PREC, SOFT, kModeGrid3d>(p, x0, yrow, z0, m.vec_ok, smem_raw, full,
-                                                                              gstage))
+        // tiles that overhang the molecule's grid in z evaluate only their points inside it
+        if (!tile_pass<ZI, XP, UNR, kSrcShared, 0, PREC, SOFT, kModeGrid3d, true>(p, x0, yrow, z0, m.vec_ok,
+                                                                                    smem_raw, full, gstage))
             return;
     }
 }

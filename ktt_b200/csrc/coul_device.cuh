@@ -309,14 +309,17 @@ __device__ __forceinline__ void pair_update(float2 r2, float2 q2, float2 qs2, fl
 // half pair resolved at compile time.  r2 per pair from the per-k term pk and the per-i term pi:
 //   SQUARE_I (3D):  r2 = pi^2 + pk   (pi = dz of the two points, pk = dx^2 + dy^2)
 //   else (2D):      r2 = pk^2 + pi   (pk = dx, pi = dy^2 + dz^2 of the two rows)
-template <bool SQUARE_I, int XP, int ZH, int SOFT, int PHASE, bool HALF, int K = 0, int I = 0>
+// Only the first ZA <= ZH lane pairs are evaluated (the rest of a tile that overhangs the grid);
+// HALF marks pair ZA - 1 as holding one point.
+template <bool SQUARE_I, int XP, int ZH, int ZA, int SOFT, int PHASE, bool HALF, int K = 0, int I = 0>
 __device__ __forceinline__ void pair_rows(const float (&pk)[XP], const float2 (&pi)[ZH], float2 q2, float2 qs2,
                                           float2 (&acc)[XP][ZH])
 {
+    static_assert(ZA >= 1 && ZA <= ZH, "active pairs within the tile");
     if constexpr (K < XP) {
-        if constexpr (I < ZH) {
+        if constexpr (I < ZA) {
             constexpr bool soft = SOFT != 0 && pair_is_soft<SOFT, XP * ZH, PHASE>(K * ZH + I);
-            constexpr bool half = HALF && I == ZH - 1;
+            constexpr bool half = HALF && I == ZA - 1;
             if constexpr (half) {
                 const float r2 = SQUARE_I ? fmaf(pi[I].x, pi[I].x, pk[K]) : fmaf(pk[K], pk[K], pi[I].x);
                 pair_update<soft, true>(make_float2(r2, 0.0f), q2, qs2, acc[K][I]);
@@ -325,15 +328,15 @@ __device__ __forceinline__ void pair_rows(const float (&pk)[XP], const float2 (&
                                            : __ffma2_rn(splat(pk[K]), splat(pk[K]), pi[I]);
                 pair_update<soft, false>(r2, q2, qs2, acc[K][I]);
             }
-            pair_rows<SQUARE_I, XP, ZH, SOFT, PHASE, HALF, K, I + 1>(pk, pi, q2, qs2, acc);
+            pair_rows<SQUARE_I, XP, ZH, ZA, SOFT, PHASE, HALF, K, I + 1>(pk, pi, q2, qs2, acc);
         } else {
-            pair_rows<SQUARE_I, XP, ZH, SOFT, PHASE, HALF, K + 1, 0>(pk, pi, q2, qs2, acc);
+            pair_rows<SQUARE_I, XP, ZH, ZA, SOFT, PHASE, HALF, K + 1, 0>(pk, pi, q2, qs2, acc);
         }
     }
 }
 
 // 3D: thread owns points (gx[k], gy, gz[i].x / gz[i].y); acc[k][i] += q / |r - a| lane-wise.
-template <int XP, int ZH, int SOFT, int PHASE, bool HALF>
+template <int XP, int ZH, int ZA, int SOFT, int PHASE, bool HALF>
 __device__ __forceinline__ void pair_block_3d(const float (&gx)[XP], float gy, const float2 (&gz)[ZH], float4 a,
                                               float2 (&acc)[XP][ZH])
 {
@@ -348,14 +351,14 @@ __device__ __forceinline__ void pair_block_3d(const float (&gx)[XP], float gy, c
     float2 dz[ZH];
     const float2 naz = splat(-a.z);
 #pragma unroll
-    for (int i = 0; i < ZH; ++i)
+    for (int i = 0; i < ZA; ++i)
         dz[i] = __fadd2_rn(gz[i], naz);
-    pair_rows<true, XP, ZH, SOFT, PHASE, HALF>(dxy, dz, splat(a.w), splat(a.w * kSoftRsqrtScale), acc);
+    pair_rows<true, XP, ZH, ZA, SOFT, PHASE, HALF>(dxy, dz, splat(a.w), splat(a.w * kSoftRsqrtScale), acc);
 }
 
 // 2D slice (KTT's 2D convention): thread owns points (gx[k], gy[i].x / gy[i].y) of one slice, the
 // atom's .z holds the squared z distance c; acc[k][i] += q / sqrt(dx^2 + dy^2 + c) lane-wise.
-template <int XP, int YH, int SOFT, int PHASE, bool HALF>
+template <int XP, int YH, int ZA, int SOFT, int PHASE, bool HALF>
 __device__ __forceinline__ void pair_block_2d(const float (&gx)[XP], const float2 (&gy)[YH], float4 a,
                                               float2 (&acc)[XP][YH])
 {
@@ -363,7 +366,7 @@ __device__ __forceinline__ void pair_block_2d(const float (&gx)[XP], const float
     const float2 nay = splat(-a.y);
     const float2 c2 = splat(a.z);
 #pragma unroll
-    for (int i = 0; i < YH; ++i) {
+    for (int i = 0; i < ZA; ++i) {
         const float2 dy = __fadd2_rn(gy[i], nay);
         dyc[i] = __ffma2_rn(dy, dy, c2);
     }
@@ -371,7 +374,7 @@ __device__ __forceinline__ void pair_block_2d(const float (&gx)[XP], const float
 #pragma unroll
     for (int k = 0; k < XP; ++k)
         dx[k] = gx[k] - a.x;
-    pair_rows<false, XP, YH, SOFT, PHASE, HALF>(dx, dyc, splat(a.w), splat(a.w * kSoftRsqrtScale), acc);
+    pair_rows<false, XP, YH, ZA, SOFT, PHASE, HALF>(dx, dyc, splat(a.w), splat(a.w * kSoftRsqrtScale), acc);
 }
 
 // ------------------------------------------------------------------------------------------

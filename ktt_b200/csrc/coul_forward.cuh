@@ -36,14 +36,14 @@ struct FwdLaunch {
     int split;      // atom-split form: CTAs per cluster sharing one point tile (0 / 1 = one CTA per tile)
 };
 
-template <int MODE, int XP, int ZH, int SOFT, int PHASE, bool HALF>
+template <int MODE, int XP, int ZH, int SOFT, int PHASE, bool HALF, int ZA = ZH>
 __device__ __forceinline__ void eval_atom(const float (&gx)[XP], float gy, const float2 (&gb)[ZH], float4 a,
                                           float2 (&dst)[XP][ZH])
 {
     if constexpr (MODE == kModeGrid3d)
-        pair_block_3d<XP, ZH, SOFT, PHASE, HALF>(gx, gy, gb, a, dst);
+        pair_block_3d<XP, ZH, ZA, SOFT, PHASE, HALF>(gx, gy, gb, a, dst);
     else
-        pair_block_2d<XP, ZH, SOFT, PHASE, HALF>(gx, gb, a, dst);
+        pair_block_2d<XP, ZH, ZA, SOFT, PHASE, HALF>(gx, gb, a, dst);
 }
 
 
@@ -111,11 +111,16 @@ __device__ __forceinline__ void ring_init(uint64_t* full, const int tid)
 // ring's stages across calls, so a persistent kernel can run many tiles through one ring.  Every
 // thread of the CTA must call this together (it synchronises per stage).  Returns false (on every
 // thread) when a bounded wait on the ring expired; the status word is then set and val is invalid.
-template <int ZI, int XP, int UNR, int SRC, int SOA, int PREC, int SOFT, int MODE>
+// ZTRIM (3D only): a tile that overhangs the grid in z evaluates only its points inside the grid;
+// the number of z points in the grid (block-uniform) selects one of ZI instantiations of the stage
+// loop.  Used where many small grids make such tiles common (the batched kernel).
+template <int ZI, int XP, int UNR, int SRC, int SOA, int PREC, int SOFT, int MODE, bool ZTRIM = false>
 __device__ __forceinline__ bool tile_accumulate(const FwdParams& p, const int x0, const int yrow, const int z0,
                                                 unsigned char* tiles, uint64_t* full, uint32_t& gstage,
                                                 float (&val)[XP][ZI], const uint32_t phase_base = 0)
 {
+    static_assert(!ZTRIM || (MODE == kModeGrid3d && SRC == kSrcShared && PREC != kPrecFp64Pairs),
+                  "z trimming: 3D maps, shared-memory atoms, FP32 pairs");
     static_assert(XP == 1 || XP == 2 || XP == 4 || XP == 8, "XP must be 1, 2, 4 or 8");
     static_assert(kTileAtoms % kSubTile == 0, "sub-tiles must divide the stage");
 
@@ -315,20 +320,34 @@ __device__ __forceinline__ bool tile_accumulate(const FwdParams& p, const int x0
                 for (int j = 0; j < kTileAtoms; ++j)
                     pair_block_3d_f64<XP, ZI>(gxd, gyd, gzd, atom_at(j), accd);
             } else {
-                with_phase<P>(static_cast<int>((phase_base + static_cast<uint32_t>(s)) % P), [&](auto phase) {
+                // G: the stage's phase of the FMA-pipe share; LA: the z points the tile evaluates
+                auto stage = [&](auto phase, auto lanes) {
                     constexpr int G = decltype(phase)::value;
+                    constexpr int LA = decltype(lanes)::value;
+                    constexpr int ZA = (LA + 1) / 2;
+                    constexpr bool HA = (LA & 1) != 0;
                     if constexpr (PREC == kPrecFp32) {
 #pragma unroll UNR
                         for (int j = 0; j < kTileAtoms; ++j)
-                            eval_atom<MODE, XP, ZH, SOFT, G, HALF>(gx, gy, gb, atom_at(j), acc);
+                            eval_atom<MODE, XP, ZH, SOFT, G, HA, ZA>(gx, gy, gb, atom_at(j), acc);
                     } else {
                         for (int j0 = 0; j0 < kTileAtoms; j0 += kSubTile) {
                             clear_part();
 #pragma unroll UNR
                             for (int j = 0; j < kSubTile; ++j)
-                                eval_atom<MODE, XP, ZH, SOFT, G, HALF>(gx, gy, gb, atom_at(j0 + j), part);
+                                eval_atom<MODE, XP, ZH, SOFT, G, HA, ZA>(gx, gy, gb, atom_at(j0 + j), part);
                             merge();
                         }
+                    }
+                };
+                with_phase<P>(static_cast<int>((phase_base + static_cast<uint32_t>(s)) % P), [&](auto phase) {
+                    if constexpr (ZTRIM) {
+                        const int lanes = p.nz - z0 < ZI ? p.nz - z0 : ZI;  // >= 1: the tile starts inside
+                        with_phase<ZI>(lanes - 1, [&](auto l) {
+                            stage(phase, std::integral_constant<int, decltype(l)::value + 1>{});
+                        });
+                    } else {
+                        stage(phase, std::integral_constant<int, ZI>{});
                     }
                 });
             }
@@ -387,12 +406,12 @@ __device__ __forceinline__ void store_tile(const FwdParams& p, const int x0, con
 }
 
 // tile_accumulate then store_tile.  Returns false when a bounded wait expired (nothing stored).
-template <int ZI, int XP, int UNR, int SRC, int SOA, int PREC, int SOFT, int MODE>
+template <int ZI, int XP, int UNR, int SRC, int SOA, int PREC, int SOFT, int MODE, bool ZTRIM = false>
 __device__ __forceinline__ bool tile_pass(const FwdParams& p, const int x0, const int yrow, const int z0, const int vec_ok,
                                           unsigned char* tiles, uint64_t* full, uint32_t& gstage)
 {
     float val[XP][ZI];
-    if (!tile_accumulate<ZI, XP, UNR, SRC, SOA, PREC, SOFT, MODE>(p, x0, yrow, z0, tiles, full, gstage, val))
+    if (!tile_accumulate<ZI, XP, UNR, SRC, SOA, PREC, SOFT, MODE, ZTRIM>(p, x0, yrow, z0, tiles, full, gstage, val))
         return false;
     store_tile<ZI, XP, MODE>(p, x0, yrow, z0, vec_ok, val);
     return true;

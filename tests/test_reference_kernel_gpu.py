@@ -138,6 +138,72 @@ def test_time_ktt_space_on_the_full_map(ctx):
     assert best["ms"] > 0
 
 
+@pytest.mark.skipif(not os.environ.get("KTT_REF_BATCH_OUT"), reason="timing comparison is opt-in")
+def test_time_batch_against_ktt_kernels(ctx):
+    """The 512-molecule uneven batch (seed 4, 8 A margin per side): this library's batched persistent
+    kernel replayed from its CUDA graph, against one synchronous launch per molecule (what a loop of
+    Tuner::Run calls does) of KTT's own directCoulombSum at its best B200 configuration and of
+    directCoulombSumReference.  KTT's kernels evaluate cubic grids from a zero origin only
+    (CoulombSum3d.cu:3-15), so each molecule runs on the cube of its largest side (a multiple of 16 for
+    the reference kernel's launch) with its atoms shifted by the origin; rates count the pairs of the
+    molecule's own grid (useful pairs) and, for KTT's kernels, also the cube's (evaluated pairs).
+    Device time of each whole mode from one event pair, best of two; results to KTT_REF_BATCH_OUT."""
+    import torch
+    mols = workloads.molecule_batch(seed=4, n_mol=512)
+    useful = float(sum(m.pairs for m in mols))
+    tune = ktt_b200.tuned("b200_batch", "batched")
+    inputs = [(torch.from_numpy(m.atoms).cuda(), m.dims, m.spacing, m.origin) for m in mols]
+    batch = ktt_b200.Batch(ctx, inputs, tune)
+    batch.run(ktt_b200.BATCH_GRAPH)
+    ctx.synchronize()
+    graph = []
+    for _ in range(2):
+        batch.run(ktt_b200.BATCH_GRAPH)
+        graph.append(ctx.elapsed_ms())
+    batch.close()
+
+    with open(os.path.join(ref_kernels.REPO, "profiles", "ktt_kernel_space_b200.json")) as f:
+        best = json.load(f)["best"]
+    cfg = {k: best[k] for k in ("WORK_GROUP_SIZE_X", "WORK_GROUP_SIZE_Y", "Z_ITERATIONS", "INNER_UNROLL_FACTOR",
+                                "USE_SOA")}
+    shifted = []
+    for m in mols:
+        a = m.atoms.copy()
+        a[:, :3] -= np.asarray(m.origin, dtype=np.float32)
+        g = max(m.dims)
+        shifted.append((torch.from_numpy(a).cuda(), _cols(a), a.shape[0], m.spacing, g, (g + 15) // 16 * 16))
+    largest = max(s[5] for s in shifted)
+    out = torch.zeros(largest ** 3, device="cuda")
+
+    def loop(reference):
+        stream = torch.cuda.current_stream()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for atoms, cols, n, h, g, g16 in shifted:
+            if reference:
+                ref_kernels.run_reference(atoms, n, h, g16, out)
+            else:
+                ref_kernels.run_tuned(cfg, atoms, cols, n, h, g, out)
+            torch.cuda.synchronize()
+        b.record(stream)
+        b.synchronize()
+        return a.elapsed_time(b)
+
+    result = {"molecules": len(mols), "useful_pairs": useful, "batched_tune": tune.as_dict(),
+              "graph_ms": min(graph), "graph_gpairs_per_s": useful / (min(graph) * 1e-3) / 1e9, "ktt_config": cfg}
+    for name, reference, cubes in (("ktt_best", False, [s[4] for s in shifted]),
+                                   ("ktt_reference", True, [s[5] for s in shifted])):
+        loop(reference)  # warm-up: module loads
+        ms = min(loop(reference) for _ in range(2))
+        evaluated = float(sum(g ** 3 * s[2] for g, s in zip(cubes, shifted)))
+        result[name] = {"ms": ms, "useful_gpairs_per_s": useful / (ms * 1e-3) / 1e9,
+                        "evaluated_gpairs_per_s": evaluated / (ms * 1e-3) / 1e9,
+                        "graph_speedup": ms / min(graph)}
+    with open(os.environ["KTT_REF_BATCH_OUT"], "w") as f:
+        json.dump(result, f, indent=1)
+    assert result["ktt_best"]["graph_speedup"] > 0
+
+
 # ---- KTT's N-body example ----
 
 def _nbody_inputs(n, seed=11):
