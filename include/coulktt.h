@@ -106,9 +106,10 @@ typedef struct coul_tune {
                          iterations) instead of the MUFU unit, in eighths (0 = all MUFU).  A thread
                          evaluates x_points * z_iterations points per atom in n lane pairs; within one
                          stage of 256 atoms each pair keeps one form for every atom.  With n >= 8, pair
-                         p is on the FMA pipe when (p % 8) < rsqrt_soft; with n < 8 the stages take
-                         turns in 8 / n phases and pair p of a stage in phase g is on the FMA pipe
-                         when g * n + p < rsqrt_soft.  Either way the share is rsqrt_soft / 8.
+                         p is on the FMA pipe when (p % 8) < rsqrt_soft; with n < 8 the stages (in
+                         the atom-split form also the warps of a block) take turns in 8 / n phases
+                         and pair p in phase g is on the FMA pipe when g * n + p < rsqrt_soft.  Either
+                         way the share is rsqrt_soft / 8.
                          10 + k (k = 0..7): successive patterns alternate between k and k + 1 eighths,
                          a share of (2k + 1) / 16 */
     int atom_split;   /* 0 or 1: one CTA per point tile; 2..16: a thread-block cluster of that many

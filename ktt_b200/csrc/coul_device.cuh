@@ -244,8 +244,9 @@ __device__ __forceinline__ float2 rsqrt_fma_x2(float2 x)
 // Static split between the MUFU unit and the FMA pipe.  A thread evaluates NP = x_points *
 // ceil(z_iterations / 2) lane pairs per atom.  Within one stage of the atom stream (kTileAtoms atoms)
 // every lane pair keeps one form for all atoms, so the form's bias scales that point's partial sum
-// and cannot correlate with a pattern in the charges.  The stages take turns in a pattern of
-// soft_group(NP) = max(1, 8 / NP) phases, which together hold 8 (or, for NP >= 8, NP) pair slots;
+// and cannot correlate with a pattern in the charges.  Stages (in the atom-split form also the
+// warps of a CTA) take turns in a pattern of soft_group(NP) = max(1, 8 / NP) phases, which together
+// hold 8 (or, for NP >= 8, NP) pair slots;
 // slot s = (stage phase) * NP + p for NP < 8, s = p % 8 otherwise, and a slot takes the FMA pipe
 // when s < SOFT.  The share is SOFT / 8 at every tile size.  From kSoftAlternate on
 // (SOFT = kSoftAlternate + k) two such patterns alternate between k and k + 1 soft slots, a share

@@ -23,6 +23,11 @@ namespace coul {
 enum : int { kSrcShared = 0, kSrcConstant = 1 };
 enum : int { kPrecFp32 = 0, kPrecCompensated = 1, kPrecFp64Merge = 2, kPrecFp64Pairs = 3 };
 
+// Cluster sizes of the atom-split form: 2..8 are portable; 9..16 use the B200's non-portable
+// cluster sizes (opted into per kernel; refused with a device-limits error where the block does not fit).
+constexpr int kMaxPortableSplit = 8;
+constexpr int kMaxSplit = 16;
+
 // Per translation unit: the constant-memory atom chunk.  Only the TU that instantiates the
 // constant-memory variants uses it; it has internal linkage so no relocatable device code is needed.
 static __constant__ float4 c_atoms[kConstAtoms];
@@ -477,10 +482,12 @@ __global__ void __launch_bounds__(kMaxThreads) split_kernel(const FwdParams p, c
     ring_init(full, tid);
     uint32_t gstage = 0;
     float val[XP][ZI];
-    // each rank starts at its own phase of the FMA-pipe share, so that a cluster whose ranks stream
-    // one stage each still splits the rsqrts SOFT/8 between the pipes
+    // the phase of the FMA-pipe share advances with the rank and with the warp, so every CTA of at
+    // least soft_phases warps splits its rsqrts SOFT/8 between the pipes even when it streams a
+    // single stage (the cluster waits for its slowest CTA; the atom loop between two stage barriers
+    // is warp-uniform code)
     (void)tile_accumulate<ZI, XP, UNR, kSrcShared, 0, kPrecFp32, SOFT, MODE>(q, x0, yrow, z0, smem_raw, full, gstage,
-                                                                            val, r);
+                                                                            val, r + static_cast<uint32_t>(tid) / 32u);
     // A CTA whose ring wait expired has set the status word; the cluster still meets at both
     // barriers so no CTA waits on one that left.
 #pragma unroll
@@ -489,18 +496,44 @@ __global__ void __launch_bounds__(kMaxThreads) split_kernel(const FwdParams p, c
         for (int m = 0; m < ZI; ++m)
             red[(k * ZI + m) * nthreads + tid] = val[k][m];
     cluster_sync();
-    if (r == 0) {
-        for (uint32_t peer = 1; peer < S; ++peer) {
-            const uint32_t base = cluster_map(red, peer);
+    // Reduce-scatter over the cluster: rank r sums the r-th of S slices of the tile's partial blocks,
+    // every rank's value of a point added in rank order (deterministic), and stores those points.
+    const int values = nthreads * XP * ZI;
+    const int per = (values + static_cast<int>(S) - 1) / static_cast<int>(S);
+    const int end = (static_cast<int>(r) + 1) * per < values ? (static_cast<int>(r) + 1) * per : values;
+    for (int i = static_cast<int>(r) * per + tid; i < end; i += nthreads) {
+        float part[kMaxSplit];
 #pragma unroll
-            for (int k = 0; k < XP; ++k)
+        for (int rank = 0; rank < kMaxSplit; ++rank)  // independent loads, issued together
+            if (rank < static_cast<int>(S))
+                part[rank] = ld_cluster_f32(cluster_map(red + i, static_cast<uint32_t>(rank)));
+        float sum = part[0];
 #pragma unroll
-                for (int m = 0; m < ZI; ++m)
-                    val[k][m] += ld_cluster_f32(base + 4u * static_cast<uint32_t>((k * ZI + m) * nthreads + tid));
+        for (int rank = 1; rank < kMaxSplit; ++rank)
+            if (rank < static_cast<int>(S))
+                sum += part[rank];
+        // the point of value i = (k * ZI + m) * nthreads + t: thread t's k-th x point, m-th blocked point
+        const int t = i % nthreads;
+        const int km = i / nthreads;
+        const int k = km / ZI;
+        const int m = km % ZI;
+        const int x = (tile_x * static_cast<int>(blockDim.x) + t % static_cast<int>(blockDim.x)) * XP + k;
+        const int ty = static_cast<int>(blockIdx.y * blockDim.y) + t / static_cast<int>(blockDim.x);
+        float* dst = nullptr;
+        if constexpr (MODE == kModeGrid3d) {
+            const int z = z0 + m;
+            if (x < p.nx && ty < p.ny && z < p.nz)
+                dst = p.out + (static_cast<int64_t>(z - p.z_base) * p.ny + ty) * p.nx + x;
+        } else {
+            const int yy = ty * ZI + m;
+            if (x < p.nx && yy < p.ny)
+                dst = p.out + static_cast<int64_t>(yy) * p.nx + x;
         }
-        store_tile<ZI, XP, MODE>(p, x0, yrow, z0, vec_ok, val);
+        if (dst != nullptr)
+            *dst = p.accumulate ? *dst + sum : sum;
     }
-    cluster_sync();  // the peers' shared memory stays valid until rank 0 has read it
+    (void)vec_ok;
+    cluster_sync();  // every rank's partial block stays valid until all ranks have read their slices
 }
 
 // ------------------------------------------------------------------------------------------
@@ -516,10 +549,6 @@ struct VariantKey {
     }
 };
 
-// Cluster sizes of the atom-split form: 2..8 are portable; 9..16 use the B200's non-portable
-// cluster sizes (opted into per kernel; refused with a device-limits error where the block does not fit).
-constexpr int kMaxPortableSplit = 8;
-constexpr int kMaxSplit = 16;
 
 // Dynamic shared memory of the atom-split form: the TMA ring, its barriers, the partial block.
 inline size_t split_smem_bytes(int threads, int values_per_thread)

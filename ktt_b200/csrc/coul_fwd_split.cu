@@ -25,6 +25,15 @@ void register_fwd_split(std::vector<VariantEntry>& v)
     add_split_unrolls<2, 1, 2, kModeSlice2d>(v);
     add_split_unrolls<4, 1, 2, kModeSlice2d>(v);
     add_split_unrolls<2, 2, 2, kModeSlice2d>(v);
+    // eight points per thread: fewer shared-memory atom loads per rsqrt, and a whole-tile FMA-pipe share
+    add_split_unrolls<4, 2, 0, kModeSlice2d>(v);
+    add_split_unrolls<4, 2, 2, kModeSlice2d>(v);
+    add_split_unrolls<4, 2, 3, kModeSlice2d>(v);
+    add_split_unrolls<2, 4, 0, kModeSlice2d>(v);
+    add_split_unrolls<2, 4, 2, kModeSlice2d>(v);
+    add_split_unrolls<8, 1, 0, kModeSlice2d>(v);
+    add_split_unrolls<8, 1, 2, kModeSlice2d>(v);
+    add_split_unrolls<2, 2, 3, kModeSlice2d>(v);
     // 3D map: z points per thread (ZI) x points per thread along x (XP)
     add_split_unrolls<4, 1, 0, kModeGrid3d>(v);
     add_split_unrolls<8, 1, 0, kModeGrid3d>(v);

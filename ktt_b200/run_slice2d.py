@@ -18,8 +18,8 @@ import time
 
 import numpy as np
 
-SHAPES = [(bx, by, xp, yi, split, soft) for (bx, by) in ((32, 4), (32, 2), (64, 2), (16, 8), (32, 8))
-          for xp in (1, 2, 4) for yi in (1, 2, 4) for split in (0, 2, 4, 8, 16) for soft in (0, 2)]
+SHAPES = [(bx, by, xp, yi, split, soft) for (bx, by) in ((32, 4), (32, 2), (64, 2), (16, 8), (32, 8), (64, 4))
+          for xp in (1, 2, 4) for yi in (1, 2, 4, 8) for split in (0, 2, 4, 8, 16) for soft in (0, 2, 3)]
 
 
 def main() -> None:
