@@ -7,15 +7,22 @@ Workload: the full 3D map, 256 x 256 x 256 grid at 0.5 A spacing, 65,536 atoms u
 evaluations per second (Gpair-evals/s, one pair = one (grid point, atom) term), whole job.
 
 Our arm (``--impl ours``, default) prints one JSON line with
-  value        device-timed throughput of the chosen form (CUDA events on the launching stream,
-               inputs resident in HBM, L2 flushed between steps), max over ranks;
-  plain        the same for the plain FP32 kernel (all-MUFU, FP32 accumulation);
-  e2e          the chosen form through the host-buffer C-ABI call (coul_forward_3d_host): atoms
+  value        device-timed throughput of the headline form -- FP32 pairs, FP64 merge of 32-atom
+               partials, part of the rsqrts on the FMA pipe, tile from ktt_b200/tuned/b200_map3d.json
+               (CUDA events on the launching stream, inputs resident in HBM, L2 flushed between
+               steps), max over ranks;
+  plain        the same for KTT's kernel form (FP32 accumulation, all rsqrts on MUFU);
+  fast_fp32    FP32 accumulation with the FMA-pipe share (faster, fails the pointwise gate);
+  exact        FP64 pairs, with its roofline against the FP64 pipe;
+  ktt_kernel   KTT's own CUDA kernels (best configuration of its space, and its reference kernel)
+               launched in this run on the same map, when built from the KTT tree;
+  e2e          the headline form through the host-buffer C-ABI call (coul_forward_3d_host): atoms
                copied from pinned host memory and the map copied back, inside the timed region;
-  roofline     achieved pair rate of the forward kernel against the MUFU+FMA pair roofline built
-               from pipe rates measured in the same run;
+  roofline     achieved pair rate of the forward kernel against the MUFU+FMA pair rooflines built
+               from pipe rates measured in the same run (and on datasheet lane counts);
   cpu_baseline the FP64 oracle (restatement of KTT's reference computation) on the host cores, on
-               a bounded sample of grid points; the same sample gives the error of the GPU maps.
+               a bounded sample of grid points; the same sample gives every form's error against the
+               accuracy gate of ktt_b200/errors.py (accuracy).
 Under torchrun each rank computes its own map (weak scaling, no collective on the data path);
 timings are reduced with MAX over ranks.
 

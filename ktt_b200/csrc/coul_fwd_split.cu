@@ -34,6 +34,10 @@ void register_fwd_split(std::vector<VariantEntry>& v)
     add_split_unrolls<8, 1, 0, kModeSlice2d>(v);
     add_split_unrolls<8, 1, 2, kModeSlice2d>(v);
     add_split_unrolls<2, 2, 3, kModeSlice2d>(v);
+    // sixteen points per thread: eight lane pairs, so the FMA-pipe share is taken within each thread
+    add_split_unrolls<8, 2, 2, kModeSlice2d>(v);
+    add_split_unrolls<8, 2, 3, kModeSlice2d>(v);
+    add_split_unrolls<4, 4, 2, kModeSlice2d>(v);
     // 3D map: z points per thread (ZI) x points per thread along x (XP)
     add_split_unrolls<4, 1, 0, kModeGrid3d>(v);
     add_split_unrolls<8, 1, 0, kModeGrid3d>(v);
