@@ -112,12 +112,18 @@ typedef struct coul_tune {
                          way the share is rsqrt_soft / 8.
                          10 + k (k = 0..7): successive patterns alternate between k and k + 1 eighths,
                          a share of (2k + 1) / 16 */
-    int atom_split;   /* 0 or 1: one CTA per point tile; 2..16: a thread-block cluster of that many
-                         CTAs shares each point tile, each streaming 1/atom_split of the atoms, the
-                         partial sums reduced over distributed shared memory (for slices and small
-                         maps with too few tiles to fill the GPU; FP32, shared-memory atoms).  Above 8
-                         the cluster uses a non-portable size; a block too large for such a cluster
-                         is refused with COUL_ERR_DEVICE_LIMITS */
+    int atom_split;   /* 0 or 1: one CTA per point tile; 2 or more: the atoms are split into that
+                         many chunks per point tile, the partial sums of a tile added in chunk order
+                         (for slices and small maps with too few tiles to fill the GPU; FP32,
+                         shared-memory atoms).  How, is split_form's choice */
+    int split_form;   /* with atom_split >= 2: 0 = a thread-block cluster of atom_split CTAs (2..16;
+                         above 8 a non-portable size, refused with COUL_ERR_DEVICE_LIMITS where the
+                         block does not fit) reduces its partial blocks over distributed shared
+                         memory; 1 = a persistent grid (as many CTAs as fit) claims (tile, chunk)
+                         items from a device queue and the CTA finishing a tile's last chunk adds the
+                         tile's partial blocks from device memory (atom_split 2..256; no clusters, so
+                         every SM gets the same share of the work; the context keeps the partial
+                         blocks, 4 bytes per point per chunk) */
 } coul_tune;
 
 typedef struct coul_grid {

@@ -16,9 +16,11 @@
 //     VECTOR_SIZE (3D) / OUTER_UNROLL_FACTOR (2D) -> points per thread along x,
 //     INNER_UNROLL_FACTOR -> atom-loop unroll, USE_CONSTANT_MEMORY -> atom source,
 //     USE_SOA -> which argument layout the 3D kernel reads,
-// plus the B200 parameters PRECISION (0 FP32, 1 compensated, 2 FP64 merge), RSQRT_SOFT (share of
-// reciprocal square roots on the FMA pipe, of 8) and ATOM_SPLIT (2..8: a thread-block cluster of
-// that many CTAs shares each point tile, each streaming a share of the atoms).  A configuration that maps to no compiled variant
+// plus the B200 parameters PRECISION (0 FP32, 1 compensated, 2 FP64 merge, 3 FP64 pairs),
+// RSQRT_SOFT (share of reciprocal square roots on the FMA pipe, of 8), ATOM_SPLIT (2 or more: the
+// atoms are split into that many chunks per point tile) and SPLIT_FORM (0: a thread-block cluster
+// of ATOM_SPLIT CTAs shares each tile, 2..16; 1: a persistent grid takes (tile, chunk) items from a
+// device queue, 2..256).  A configuration that maps to no compiled variant
 // ends with ResultStatus::CompilationFailed, one beyond the device's launch limits with
 // DeviceLimitsExceeded -- the statuses KTT reports for a kernel that fails to compile or launch.
 // A definition with no built-in implementation is rejected when it is run.  GetKernelSource still

@@ -46,7 +46,8 @@ class CoulombError(RuntimeError):
 class _Tune(ctypes.Structure):
     _fields_ = [("block_x", ctypes.c_int), ("block_y", ctypes.c_int), ("z_iterations", ctypes.c_int),
                 ("x_points", ctypes.c_int), ("unroll", ctypes.c_int), ("atom_source", ctypes.c_int),
-                ("precision", ctypes.c_int), ("rsqrt_soft", ctypes.c_int), ("atom_split", ctypes.c_int)]
+                ("precision", ctypes.c_int), ("rsqrt_soft", ctypes.c_int), ("atom_split", ctypes.c_int),
+                ("split_form", ctypes.c_int)]
 
 
 class _PipeRates(ctypes.Structure):
@@ -67,8 +68,9 @@ class Tune:
 
     block_x [WORK_GROUP_SIZE_X], block_y [WORK_GROUP_SIZE_Y], z_iterations [Z_ITERATIONS],
     x_points [VECTOR_SIZE / OUTER_UNROLL_FACTOR], unroll [INNER_UNROLL_FACTOR],
-    atom_source [USE_CONSTANT_MEMORY], precision, rsqrt_soft, atom_split (CTAs per cluster sharing a
-    point tile in the atom-split form; 0 = off).
+    atom_source [USE_CONSTANT_MEMORY], precision, rsqrt_soft, atom_split (atom chunks per point tile
+    in the atom-split form; 0 = off), split_form (0: a thread-block cluster per tile, 1: a persistent
+    grid over (tile, chunk) items from a device queue).
     """
     block_x: int = 32
     block_y: int = 4
@@ -79,6 +81,7 @@ class Tune:
     precision: int = PREC_FP32
     rsqrt_soft: int = 0
     atom_split: int = 0
+    split_form: int = 0
 
     def c(self) -> _Tune:
         return _Tune(*(int(getattr(self, f.name)) for f in fields(self)))

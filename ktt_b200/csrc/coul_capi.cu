@@ -42,6 +42,7 @@ std::vector<VariantEntry>& registry()
         register_fwd_3d_fp64(v);
         register_fwd_2d(v);
         register_fwd_split(v);
+        register_fwd_queue_split(v);
     });
     return v;
 }
@@ -244,9 +245,12 @@ int validate_tune(const coul_tune* t, int mode, int soa, const VariantEntry** ou
         return set_error(COUL_ERR_INVALID_ARGUMENT, "unknown precision");
     if (t->rsqrt_soft < 0 || (t->rsqrt_soft > 8 && t->rsqrt_soft < kSoftAlternate) || t->rsqrt_soft > kSoftAlternate + 7)
         return set_error(COUL_ERR_INVALID_ARGUMENT, "rsqrt_soft must be in 0..8 or 10..17");
-    if (t->atom_split < 0 || t->atom_split > kMaxSplit)
-        return set_error(COUL_ERR_INVALID_ARGUMENT, "atom_split must be in 0.." + std::to_string(kMaxSplit));
-    const int split = t->atom_split >= 2 ? 1 : 0;
+    if (t->split_form != 0 && t->split_form != 1)
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "split_form must be 0 (cluster) or 1 (queue)");
+    const int max_split = t->split_form ? kMaxQueueSplit : kMaxSplit;
+    if (t->atom_split < 0 || t->atom_split > max_split)
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "atom_split must be in 0.." + std::to_string(max_split));
+    const int split = t->atom_split >= 2 ? (t->split_form ? 2 : 1) : 0;
     if (split && (t->atom_source != COUL_ATOMS_SHARED_TMA || soa || t->precision != COUL_PREC_FP32))
         return set_error(COUL_ERR_UNSUPPORTED,
                          "the atom-split form streams float4 atoms through shared memory with FP32 accumulation");
@@ -280,6 +284,65 @@ int validate_grid(const coul_grid* g)
     return COUL_OK;
 }
 
+// Device memory of the queue form, kept in the context and grown on demand: the partial blocks of
+// every (tile, chunk) item, one counter per tile and the queue head.
+struct QueueWorkspace {
+    void* mem = nullptr;
+    size_t bytes = 0;
+};
+
+// The queue form's persistent grid and zeroed counters, enqueued on the context's stream.
+int queue_split_setup(coul_ctx* ctx, const VariantEntry* v, FwdLaunch& L, const coul_tune* t)
+{
+    const int threads = t->block_x * t->block_y;
+    const int64_t tiles = static_cast<int64_t>(L.grid.x) * L.grid.y * L.grid.z;
+    const int64_t values = static_cast<int64_t>(threads) * t->z_iterations * t->x_points;
+    const size_t partial_bytes = static_cast<size_t>(tiles * t->atom_split * values) * sizeof(float);
+    const size_t done_offset = (partial_bytes + 255) / 256 * 256;
+    const size_t counter_offset = (done_offset + static_cast<size_t>(tiles) * sizeof(unsigned) + 255) / 256 * 256;
+    const size_t need = counter_offset + 256;
+    auto* ws = static_cast<QueueWorkspace*>(ctx->queue_workspace);
+    if (ws == nullptr) {
+        ws = new QueueWorkspace();
+        ctx->queue_workspace = ws;
+        ctx->cleanups.push_back([ws] {
+            if (ws->mem)
+                cudaFree(ws->mem);
+            delete ws;
+        });
+    }
+    cudaError_t e;
+    if (need > ws->bytes) {
+        if (ws->mem) {
+            cudaStreamSynchronize(ctx->stream);
+            cudaFree(ws->mem);
+            ws->mem = nullptr;
+            ws->bytes = 0;
+        }
+        if ((e = cudaMalloc(&ws->mem, need)) != cudaSuccess)
+            return set_error(COUL_ERR_OUT_OF_MEMORY, std::string("atom-split queue workspace: ") + cudaGetErrorString(e));
+        ws->bytes = need;
+    }
+    auto* base = static_cast<unsigned char*>(ws->mem);
+    // the per-tile counters and the queue head start every launch at zero
+    if ((e = cudaMemsetAsync(base + done_offset, 0, need - done_offset, ctx->stream)) != cudaSuccess)
+        return cuda_error(e, "queue counters reset");
+    int blocks_per_sm = 0;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, v->occupancy_kernel, threads, L.smem)) !=
+        cudaSuccess)
+        return cuda_error(e, "occupancy query");
+    if (blocks_per_sm < 1)
+        return set_error(COUL_ERR_DEVICE_LIMITS, "the queue form's block does not fit on an SM");
+    L.queue.partial = reinterpret_cast<float*>(base);
+    L.queue.tile_done = reinterpret_cast<unsigned*>(base + done_offset);
+    L.queue.counter = reinterpret_cast<unsigned long long*>(base + counter_offset);
+    L.queue.chunks = t->atom_split;
+    const int64_t items = tiles * t->atom_split;
+    const int64_t ctas = static_cast<int64_t>(blocks_per_sm) * ctx->sm_count;
+    L.queue.ctas = static_cast<int>(ctas < items ? ctas : items);
+    return COUL_OK;
+}
+
 // Launch one forward variant over a grid; shared by the 3D AoS/SoA and 2D entry points and by
 // the batched path's plain-launch baseline.
 int launch_forward(coul_ctx* ctx, const VariantEntry* v, const FwdParams& prm, int mode, const coul_tune* t)
@@ -303,11 +366,16 @@ int launch_forward(coul_ctx* ctx, const VariantEntry* v, const FwdParams& prm, i
         return set_error(COUL_ERR_DEVICE_LIMITS, "grid too large for one launch");
     L.grid = dim3(static_cast<unsigned>(gx), static_cast<unsigned>(gy), static_cast<unsigned>(gz));
     L.smem = (t->atom_source == COUL_ATOMS_SHARED_TMA) ? (kStages * kTileAtoms * 16 + kStages * 8) : 0;
-    if (v->key.split) {
+    if (v->key.split == 1) {
         L.split = t->atom_split;
         L.smem = split_smem_bytes(t->block_x * t->block_y, t->z_iterations * t->x_points);
         if (static_cast<int64_t>(L.grid.x) * L.split > 2147483647LL)
             return set_error(COUL_ERR_DEVICE_LIMITS, "grid too large for one launch");
+    } else if (v->key.split == 2) {
+        L.split = t->atom_split;
+        const int rc = queue_split_setup(ctx, v, L, t);
+        if (rc != COUL_OK)
+            return rc;
     }
     const int xp = t->x_points;
     L.vec_store = (xp > 1 && prm.nx % xp == 0 &&
@@ -574,6 +642,7 @@ COUL_API void coul_tune_default(coul_tune* t)
     t->precision = COUL_PREC_FP32;
     t->rsqrt_soft = 0;
     t->atom_split = 0;
+    t->split_form = 0;
 }
 
 COUL_API int coul_tune_supported(const coul_tune* t) { return validate_tune(t, kModeGrid3d, 0, nullptr); }
@@ -595,6 +664,7 @@ COUL_API int coul_variant_get(int i, coul_tune* t, int* is_2d, int* is_soa)
     t->precision = k.prec;
     t->rsqrt_soft = k.soft;
     t->atom_split = k.split ? 2 : 0;
+    t->split_form = k.split == 2 ? 1 : 0;
     if (is_2d)
         *is_2d = k.mode == kModeSlice2d ? 1 : 0;
     if (is_soa)

@@ -27,18 +27,29 @@ enum : int { kPrecFp32 = 0, kPrecCompensated = 1, kPrecFp64Merge = 2, kPrecFp64P
 // cluster sizes (opted into per kernel; refused with a device-limits error where the block does not fit).
 constexpr int kMaxPortableSplit = 8;
 constexpr int kMaxSplit = 16;
+constexpr int kMaxQueueSplit = 256;  // chunks per tile of the queue form
 
 // Per translation unit: the constant-memory atom chunk.  Only the TU that instantiates the
 // constant-memory variants uses it; it has internal linkage so no relocatable device code is needed.
 static __constant__ float4 c_atoms[kConstAtoms];
 
+// Device-memory state of the queue form of the atom split (kept in the context, grown on demand).
+struct SplitQueue {
+    float* partial;               // one partial block per (tile, chunk) item
+    unsigned* tile_done;          // items finished per tile, zero at launch
+    unsigned long long* counter;  // the item queue's head, zero at launch
+    int chunks;                   // atom chunks per tile
+    int ctas;                     // persistent CTAs of the launch
+};
+
 struct FwdLaunch {
     FwdParams p;
-    dim3 grid;  // one entry per point tile (the atom-split form multiplies grid.x by `split`)
+    dim3 grid;  // one entry per point tile (the cluster form multiplies grid.x by `split`)
     dim3 block;
     size_t smem;
     int vec_store;  // 1 if x-vector stores are aligned for this launch
-    int split;      // atom-split form: CTAs per cluster sharing one point tile (0 / 1 = one CTA per tile)
+    int split;      // atom split: chunks of the atoms per point tile (0 / 1 = none)
+    SplitQueue queue;  // the queue form's device memory (unused by the other forms)
 };
 
 template <int MODE, int XP, int ZH, int SOFT, int PHASE, bool HALF, int ZA = ZH>
@@ -446,6 +457,34 @@ __global__ void __launch_bounds__(kMaxThreads) fwd_kernel(const FwdParams p, con
     }
 }
 
+// Stores value i = (k * ZI + m) * nthreads + t of a tile's register blocks -- thread t's k-th x point,
+// m-th blocked point -- at its grid point (edge-guarded, accumulate semantics of p).  The tile is
+// (tile_x, tile_y) of the launch's block geometry, z0 its first z point (3D).
+template <int ZI, int XP, int MODE>
+__device__ __forceinline__ void store_value(const FwdParams& p, const int tile_x, const int tile_y, const int z0,
+                                            const int i, const float v)
+{
+    const int nthreads = static_cast<int>(blockDim.x * blockDim.y);
+    const int t = i % nthreads;
+    const int km = i / nthreads;
+    const int k = km / ZI;
+    const int m = km % ZI;
+    const int x = (tile_x * static_cast<int>(blockDim.x) + t % static_cast<int>(blockDim.x)) * XP + k;
+    const int ty = tile_y * static_cast<int>(blockDim.y) + t / static_cast<int>(blockDim.x);
+    float* dst = nullptr;
+    if constexpr (MODE == kModeGrid3d) {
+        const int z = z0 + m;
+        if (x < p.nx && ty < p.ny && z < p.nz)
+            dst = p.out + (static_cast<int64_t>(z - p.z_base) * p.ny + ty) * p.nx + x;
+    } else {
+        const int yy = ty * ZI + m;
+        if (x < p.nx && yy < p.ny)
+            dst = p.out + static_cast<int64_t>(yy) * p.nx + x;
+    }
+    if (dst != nullptr)
+        *dst = p.accumulate ? *dst + v : v;
+}
+
 // Atom-split form for maps with too few points to fill the GPU one tile per CTA (a 2D slice, a
 // small 3D map): a thread-block cluster of S CTAs shares one point tile, CTA rank r takes the r-th
 // of S contiguous atom ranges through its own TMA ring, and rank 0 sums the S partial blocks from
@@ -498,6 +537,7 @@ __global__ void __launch_bounds__(kMaxThreads) split_kernel(const FwdParams p, c
     cluster_sync();
     // Reduce-scatter over the cluster: rank r sums the r-th of S slices of the tile's partial blocks,
     // every rank's value of a point added in rank order (deterministic), and stores those points.
+    const int tile_y = static_cast<int>(blockIdx.y);
     const int values = nthreads * XP * ZI;
     const int per = (values + static_cast<int>(S) - 1) / static_cast<int>(S);
     const int end = (static_cast<int>(r) + 1) * per < values ? (static_cast<int>(r) + 1) * per : values;
@@ -512,28 +552,89 @@ __global__ void __launch_bounds__(kMaxThreads) split_kernel(const FwdParams p, c
         for (int rank = 1; rank < kMaxSplit; ++rank)
             if (rank < static_cast<int>(S))
                 sum += part[rank];
-        // the point of value i = (k * ZI + m) * nthreads + t: thread t's k-th x point, m-th blocked point
-        const int t = i % nthreads;
-        const int km = i / nthreads;
-        const int k = km / ZI;
-        const int m = km % ZI;
-        const int x = (tile_x * static_cast<int>(blockDim.x) + t % static_cast<int>(blockDim.x)) * XP + k;
-        const int ty = static_cast<int>(blockIdx.y * blockDim.y) + t / static_cast<int>(blockDim.x);
-        float* dst = nullptr;
-        if constexpr (MODE == kModeGrid3d) {
-            const int z = z0 + m;
-            if (x < p.nx && ty < p.ny && z < p.nz)
-                dst = p.out + (static_cast<int64_t>(z - p.z_base) * p.ny + ty) * p.nx + x;
-        } else {
-            const int yy = ty * ZI + m;
-            if (x < p.nx && yy < p.ny)
-                dst = p.out + static_cast<int64_t>(yy) * p.nx + x;
-        }
-        if (dst != nullptr)
-            *dst = p.accumulate ? *dst + sum : sum;
+        store_value<ZI, XP, MODE>(p, tile_x, tile_y, z0, i, sum);
     }
     (void)vec_ok;
     cluster_sync();  // every rank's partial block stays valid until all ranks have read their slices
+}
+
+// The queue form of the atom split, for the same small maps without thread-block clusters: a
+// persistent grid (as many CTAs as fit, so every SM gets the same share) claims (tile, chunk) items
+// from a device counter -- the chunks of one tile are consecutive items -- evaluates the chunk's
+// atoms on the tile through its TMA ring and writes the tile's partial block to device memory.  The
+// CTA that finishes a tile's last chunk (a counter per tile; each writer fences its partial before
+// counting) sums the tile's C partial blocks in chunk order, deterministic whichever CTAs ran them,
+// and stores the tile.  No CTA waits on another.
+template <int ZI, int XP, int UNR, int SOFT, int MODE>
+__global__ void __launch_bounds__(kMaxThreads) queue_split_kernel(const FwdParams p, const SplitQueue sq,
+                                                                  const int tiles_x, const int tiles_y,
+                                                                  const int64_t items)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + kStages * kTileAtoms * 16);
+    __shared__ long long s_item;
+    __shared__ int s_last;
+    const int nthreads = blockDim.x * blockDim.y;
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    const int values = nthreads * XP * ZI;
+    const int C = sq.chunks;
+    const int64_t chunk = (p.n_atoms + C - 1) / C;
+    ring_init(full, tid);
+    uint32_t gstage = 0;
+
+    for (;;) {
+        if (tid == 0)
+            s_item = static_cast<long long>(atomicAdd(sq.counter, 1ull));
+        __syncthreads();
+        const long long item = s_item;
+        __syncthreads();
+        if (item >= items)
+            return;
+        const int t = static_cast<int>(item / C);
+        const int c = static_cast<int>(item % C);
+        const int tile_x = t % tiles_x;
+        const int tile_y = (t / tiles_x) % tiles_y;
+        const int tile_z = t / (tiles_x * tiles_y);
+        const int x0 = (tile_x * static_cast<int>(blockDim.x) + static_cast<int>(threadIdx.x)) * XP;
+        int yrow, z0;
+        if constexpr (MODE == kModeGrid3d) {
+            yrow = tile_y * static_cast<int>(blockDim.y) + static_cast<int>(threadIdx.y);
+            z0 = p.z_base + tile_z * ZI;
+        } else {
+            yrow = (tile_y * static_cast<int>(blockDim.y) + static_cast<int>(threadIdx.y)) * ZI;
+            z0 = 0;
+        }
+        FwdParams q = p;
+        const int64_t begin = chunk * c < p.n_atoms ? chunk * c : p.n_atoms;
+        q.atoms = p.atoms + begin;
+        q.n_atoms = (p.n_atoms - begin) < chunk ? (p.n_atoms - begin) : chunk;
+        float val[XP][ZI];
+        // the FMA-pipe share's phase advances with the chunk and the warp (as in the cluster form)
+        if (!tile_accumulate<ZI, XP, UNR, kSrcShared, 0, kPrecFp32, SOFT, MODE>(
+                q, x0, yrow, z0, smem_raw, full, gstage, val, static_cast<uint32_t>(c) + static_cast<uint32_t>(tid) / 32u))
+            return;  // a bounded wait expired: the status word says so, the tile stays unfinished
+        float* part = sq.partial + item * values;
+#pragma unroll
+        for (int k = 0; k < XP; ++k)
+#pragma unroll
+            for (int m = 0; m < ZI; ++m)
+                part[(k * ZI + m) * nthreads + tid] = val[k][m];
+        __threadfence();  // the partial block is visible device-wide before this chunk is counted
+        __syncthreads();
+        if (tid == 0)
+            s_last = atomicAdd(&sq.tile_done[t], 1u) == static_cast<unsigned>(C - 1) ? 1 : 0;
+        __syncthreads();
+        if (s_last) {
+            __threadfence();
+            const float* tile_parts = sq.partial + static_cast<int64_t>(t) * C * values;
+            for (int i = tid; i < values; i += nthreads) {
+                float sum = __ldcg(tile_parts + i);  // the L2 copy: other SMs wrote these
+                for (int cc = 1; cc < C; ++cc)
+                    sum += __ldcg(tile_parts + static_cast<int64_t>(cc) * values + i);
+                store_value<ZI, XP, MODE>(p, tile_x, tile_y, z0, i, sum);
+            }
+        }
+    }
 }
 
 // ------------------------------------------------------------------------------------------
@@ -541,7 +642,7 @@ __global__ void __launch_bounds__(kMaxThreads) split_kernel(const FwdParams p, c
 // ------------------------------------------------------------------------------------------
 struct VariantKey {
     int zi, xp, unroll, src, soa, prec, soft, mode;
-    int split;  // 1 for the atom-split (cluster) form
+    int split;  // 1 for the atom-split cluster form, 2 for its queue form
     bool operator==(const VariantKey& o) const
     {
         return zi == o.zi && xp == o.xp && unroll == o.unroll && src == o.src && soa == o.soa && prec == o.prec &&
@@ -562,7 +663,8 @@ using FwdLaunchFn = cudaError_t (*)(const FwdLaunch&, cudaStream_t);
 struct VariantEntry {
     VariantKey key;
     FwdLaunchFn launch;
-    int regs;  // filled lazily from cudaFuncGetAttributes (0 = unknown)
+    int regs;                        // filled lazily from cudaFuncGetAttributes (0 = unknown)
+    const void* occupancy_kernel;    // the kernel a persistent form sizes its grid by (else null)
 };
 
 template <int ZI, int XP, int UNR, int SRC, int SOA, int PREC, int SOFT, int MODE>
@@ -602,7 +704,7 @@ template <int ZI, int XP, int UNR, int SRC, int SOA, int PREC, int SOFT, int MOD
 void add_variant(std::vector<VariantEntry>& v)
 {
     v.push_back(VariantEntry{VariantKey{ZI, XP, UNR, SRC, SOA, PREC, SOFT, MODE, 0},
-                             &launch_fwd<ZI, XP, UNR, SRC, SOA, PREC, SOFT, MODE>, 0});
+                             &launch_fwd<ZI, XP, UNR, SRC, SOA, PREC, SOFT, MODE>, 0, nullptr});
 }
 
 // Cluster launch of the atom-split form: grid.x tiles x `split` CTAs, clusters of `split` along x.
@@ -645,11 +747,32 @@ cudaError_t launch_split(const FwdLaunch& L, cudaStream_t stream)
     return cudaLaunchKernelEx(&cfg, kernel, L.p, L.vec_store);
 }
 
+// Persistent launch of the queue form: L.queue holds the zeroed counters and the partial blocks,
+// L.grid the point tiles.
+template <int ZI, int XP, int UNR, int SOFT, int MODE>
+cudaError_t launch_queue_split(const FwdLaunch& L, cudaStream_t stream)
+{
+    auto kernel = queue_split_kernel<ZI, XP, UNR, SOFT, MODE>;
+    const int64_t tiles = static_cast<int64_t>(L.grid.x) * L.grid.y * L.grid.z;
+    const int64_t items = tiles * L.queue.chunks;
+    kernel<<<dim3(static_cast<unsigned>(L.queue.ctas)), L.block, L.smem, stream>>>(
+        L.p, L.queue, static_cast<int>(L.grid.x), static_cast<int>(L.grid.y), items);
+    return cudaGetLastError();
+}
+
+template <int ZI, int XP, int UNR, int SOFT, int MODE>
+void add_queue_split_variant(std::vector<VariantEntry>& v)
+{
+    v.push_back(VariantEntry{VariantKey{ZI, XP, UNR, kSrcShared, 0, kPrecFp32, SOFT, MODE, 2},
+                             &launch_queue_split<ZI, XP, UNR, SOFT, MODE>, 0,
+                             reinterpret_cast<const void*>(&queue_split_kernel<ZI, XP, UNR, SOFT, MODE>)});
+}
+
 template <int ZI, int XP, int UNR, int SOFT, int MODE>
 void add_split_variant(std::vector<VariantEntry>& v)
 {
     v.push_back(VariantEntry{VariantKey{ZI, XP, UNR, kSrcShared, 0, kPrecFp32, SOFT, MODE, 1},
-                             &launch_split<ZI, XP, UNR, SOFT, MODE>, 0});
+                             &launch_split<ZI, XP, UNR, SOFT, MODE>, 0, nullptr});
 }
 
 // Register the four atom-loop unrolls {1, 2, 4, 8} of one variant family.
@@ -674,5 +797,6 @@ void register_fwd_3d_soft_fp64m(std::vector<VariantEntry>& v);
 void register_fwd_3d_fp64(std::vector<VariantEntry>& v);
 void register_fwd_2d(std::vector<VariantEntry>& v);
 void register_fwd_split(std::vector<VariantEntry>& v);
+void register_fwd_queue_split(std::vector<VariantEntry>& v);
 
 }  // namespace coul

@@ -28,6 +28,7 @@ struct coul_ctx {
     int cc_minor = 0;
     std::vector<std::function<void()>> cleanups;  // frees buffers owned by other units (run at destroy)
     void* adjoint_workspace = nullptr;            // FP64 partials of coul_adjoint_3d (coul_adjoint.cu)
+    void* queue_workspace = nullptr;              // partial blocks and counters of the atom split's queue form
 };
 
 namespace coul {
@@ -41,5 +42,6 @@ bool aligned16(const void* p);
 int validate_tune(const coul_tune* t, int mode, int soa, const VariantEntry** out);
 int validate_grid(const coul_grid* g);
 int launch_forward(coul_ctx* ctx, const VariantEntry* v, const FwdParams& prm, int mode, const coul_tune* t);
+int queue_split_setup(coul_ctx* ctx, const VariantEntry* v, FwdLaunch& L, const coul_tune* t);
 
 }  // namespace coul

@@ -1184,6 +1184,7 @@ Nanoseconds TunerCore::LaunchDefinition(const KernelData& kernel, const KernelDe
     tune.precision = static_cast<int>(parameter("PRECISION", 0));
     tune.rsqrt_soft = static_cast<int>(parameter("RSQRT_SOFT", 0));
     tune.atom_split = static_cast<int>(parameter("ATOM_SPLIT", 0));
+    tune.split_form = static_cast<int>(parameter("SPLIT_FORM", 0));
 
     // a 3D launch: the definition's global size, or (for definitions sized by modifier scripts) the
     // launch's, spans more than one z plane

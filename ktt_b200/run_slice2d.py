@@ -5,8 +5,8 @@
 Atoms x, y ~ U[0, 128), z ~ U[0, 32), q ~ U[-1, 1]; the slice at z = 16 A.  For each compiled 2D
 tile shape: device time of the slice kernel (median of --repeat event-timed launches), pair rate,
 error against the FP64 oracle over the whole slice.  Shapes include the atom-split form (a cluster
-of 2, 4 or 8 CTAs per point tile, each streaming a share of the atoms) and 2/8 of the rsqrts on the
-FMA pipe.  Then the whole call as a KTT user makes it (host atoms in, dz^2 slicing on the device,
+of 2 .. 16 CTAs per point tile, each streaming a share of the atoms, or its queue form, a persistent
+grid over (tile, atom chunk) items) and 2/8 or 3/8 of the rsqrts on the FMA pipe.  Then the whole call as a KTT user makes it (host atoms in, dz^2 slicing on the device,
 host slice out; wall clock, median) for the fastest shape, and the FP64 oracle's own time on the
 host.  One JSON line per measurement.
 """
@@ -18,17 +18,20 @@ import time
 
 import numpy as np
 
-SHAPES = [(bx, by, xp, yi, split, soft) for (bx, by) in ((32, 4), (32, 2), (64, 2), (16, 8), (32, 8), (64, 4))
+SHAPES = [(bx, by, xp, yi, split, soft, 0) for (bx, by) in ((32, 4), (32, 2), (64, 2), (16, 8), (32, 8), (64, 4))
           for xp in (1, 2, 4) for yi in (1, 2, 4, 8) for split in (0, 2, 4, 8, 16) for soft in (0, 2, 3)]
+# the queue form of the atom split (split_form 1): chunk counts beyond a cluster's 16 as well
+SHAPES += [(bx, by, xp, yi, split, soft, 1) for (bx, by) in ((32, 4), (16, 8), (64, 2), (32, 8), (64, 4))
+           for xp in (1, 2, 4) for yi in (2, 4, 8) for split in (8, 16, 24, 32, 48, 64) for soft in (0, 2, 3)]
 
 
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--repeat", type=int, default=50)
     ap.add_argument("--only", default="", help="one configuration: block x, block y, x points, rows, atom split, "
-                                               "rsqrt share (for profiling)")
+                                               "rsqrt share[, split form] (for profiling)")
     args = ap.parse_args()
-    shapes = [tuple(int(v) for v in args.only.split(","))] if args.only else SHAPES
+    shapes = [(tuple(int(v) for v in args.only.split(",")) + (0,))[:7]] if args.only else SHAPES
 
     import torch
 
@@ -48,9 +51,9 @@ def main() -> None:
     d_sliced = ctx.slice_atoms(atoms, case.z_slice)
     out = torch.empty((ny, nx), dtype=torch.float32, device="cuda")
     results = []
-    for bx, by, xp, yi, split, soft in shapes:
+    for bx, by, xp, yi, split, soft, form in shapes:
         tune = ktt_b200.Tune(block_x=bx, block_y=by, x_points=xp, z_iterations=yi, atom_split=split,
-                             rsqrt_soft=soft)
+                             rsqrt_soft=soft, split_form=form)
         if not ktt_b200.tune_supported_2d(tune):
             continue
         ms = []

@@ -62,6 +62,13 @@ def test_tune_validation_without_device():
     assert ktt_b200.tune_supported_2d(T(z_iterations=2, x_points=1, atom_split=4))
     assert ktt_b200.tune_supported_2d(T(z_iterations=4, x_points=4))
     assert not ktt_b200.tune_supported_2d(T(z_iterations=8, x_points=2, atom_split=4))
+    # the queue form of the atom split: any chunk count 2..256, no clusters
+    for s in (2, 17, 64, 256):
+        assert ktt_b200.tune_supported(T(atom_split=s, split_form=1, **split))
+        assert ktt_b200.tune_supported_2d(T(z_iterations=4, x_points=2, rsqrt_soft=2, atom_split=s, split_form=1))
+    assert not ktt_b200.tune_supported(T(atom_split=257, split_form=1, **split))
+    assert not ktt_b200.tune_supported(T(atom_split=4, split_form=2, **split))
+    assert not ktt_b200.tune_supported(T(atom_split=4, split_form=1, precision=ktt_b200.PREC_FP64_MERGE, **split))
 
 
 def test_variant_inventory():
@@ -69,11 +76,13 @@ def test_variant_inventory():
     assert len(vs) == ktt_b200.load_library().coul_variant_count()
     keys = {(t.z_iterations, t.x_points, t.unroll, t.atom_source, t.precision, t.rsqrt_soft, d2, soa)
             for t, d2, soa in vs if t.atom_split == 0}
-    split_keys = {(t.z_iterations, t.x_points, t.unroll, t.rsqrt_soft, d2) for t, d2, soa in vs if t.atom_split}
+    split_keys = {(t.z_iterations, t.x_points, t.unroll, t.rsqrt_soft, t.split_form, d2)
+                  for t, d2, soa in vs if t.atom_split}
     assert len(keys) + len(split_keys) == len(vs)  # no duplicates
-    # the atom-split (cluster) form: FP32, float4 atoms through shared memory, 2D and 3D
+    # the atom-split forms (cluster and queue): FP32, float4 atoms through shared memory, 2D and 3D
     assert all(t.precision == 0 and t.atom_source == 0 and not soa for t, _, soa in vs if t.atom_split)
-    assert any(d2 for _, _, _, _, d2 in split_keys) and any(not d2 for _, _, _, _, d2 in split_keys)
+    for form in (0, 1):
+        assert any(d2 for *_, f, d2 in split_keys if f == form) and any(not d2 for *_, f, d2 in split_keys if f == form)
     # the KTT CUDA space of CoulombSum3d.cpp: Z_ITERATIONS x unroll x USE_SOA, all present for x_points 1
     for zi in (1, 2, 4, 8, 16, 32):
         for un in (1, 2, 4, 8):

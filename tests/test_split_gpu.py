@@ -1,7 +1,8 @@
-"""The atom-split (thread-block cluster) form of the forward kernel against the FP64 oracle and
-against the one-CTA-per-tile form: 3D maps and 2D slices, cluster sizes 2..16 (above 8 the B200's
-non-portable cluster sizes), ragged atom counts
-(fewer atoms than CTAs in a cluster included), accumulate semantics, run-to-run determinism."""
+"""The atom-split forms of the forward kernel against the FP64 oracle and against the
+one-CTA-per-tile form: the thread-block cluster form (cluster sizes 2..16, above 8 the B200's
+non-portable cluster sizes) and the queue form (a persistent grid over (tile, chunk) items, 2..256
+chunks); 3D maps and 2D slices, ragged atom counts (fewer atoms than chunks included), accumulate
+semantics, run-to-run determinism, and the two forms equal bit for bit for the same chunk count."""
 import numpy as np
 import pytest
 
@@ -84,3 +85,47 @@ def test_split_slab_equals_split_map(ctx):
     full = ctx.forward_3d(atoms, dims, h, tune=tune)
     slab = ctx.forward_3d_slab(atoms, dims, h, 16, 40, tune=tune)
     assert torch.equal(slab, full[16:40])
+
+
+@pytest.mark.parametrize("n_atoms", [0, 1, 5, 300, 4000, 8195])
+@pytest.mark.parametrize("chunks", [2, 16, 64, 256])
+def test_queue_split_3d_matches_oracle(ctx, n_atoms, chunks):
+    import torch
+    a = _atoms(n_atoms, seed=n_atoms + 57)
+    dims, h, origin = (37, 29, 19), 0.5, (-1.0, 0.5, 2.0)
+    tune = ktt_b200.Tune(block_x=32, block_y=4, z_iterations=8, x_points=2, rsqrt_soft=2, atom_split=chunks,
+                         split_form=1)
+    atoms = torch.from_numpy(a).cuda() if n_atoms else torch.zeros((0, 4), device="cuda")
+    out = torch.full((dims[2], dims[1], dims[0]), float("nan"), device="cuda")
+    ctx.forward_3d(atoms, dims, h, origin, tune=tune, out=out)
+    got = out.cpu().numpy()
+    if n_atoms == 0:
+        assert np.all(got == 0.0)
+        return
+    ref = oracle.grid3d(a, h, dims, origin)
+    assert errors.report(got, ref)["rel_norm"] <= TOL
+    again = ctx.forward_3d(atoms, dims, h, origin, tune=tune)
+    assert torch.equal(out, again)  # the chunk order of the sums does not depend on scheduling
+
+
+@pytest.mark.parametrize("shape", [(2, 2, 0), (4, 2, 2), (4, 1, 2), (8, 2, 2)])
+@pytest.mark.parametrize("chunks", [4, 16, 48])
+def test_queue_split_2d_slice(ctx, shape, chunks):
+    import torch
+    zi, xp, soft = shape
+    case = workloads.slice_2d(n_atoms=4000, n=256)
+    ref = oracle.slice2d(case.ktt_atoms(), case.spacing, case.nx, case.ny)
+    sliced = ctx.slice_atoms(torch.from_numpy(case.atoms).cuda(), case.z_slice)
+    tune = ktt_b200.Tune(block_x=32, block_y=4, z_iterations=zi, x_points=xp, rsqrt_soft=soft, atom_split=chunks,
+                         split_form=1)
+    got = ctx.forward_2d(sliced, case.spacing, case.nx, case.ny, tune=tune)
+    assert errors.report(got.cpu().numpy(), ref)["rel_norm"] <= TOL
+    if chunks <= 16:
+        # the cluster form with as many CTAs per tile adds the same partials in the same order
+        cluster = ktt_b200.Tune(**dict(tune.as_dict(), split_form=0))
+        if ktt_b200.tune_supported_2d(cluster):
+            assert torch.equal(got, ctx.forward_2d(sliced, case.spacing, case.nx, case.ny, tune=cluster))
+    base = torch.linspace(-2, 2, case.nx * case.ny, device="cuda").reshape(case.ny, case.nx)
+    acc = base.clone()
+    ctx.forward_2d(sliced, case.spacing, case.nx, case.ny, tune=tune, out=acc, accumulate=True)
+    assert torch.equal(acc, base + got)
