@@ -570,6 +570,7 @@ __global__ void __launch_bounds__(kMaxThreads) queue_split_kernel(const FwdParam
                                                                   const int tiles_x, const int tiles_y,
                                                                   const int64_t items)
 {
+    static_assert((XP * ZI) % 4 == 0, "the reduction reads a thread's values four at a time");
     extern __shared__ __align__(128) unsigned char smem_raw[];
     uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + kStages * kTileAtoms * 16);
     __shared__ long long s_item;
@@ -626,12 +627,37 @@ __global__ void __launch_bounds__(kMaxThreads) queue_split_kernel(const FwdParam
         __syncthreads();
         if (s_last) {
             __threadfence();
-            const float* tile_parts = sq.partial + static_cast<int64_t>(t) * C * values;
-            for (int i = tid; i < values; i += nthreads) {
-                float sum = __ldcg(tile_parts + i);  // the L2 copy: other SMs wrote these
-                for (int cc = 1; cc < C; ++cc)
-                    sum += __ldcg(tile_parts + static_cast<int64_t>(cc) * values + i);
-                store_value<ZI, XP, MODE>(p, tile_x, tile_y, z0, i, sum);
+            // four consecutive values per thread (values is a multiple of 4: the partial blocks are
+            // 16-byte aligned), the chunks' partials loaded kBatch at a time as independent 16-byte
+            // loads of the L2 copies (other SMs wrote them), added in chunk order
+            const float4* tile_parts = reinterpret_cast<const float4*>(sq.partial + static_cast<int64_t>(t) * C * values);
+            const int quads = values / 4;
+            constexpr int kBatch = 8;
+            for (int i = tid; i < quads; i += nthreads) {
+                float4 sum = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                for (int c0 = 0; c0 < C; c0 += kBatch) {
+                    float4 part[kBatch];
+#pragma unroll
+                    for (int j = 0; j < kBatch; ++j)
+                        part[j] = c0 + j < C ? __ldcg(tile_parts + static_cast<int64_t>(c0 + j) * quads + i)
+                                             : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+#pragma unroll
+                    for (int j = 0; j < kBatch; ++j)
+                        if (c0 + j < C) {
+                            if (c0 + j == 0) {
+                                sum = part[j];
+                            } else {
+                                sum.x += part[j].x;
+                                sum.y += part[j].y;
+                                sum.z += part[j].z;
+                                sum.w += part[j].w;
+                            }
+                        }
+                }
+                store_value<ZI, XP, MODE>(p, tile_x, tile_y, z0, 4 * i + 0, sum.x);
+                store_value<ZI, XP, MODE>(p, tile_x, tile_y, z0, 4 * i + 1, sum.y);
+                store_value<ZI, XP, MODE>(p, tile_x, tile_y, z0, 4 * i + 2, sum.z);
+                store_value<ZI, XP, MODE>(p, tile_x, tile_y, z0, 4 * i + 3, sum.w);
             }
         }
     }
