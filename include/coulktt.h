@@ -123,7 +123,11 @@ typedef struct coul_tune {
                          items from a device queue and the CTA finishing a tile's last chunk adds the
                          tile's partial blocks from device memory (atom_split 2..256; no clusters, so
                          every SM gets the same share of the work; the context keeps the partial
-                         blocks, 4 bytes per point per chunk) */
+                         blocks, 4 bytes per point per chunk); 2 = balanced: a resident grid whose
+                         CTAs take equal contiguous ranges of the (point tile, atom) space, each CTA
+                         block_x x block_y x atom_split threads (at most 1024; atom_split 2..32 groups
+                         that share the tile's points and split every atom stage), a tile split
+                         between CTAs finished from device memory by the CTA adding its last piece */
 } coul_tune;
 
 typedef struct coul_grid {

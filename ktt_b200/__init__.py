@@ -69,8 +69,10 @@ class Tune:
     block_x [WORK_GROUP_SIZE_X], block_y [WORK_GROUP_SIZE_Y], z_iterations [Z_ITERATIONS],
     x_points [VECTOR_SIZE / OUTER_UNROLL_FACTOR], unroll [INNER_UNROLL_FACTOR],
     atom_source [USE_CONSTANT_MEMORY], precision, rsqrt_soft, atom_split (atom chunks per point tile
-    in the atom-split form; 0 = off), split_form (0: a thread-block cluster per tile, 1: a persistent
-    grid over (tile, chunk) items from a device queue).
+    in the atom-split form, or atom groups per CTA in its balanced form; 0 = off), split_form (0: a
+    thread-block cluster per tile, 1: a persistent grid over (tile, chunk) items from a device queue,
+    2: a resident grid whose CTAs take equal ranges of the (tile, atom) space, the block being
+    block_x x block_y x atom_split threads).
     """
     block_x: int = 32
     block_y: int = 4

@@ -43,6 +43,7 @@ std::vector<VariantEntry>& registry()
         register_fwd_2d(v);
         register_fwd_split(v);
         register_fwd_queue_split(v);
+        register_fwd_balanced_split(v);
     });
     return v;
 }
@@ -245,12 +246,15 @@ int validate_tune(const coul_tune* t, int mode, int soa, const VariantEntry** ou
         return set_error(COUL_ERR_INVALID_ARGUMENT, "unknown precision");
     if (t->rsqrt_soft < 0 || (t->rsqrt_soft > 8 && t->rsqrt_soft < kSoftAlternate) || t->rsqrt_soft > kSoftAlternate + 7)
         return set_error(COUL_ERR_INVALID_ARGUMENT, "rsqrt_soft must be in 0..8 or 10..17");
-    if (t->split_form != 0 && t->split_form != 1)
-        return set_error(COUL_ERR_INVALID_ARGUMENT, "split_form must be 0 (cluster) or 1 (queue)");
-    const int max_split = t->split_form ? kMaxQueueSplit : kMaxSplit;
+    if (t->split_form < 0 || t->split_form > 2)
+        return set_error(COUL_ERR_INVALID_ARGUMENT, "split_form must be 0 (cluster), 1 (queue) or 2 (balanced)");
+    const int max_split = t->split_form == 2 ? kBalMaxGroups : t->split_form == 1 ? kMaxQueueSplit : kMaxSplit;
     if (t->atom_split < 0 || t->atom_split > max_split)
         return set_error(COUL_ERR_INVALID_ARGUMENT, "atom_split must be in 0.." + std::to_string(max_split));
-    const int split = t->atom_split >= 2 ? (t->split_form ? 2 : 1) : 0;
+    const int split = t->atom_split >= 2 ? t->split_form + 1 : 0;
+    if (split == 3 && threads * t->atom_split > kBalThreads)
+        return set_error(COUL_ERR_DEVICE_LIMITS, "the balanced form's block (tile threads x atom groups) is limited to " +
+                                                     std::to_string(kBalThreads) + " threads");
     if (split && (t->atom_source != COUL_ATOMS_SHARED_TMA || soa || t->precision != COUL_PREC_FP32))
         return set_error(COUL_ERR_UNSUPPORTED,
                          "the atom-split form streams float4 atoms through shared memory with FP32 accumulation");
@@ -284,12 +288,101 @@ int validate_grid(const coul_grid* g)
     return COUL_OK;
 }
 
-// Device memory of the queue form, kept in the context and grown on demand: the partial blocks of
-// every (tile, chunk) item, one counter per tile and the queue head.
+// Device memory of the queue and balanced forms of the atom split, kept in the context and grown on
+// demand: partial blocks and counters (the layout is each form's own).
 struct QueueWorkspace {
     void* mem = nullptr;
     size_t bytes = 0;
+    // The balanced form's counters (at the start of the memory, one per CTA) are known to be zero for
+    // this many CTAs (0: unknown).  Its kernel leaves them at zero when it completes, so a following
+    // launch of the same grid needs no reset; the queue form's use of the memory, a reallocation or
+    // a timed-out kernel clears this.
+    int64_t balanced_clean_ctas = 0;
 };
+
+// Grow the context's split workspace to `need` bytes (drains the stream before freeing the old one).
+static int split_workspace(coul_ctx* ctx, size_t need, unsigned char** base)
+{
+    auto* ws = static_cast<QueueWorkspace*>(ctx->queue_workspace);
+    if (ws == nullptr) {
+        ws = new QueueWorkspace();
+        ctx->queue_workspace = ws;
+        ctx->cleanups.push_back([ws] {
+            if (ws->mem)
+                cudaFree(ws->mem);
+            delete ws;
+        });
+    }
+    if (need > ws->bytes) {
+        ws->balanced_clean_ctas = 0;
+        if (ws->mem) {
+            cudaStreamSynchronize(ctx->stream);
+            cudaFree(ws->mem);
+            ws->mem = nullptr;
+            ws->bytes = 0;
+        }
+        cudaError_t e;
+        if ((e = cudaMalloc(&ws->mem, need)) != cudaSuccess)
+            return set_error(COUL_ERR_OUT_OF_MEMORY, std::string("atom-split workspace: ") + cudaGetErrorString(e));
+        ws->bytes = need;
+    }
+    *base = static_cast<unsigned char*>(ws->mem);
+    return COUL_OK;
+}
+
+// The balanced form's resident grid, block (tile threads x atom groups), shared memory and zeroed
+// counters (reset on the context's stream only when they are not known to be zero).  One counter
+// and two partial-block slots per CTA.
+int balanced_split_setup(coul_ctx* ctx, const VariantEntry* v, FwdLaunch& L, const coul_tune* t)
+{
+    const int groups = t->atom_split;
+    const int tile_threads = t->block_x * t->block_y;
+    const int threads = tile_threads * groups;
+    const int64_t tiles = static_cast<int64_t>(L.grid.x) * L.grid.y * L.grid.z;
+    if (tiles > 2147483647LL || L.p.n_atoms > 2147483647LL)
+        return set_error(COUL_ERR_DEVICE_LIMITS, "the balanced form takes fewer than 2^31 point tiles and atoms");
+    const int64_t values = static_cast<int64_t>(tile_threads) * t->z_iterations * t->x_points;
+    L.block.z = static_cast<unsigned>(groups);
+    L.split = groups;
+    L.smem = static_cast<size_t>(kStages) * kBalStageAtoms * 16 + kStages * 8 +
+             static_cast<size_t>(groups * values) * sizeof(float);
+    cudaError_t e;
+    if ((e = cudaFuncSetAttribute(v->occupancy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(L.smem))) != cudaSuccess)
+        return cuda_error(e, "balanced form shared memory");
+    int blocks_per_sm = 0;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, v->occupancy_kernel, threads, L.smem)) !=
+        cudaSuccess)
+        return cuda_error(e, "occupancy query");
+    if (blocks_per_sm < 1)
+        return set_error(COUL_ERR_DEVICE_LIMITS, "the balanced form's block does not fit on an SM");
+    // every CTA resident, at least one unit each
+    const int64_t units = tiles * L.p.n_atoms;
+    int64_t ctas = static_cast<int64_t>(blocks_per_sm) * ctx->sm_count;
+    const int64_t cap = units > 0 ? units : tiles;
+    if (ctas > cap)
+        ctas = cap;
+    // the counters first, so that their place depends on the grid alone
+    const size_t done_bytes = static_cast<size_t>(ctas) * sizeof(unsigned);
+    const size_t partial_offset = (done_bytes + 255) / 256 * 256;
+    const size_t need = partial_offset + static_cast<size_t>(2 * ctas * values) * sizeof(float);
+    unsigned char* base = nullptr;
+    const int rc = split_workspace(ctx, need, &base);
+    if (rc != COUL_OK)
+        return rc;
+    auto* ws = static_cast<QueueWorkspace*>(ctx->queue_workspace);
+    if (ws->balanced_clean_ctas != ctas) {
+        if ((e = cudaMemsetAsync(base, 0, done_bytes, ctx->stream)) != cudaSuccess)
+            return cuda_error(e, "balanced form counters reset");
+        ws->balanced_clean_ctas = ctas;
+    }
+    L.queue.partial = reinterpret_cast<float*>(base + partial_offset);
+    L.queue.tile_done = reinterpret_cast<unsigned*>(base);
+    L.queue.counter = nullptr;
+    L.queue.chunks = 2;
+    L.queue.ctas = static_cast<int>(ctas);
+    return COUL_OK;
+}
 
 // The queue form's persistent grid and zeroed counters, enqueued on the context's stream.
 int queue_split_setup(coul_ctx* ctx, const VariantEntry* v, FwdLaunch& L, const coul_tune* t)
@@ -301,29 +394,12 @@ int queue_split_setup(coul_ctx* ctx, const VariantEntry* v, FwdLaunch& L, const 
     const size_t done_offset = (partial_bytes + 255) / 256 * 256;
     const size_t counter_offset = (done_offset + static_cast<size_t>(tiles) * sizeof(unsigned) + 255) / 256 * 256;
     const size_t need = counter_offset + 256;
-    auto* ws = static_cast<QueueWorkspace*>(ctx->queue_workspace);
-    if (ws == nullptr) {
-        ws = new QueueWorkspace();
-        ctx->queue_workspace = ws;
-        ctx->cleanups.push_back([ws] {
-            if (ws->mem)
-                cudaFree(ws->mem);
-            delete ws;
-        });
-    }
+    unsigned char* base = nullptr;
+    const int rc = split_workspace(ctx, need, &base);
+    if (rc != COUL_OK)
+        return rc;
+    static_cast<QueueWorkspace*>(ctx->queue_workspace)->balanced_clean_ctas = 0;
     cudaError_t e;
-    if (need > ws->bytes) {
-        if (ws->mem) {
-            cudaStreamSynchronize(ctx->stream);
-            cudaFree(ws->mem);
-            ws->mem = nullptr;
-            ws->bytes = 0;
-        }
-        if ((e = cudaMalloc(&ws->mem, need)) != cudaSuccess)
-            return set_error(COUL_ERR_OUT_OF_MEMORY, std::string("atom-split queue workspace: ") + cudaGetErrorString(e));
-        ws->bytes = need;
-    }
-    auto* base = static_cast<unsigned char*>(ws->mem);
     // the per-tile counters and the queue head start every launch at zero
     if ((e = cudaMemsetAsync(base + done_offset, 0, need - done_offset, ctx->stream)) != cudaSuccess)
         return cuda_error(e, "queue counters reset");
@@ -374,6 +450,10 @@ int launch_forward(coul_ctx* ctx, const VariantEntry* v, const FwdParams& prm, i
     } else if (v->key.split == 2) {
         L.split = t->atom_split;
         const int rc = queue_split_setup(ctx, v, L, t);
+        if (rc != COUL_OK)
+            return rc;
+    } else if (v->key.split == 3) {
+        const int rc = balanced_split_setup(ctx, v, L, t);
         if (rc != COUL_OK)
             return rc;
     }
@@ -606,6 +686,8 @@ COUL_API int coul_synchronize(coul_ctx* ctx)
         return cuda_error(e, "status read-back");
     if (status != kStatusOk) {
         cudaMemset(ctx->d_status, 0, sizeof(int));
+        if (ctx->queue_workspace)  // a kernel that gave up may have left counters behind
+            static_cast<QueueWorkspace*>(ctx->queue_workspace)->balanced_clean_ctas = 0;
         return set_error(COUL_ERR_TIMEOUT, "a kernel gave up on a bounded wait (status " + std::to_string(status) +
                                                "); its output is invalid");
     }
@@ -664,7 +746,7 @@ COUL_API int coul_variant_get(int i, coul_tune* t, int* is_2d, int* is_soa)
     t->precision = k.prec;
     t->rsqrt_soft = k.soft;
     t->atom_split = k.split ? 2 : 0;
-    t->split_form = k.split == 2 ? 1 : 0;
+    t->split_form = k.split ? k.split - 1 : 0;
     if (is_2d)
         *is_2d = k.mode == kModeSlice2d ? 1 : 0;
     if (is_soa)

@@ -62,6 +62,26 @@ __device__ __forceinline__ void eval_atom(const float (&gx)[XP], float gy, const
         pair_block_2d<XP, ZH, ZA, SOFT, PHASE, HALF>(gx, gb, a, dst);
 }
 
+// A thread's blocked-axis points in lane pairs: (z0 + 2i, z0 + 2i + 1) in 3D (gy = the row's y),
+// rows (yrow + 2i, yrow + 2i + 1) in 2D (gy unused).
+template <int ZH, int MODE>
+__device__ __forceinline__ void blocked_coords(const FwdParams& p, const int yrow, const int z0, float& gy,
+                                               float2 (&gb)[ZH])
+{
+    if constexpr (MODE == kModeGrid3d) {
+        gy = fmaf(static_cast<float>(yrow), p.h, p.oy);
+#pragma unroll
+        for (int i = 0; i < ZH; ++i)
+            gb[i] = make_float2(fmaf(static_cast<float>(z0 + 2 * i), p.h, p.oz),
+                                fmaf(static_cast<float>(z0 + 2 * i + 1), p.h, p.oz));
+    } else {
+        gy = 0.0f;
+#pragma unroll
+        for (int i = 0; i < ZH; ++i)
+            gb[i] = make_float2(fmaf(static_cast<float>(yrow + 2 * i), p.h, p.oy),
+                                fmaf(static_cast<float>(yrow + 2 * i + 1), p.h, p.oy));
+    }
+}
 
 __device__ __forceinline__ float lane(const float2& v, int l) { return l == 0 ? v.x : v.y; }
 
@@ -144,26 +164,14 @@ __device__ __forceinline__ bool tile_accumulate(const FwdParams& p, const int x0
 #pragma unroll
     for (int k = 0; k < XP; ++k)
         gx[k] = fmaf(static_cast<float>(x0 + k), p.h, p.ox);
-    // Blocked-axis points in lane pairs: (z0 + 2i, z0 + 2i + 1) in 3D, rows in 2D.  With an odd ZI
-    // the last pair holds one point (HALF), evaluated on its own.
+    // Blocked-axis points in lane pairs (blocked_coords).  With an odd ZI the last pair holds one
+    // point (HALF), evaluated on its own.
     constexpr int ZH = (ZI + 1) / 2;
     constexpr bool HALF = (ZI & 1) != 0;
     constexpr int P = soft_phases(SOFT, XP * ZH);  // stage phases of the FMA-pipe share's pattern
     float2 gb[ZH];
     float gy;
-    if constexpr (MODE == kModeGrid3d) {
-        gy = fmaf(static_cast<float>(yrow), p.h, p.oy);
-#pragma unroll
-        for (int i = 0; i < ZH; ++i)
-            gb[i] = make_float2(fmaf(static_cast<float>(z0 + 2 * i), p.h, p.oz),
-                                fmaf(static_cast<float>(z0 + 2 * i + 1), p.h, p.oz));
-    } else {
-        gy = 0.0f;
-#pragma unroll
-        for (int i = 0; i < ZH; ++i)
-            gb[i] = make_float2(fmaf(static_cast<float>(yrow + 2 * i), p.h, p.oy),
-                                fmaf(static_cast<float>(yrow + 2 * i + 1), p.h, p.oy));
-    }
+    blocked_coords<ZH, MODE>(p, yrow, z0, gy, gb);
 
     float2 acc[XP][ZH];
     float2 part[XP][ZH];
@@ -283,10 +291,13 @@ __device__ __forceinline__ bool tile_accumulate(const FwdParams& p, const int x0
             const uint32_t parity = static_cast<uint32_t>((g / kStages) & 1);
             const bool ok = mbar_wait_bounded(&full[buf], parity);
             const int cnt = stage_count(s);
+            // atoms the stage evaluates: a ragged last stage rounds up to whole sub-tiles only
+            const int ntr = cnt < kTileAtoms ? (cnt + kSubTile - 1) / kSubTile * kSubTile : kTileAtoms;
             unsigned char* tile = tiles + buf * kTileAtoms * 16;
             if (ok && cnt < kTileAtoms) {
                 // Ragged last stage: the SoA remainder (< 4 atoms) by plain loads, then padding atoms
-                // far away with zero charge so the unrolled loop below needs no bound.
+                // far away with zero charge up to the next whole sub-tile, so the unrolled sub-tile
+                // loops below need no bound.
                 if constexpr (SOA == 1) {
                     const int cnt4 = cnt & ~3;
                     for (int j = cnt4 + tid; j < cnt; j += nthreads) {
@@ -297,7 +308,7 @@ __device__ __forceinline__ bool tile_accumulate(const FwdParams& p, const int x0
                         reinterpret_cast<float*>(tile)[3 * kTileAtoms + j] = p.sq[g];
                     }
                 }
-                for (int j = cnt + tid; j < kTileAtoms; j += nthreads) {
+                for (int j = cnt + tid; j < ntr; j += nthreads) {
                     if constexpr (SOA == 0) {
                         reinterpret_cast<float4*>(tile)[j] = make_float4(kPadCoord, kPadCoord, kPadCoord, 0.0f);
                     } else {
@@ -329,12 +340,14 @@ __device__ __forceinline__ bool tile_accumulate(const FwdParams& p, const int x0
                     return make_float4(f[j], f[kTileAtoms + j], f[2 * kTileAtoms + j], f[3 * kTileAtoms + j]);
                 }
             };
-            // the stage is padded to kTileAtoms atoms; the whole stage is one phase of the FMA-pipe
-            // share's pattern
+            // the stage runs in whole sub-tiles of kSubTile atoms (ntr of them: all kTileAtoms, or the
+            // ragged last stage rounded up); the whole stage is one phase of the FMA-pipe share's pattern
             if constexpr (PREC == kPrecFp64Pairs) {
+                for (int j0 = 0; j0 < ntr; j0 += kSubTile) {
 #pragma unroll UNR
-                for (int j = 0; j < kTileAtoms; ++j)
-                    pair_block_3d_f64<XP, ZI>(gxd, gyd, gzd, atom_at(j), accd);
+                    for (int j = 0; j < kSubTile; ++j)
+                        pair_block_3d_f64<XP, ZI>(gxd, gyd, gzd, atom_at(j0 + j), accd);
+                }
             } else {
                 // G: the stage's phase of the FMA-pipe share; LA: the z points the tile evaluates
                 auto stage = [&](auto phase, auto lanes) {
@@ -343,11 +356,13 @@ __device__ __forceinline__ bool tile_accumulate(const FwdParams& p, const int x0
                     constexpr int ZA = (LA + 1) / 2;
                     constexpr bool HA = (LA & 1) != 0;
                     if constexpr (PREC == kPrecFp32) {
+                        for (int j0 = 0; j0 < ntr; j0 += kSubTile) {
 #pragma unroll UNR
-                        for (int j = 0; j < kTileAtoms; ++j)
-                            eval_atom<MODE, XP, ZH, SOFT, G, HA, ZA>(gx, gy, gb, atom_at(j), acc);
+                            for (int j = 0; j < kSubTile; ++j)
+                                eval_atom<MODE, XP, ZH, SOFT, G, HA, ZA>(gx, gy, gb, atom_at(j0 + j), acc);
+                        }
                     } else {
-                        for (int j0 = 0; j0 < kTileAtoms; j0 += kSubTile) {
+                        for (int j0 = 0; j0 < ntr; j0 += kSubTile) {
                             clear_part();
 #pragma unroll UNR
                             for (int j = 0; j < kSubTile; ++j)
@@ -487,8 +502,9 @@ __device__ __forceinline__ void store_value(const FwdParams& p, const int tile_x
 
 // Atom-split form for maps with too few points to fill the GPU one tile per CTA (a 2D slice, a
 // small 3D map): a thread-block cluster of S CTAs shares one point tile, CTA rank r takes the r-th
-// of S contiguous atom ranges through its own TMA ring, and rank 0 sums the S partial blocks from
-// the peers' shared memory in rank order (deterministic) and stores them.  The cluster size is a
+// of S contiguous atom ranges through its own TMA ring, and the ranks reduce-scatter the S partial
+// blocks over distributed shared memory (rank r sums the r-th slice of the points, every rank's
+// value added in rank order: deterministic) and store them.  The cluster size is a
 // launch-time choice (2..8 portable, up to 16 with the B200's non-portable cluster sizes); plain FP32
 // accumulation, AoS atoms.
 template <int ZI, int XP, int UNR, int SOFT, int MODE>
@@ -663,12 +679,273 @@ __global__ void __launch_bounds__(kMaxThreads) queue_split_kernel(const FwdParam
     }
 }
 
+// Balanced form of the atom split: the work of a small map is the space of (point tile, atom)
+// units, T tiles x N atoms, and CTA b of a resident grid of B takes the b-th of B contiguous,
+// equal ranges of it (to one unit), so every SM does the same number of pairs.  A CTA's range
+// crosses tile boundaries: it is a sequence of pieces (one tile, a contiguous atom range), streamed
+// through the CTA's TMA ring in stages of kBalStageAtoms atoms; the ring runs on from one piece to
+// the next.  Inside the CTA, blockDim.z groups of the tile's thread layout share the piece's
+// points and split every stage's atoms between them; at the end of a piece the groups' partial
+// blocks are added in group order in shared memory.  A piece that covers its tile's atoms is stored;
+// the pieces of a tile split between CTAs go to device memory, each CTA counts its split pieces when
+// it ends (a counter per split tile), and the CTA that counts a tile's last piece adds the tile's
+// pieces in CTA order, stores it and zeroes the counter for the next launch: deterministic for a
+// given grid, and no CTA waits on another.
+// A CTA of up to kBalThreads threads fills an SM by itself (64 registers a thread): its warps meet at
+// every stage, so they progress together -- where two CTAs share an SM, the warp schedulers let one
+// run ahead and the other finishes alone at half the occupancy.
+constexpr int kBalStageAtoms = 4096;  // atoms per stage of the balanced form's ring (at most)
+constexpr int kBalFirstAtoms = 1024;  // atoms in a CTA's first stage: the SM starts work sooner
+constexpr int kBalThreads = 1024;     // launch bound of the balanced form (tile threads x groups)
+constexpr int kBalMaxGroups = 32;     // atom groups per CTA
+constexpr int kBalAtomStep = 8;       // a group's atoms are evaluated in steps of this many
+
+// The balanced form's split of the T x N unit space over B CTAs: q = U / B units per CTA, the first
+// r = U % B CTAs one more.  start(b) = b q + min(b, r); cta_of(u) inverts it.
+struct BalanceSplit {
+    int64_t n, q, r;
+    __host__ __device__ int64_t start(int64_t b) const { return b * q + (b < r ? b : r); }
+    __host__ __device__ int64_t cta_of(int64_t u) const
+    {
+        const int64_t big = r * (q + 1);
+        return u < big ? u / (q + 1) : r + (u - big) / q;
+    }
+};
+
+template <int ZI, int XP, int UNR, int SOFT, int MODE>
+__global__ void __launch_bounds__(kBalThreads, 1) balanced_split_kernel(const FwdParams p, const SplitQueue sq,
+                                                                     const int tiles_x, const int tiles_y,
+                                                                     const int tiles)
+{
+    constexpr int ZH = (ZI + 1) / 2;
+    constexpr bool HALF = (ZI & 1) != 0;
+    constexpr int P = soft_phases(SOFT, XP * ZH);
+    static_assert(kBalStageAtoms % kBalAtomStep == 0, "steps must divide the stage");
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const float4* ring = reinterpret_cast<const float4*>(smem_raw);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + kStages * kBalStageAtoms * 16);
+    float* red = reinterpret_cast<float*>(smem_raw + kStages * kBalStageAtoms * 16 + kStages * 8);
+    __shared__ int s_last;
+    __shared__ int s_issue_t, s_issue_a;  // the producer's cursor: the next stage's tile and first atom
+    __shared__ unsigned s_issued;         // stages issued so far
+
+    const int tile_threads = static_cast<int>(blockDim.x * blockDim.y);
+    const int groups = static_cast<int>(blockDim.z);
+    const int grp = static_cast<int>(threadIdx.z);
+    const int ttid = static_cast<int>(threadIdx.y * blockDim.x + threadIdx.x);
+    const int tid = grp * tile_threads + ttid;
+    const int nthreads = tile_threads * groups;
+    const int values = tile_threads * XP * ZI;
+    const int N = static_cast<int>(p.n_atoms);  // the host keeps tiles x atoms below 2^62 and atoms below 2^31
+
+    // tile t's origin for this thread
+    auto locate = [&](int t, int& tile_x, int& tile_y, int& x0, int& yrow, int& z0) {
+        tile_x = t % tiles_x;
+        tile_y = (t / tiles_x) % tiles_y;
+        const int tile_z = t / (tiles_x * tiles_y);
+        x0 = (tile_x * static_cast<int>(blockDim.x) + static_cast<int>(threadIdx.x)) * XP;
+        if constexpr (MODE == kModeGrid3d) {
+            yrow = tile_y * static_cast<int>(blockDim.y) + static_cast<int>(threadIdx.y);
+            z0 = p.z_base + tile_z * ZI;
+        } else {
+            yrow = (tile_y * static_cast<int>(blockDim.y) + static_cast<int>(threadIdx.y)) * ZI;
+            z0 = 0;
+        }
+    };
+
+    if (N == 0) {  // no units: the tiles' potentials are zero
+        for (int t = static_cast<int>(blockIdx.x); t < tiles; t += static_cast<int>(gridDim.x)) {
+            int tile_x, tile_y, x0, yrow, z0;
+            locate(t, tile_x, tile_y, x0, yrow, z0);
+            for (int v = tid; v < values; v += nthreads)
+                store_value<ZI, XP, MODE>(p, tile_x, tile_y, z0, v, 0.0f);
+        }
+        return;
+    }
+
+    // This CTA's units [u_begin, u_end): from atom a_begin of tile t_begin to atom a_stop - 1 of tile
+    // t_end.  Its pieces: tile t_begin from a_begin, the tiles between whole, tile t_end up to a_stop.
+    const int64_t b = blockIdx.x;
+    const BalanceSplit split{N, static_cast<int64_t>(tiles) * N / gridDim.x, static_cast<int64_t>(tiles) * N % gridDim.x};
+    const int64_t u_begin = split.start(b);
+    const int64_t u_last = split.start(b + 1) - 1;
+    const int t_begin = static_cast<int>(u_begin / N);
+    const int a_begin = static_cast<int>(u_begin - static_cast<int64_t>(t_begin) * N);
+    const int t_end = static_cast<int>(u_last / N);
+    const int a_stop = static_cast<int>(u_last - static_cast<int64_t>(t_end) * N) + 1;
+    // the stage at (tile t, atom a): its atom count (a stage never leaves its piece)
+    auto stage_count = [&](int t, int a) -> int {
+        const int pe = t == t_end ? a_stop : N;
+        const int cap = t == t_begin && a == a_begin ? kBalFirstAtoms : kBalStageAtoms;
+        return pe - a < cap ? pe - a : cap;
+    };
+
+    // the producer (thread 0) keeps its cursor in shared memory, off the other threads' registers
+    auto issue = [&]() {
+        const int t = s_issue_t;
+        const int a = s_issue_a;
+        const int cnt = stage_count(t, a);
+        const int buf = static_cast<int>(s_issued % kStages);
+        const uint32_t bytes = static_cast<uint32_t>(cnt) * 16u;
+        mbar_arrive_expect_tx(&full[buf], bytes);
+        bulk_copy_g2s(smem_raw + buf * kBalStageAtoms * 16, p.atoms + a, bytes, &full[buf]);
+        const bool piece_end = a + cnt == (t == t_end ? a_stop : N);
+        s_issue_t = piece_end ? t + 1 : t;
+        s_issue_a = piece_end ? 0 : a + cnt;
+        s_issued += 1u;
+    };
+    if (tid == 0) {
+        s_issue_t = t_begin;
+        s_issue_a = a_begin;
+        s_issued = 0u;
+    }
+    ring_init(full, tid);
+    if (tid == 0)
+        while (s_issued < static_cast<uint32_t>(kStages) && s_issue_t <= t_end)
+            issue();
+
+    float gx[XP];
+    float gy = 0.0f;
+    float2 gb[ZH];
+    float2 acc[XP][ZH];
+    int tile_x = 0, tile_y = 0, x0 = 0, yrow = 0, z0 = 0;
+    uint32_t k = 0;
+    for (int t = t_begin, a = a_begin; t <= t_end; ++k) {
+        const int cnt = stage_count(t, a);
+        const int piece_first = t == t_begin ? a_begin : 0;
+        if (a == piece_first) {  // a new piece: this thread's points of tile t, zero partials
+            locate(t, tile_x, tile_y, x0, yrow, z0);
+#pragma unroll
+            for (int i = 0; i < XP; ++i)
+                gx[i] = fmaf(static_cast<float>(x0 + i), p.h, p.ox);
+            blocked_coords<ZH, MODE>(p, yrow, z0, gy, gb);
+#pragma unroll
+            for (int i = 0; i < XP; ++i)
+#pragma unroll
+                for (int j = 0; j < ZH; ++j)
+                    acc[i][j] = make_float2(0.0f, 0.0f);
+        }
+        const int buf = static_cast<int>(k % kStages);
+        const bool ok = mbar_wait_bounded(&full[buf], (k / kStages) & 1u);
+        // a ragged stage: zero-charge padding atoms up to the next whole step
+        const int cnt_step = (cnt + kBalAtomStep - 1) / kBalAtomStep * kBalAtomStep;
+        if (ok)
+            for (int j = cnt + tid; j < cnt_step; j += nthreads)
+                reinterpret_cast<float4*>(smem_raw)[buf * kBalStageAtoms + j] =
+                    make_float4(kPadCoord, kPadCoord, kPadCoord, 0.0f);
+        if (__syncthreads_or(ok ? 0 : 1)) {
+            // a copy never completed: record it, drain what may still be in flight (bounded), leave
+            if (tid == 0) {
+                report_status(p.status, kStatusTimeout);
+                for (uint32_t r = k; r < s_issued; ++r)
+                    (void)mbar_wait_bounded(&full[r % kStages], (r / kStages) & 1u);
+            }
+            return;
+        }
+        // group grp's share of the stage: `per` atoms (a whole number of steps) from grp * per
+        const int per = ((cnt + groups - 1) / groups + kBalAtomStep - 1) / kBalAtomStep * kBalAtomStep;
+        const int j_begin = grp * per;
+        const int j_count = cnt - j_begin < per ? cnt - j_begin : per;
+        if (j_count > 0) {
+            const int j_end = j_begin + (j_count + kBalAtomStep - 1) / kBalAtomStep * kBalAtomStep;
+            const float4* tile = ring + buf * kBalStageAtoms;
+            // the stage and the group select the phase of the FMA-pipe share (as in the other forms,
+            // one form per lane pair for a contiguous run of atoms)
+            with_phase<P>(static_cast<int>((k + static_cast<uint32_t>(grp)) % P), [&](auto phase) {
+                constexpr int G = decltype(phase)::value;
+                for (int j0 = j_begin; j0 < j_end; j0 += kBalAtomStep) {
+#pragma unroll UNR
+                    for (int j = 0; j < kBalAtomStep; ++j)
+                        eval_atom<MODE, XP, ZH, SOFT, G, HALF>(gx, gy, gb, tile[j0 + j], acc);
+                }
+            });
+        }
+        fence_proxy_async_smem();
+        __syncthreads();
+        if (tid == 0 && s_issue_t <= t_end)
+            issue();
+        a += cnt;
+        const int piece_stop = t == t_end ? a_stop : N;
+        if (a == piece_stop) {
+            // the piece ends: add the groups' partial blocks in group order
+#pragma unroll
+            for (int i = 0; i < XP; ++i)
+#pragma unroll
+                for (int m = 0; m < ZI; ++m)
+                    red[(grp * XP * ZI + i * ZI + m) * tile_threads + ttid] = lane(acc[i][m / 2], m & 1);
+            __syncthreads();
+            // A split tile's pieces: CTA c's first piece when c starts inside the tile, else its last
+            // one; two partial-block slots per CTA.  Only a CTA's first and last pieces can be split;
+            // they are counted when the CTA ends.
+            const bool whole = piece_first == 0 && piece_stop == N;
+            float* slot = sq.partial + (2 * b + (t == t_begin ? 0 : 1)) * values;
+            for (int v = tid; v < values; v += nthreads) {
+                float sum = red[v];
+#pragma unroll 8
+                for (int g2 = 1; g2 < groups; ++g2)
+                    sum += red[g2 * values + v];
+                if (whole)
+                    store_value<ZI, XP, MODE>(p, tile_x, tile_y, z0, v, sum);
+                else
+                    slot[v] = sum;
+            }
+            __syncthreads();  // red is free for the next piece
+            ++t;
+            a = 0;
+        }
+    }
+
+    // Count this CTA's split pieces (after all its partial blocks are written) and finish the tiles
+    // whose last piece it added.  The counting thread releases the CTA's writes before its count and
+    // acquires the other CTAs' after it; the barriers order the CTA's threads against it.
+    const bool first_split = a_begin > 0 || (t_begin == t_end && a_stop < N);
+    const bool last_split = t_end != t_begin && a_stop < N;
+    if (first_split || last_split) {
+        if (tid == 0)
+            s_last = 0;
+        __syncthreads();
+        // lane 0 of warp i counts the CTA's first (i = 0) or last (i = 1) split piece
+        const int i = tid / 32;
+        if (tid % 32 == 0 && i < 2 && (i == 0 ? first_split : last_split)) {
+            __threadfence();
+            const int64_t t = i == 0 ? t_begin : t_end;
+            const int64_t first = split.cta_of(t * N);
+            const int64_t last = split.cta_of((t + 1) * N - 1);
+            if (atomicAdd(&sq.tile_done[first], 1u) == static_cast<unsigned>(last - first)) {
+                __threadfence();
+                atomicOr(&s_last, 1 << i);
+            }
+        }
+        __syncthreads();
+        const int mask = s_last;
+        for (int i = 0; i < 2; ++i) {
+            if (!(mask & (1 << i)))
+                continue;
+            const int t = i == 0 ? t_begin : t_end;
+            const int64_t t0 = static_cast<int64_t>(t) * N;
+            const int64_t first = split.cta_of(t0);
+            const int64_t last = split.cta_of(t0 + N - 1);
+            locate(t, tile_x, tile_y, x0, yrow, z0);
+            for (int v = tid; v < values; v += nthreads) {
+                float sum = 0.0f;
+                for (int64_t c = first; c <= last; ++c) {
+                    const float part = __ldcg(sq.partial + (2 * c + (split.start(c) >= t0 ? 0 : 1)) * values + v);
+                    sum = c == first ? part : sum + part;
+                }
+                store_value<ZI, XP, MODE>(p, tile_x, tile_y, z0, v, sum);
+            }
+            if (tid == 0)
+                sq.tile_done[first] = 0u;  // every piece is counted: zero for the next launch
+        }
+    }
+}
+
 // ------------------------------------------------------------------------------------------
 // Launchers and the variant registry
 // ------------------------------------------------------------------------------------------
 struct VariantKey {
     int zi, xp, unroll, src, soa, prec, soft, mode;
-    int split;  // 1 for the atom-split cluster form, 2 for its queue form
+    int split;  // 1 for the atom-split cluster form, 2 for its queue form, 3 for its balanced form
     bool operator==(const VariantKey& o) const
     {
         return zi == o.zi && xp == o.xp && unroll == o.unroll && src == o.src && soa == o.soa && prec == o.prec &&
@@ -794,6 +1071,26 @@ void add_queue_split_variant(std::vector<VariantEntry>& v)
                              reinterpret_cast<const void*>(&queue_split_kernel<ZI, XP, UNR, SOFT, MODE>)});
 }
 
+// Persistent launch of the balanced form: L.queue holds the counters (zero) and the pieces' partial
+// blocks, L.grid the point tiles, L.block.z the atom groups, L.queue.ctas the resident grid.
+template <int ZI, int XP, int UNR, int SOFT, int MODE>
+cudaError_t launch_balanced_split(const FwdLaunch& L, cudaStream_t stream)
+{
+    auto kernel = balanced_split_kernel<ZI, XP, UNR, SOFT, MODE>;
+    const int tiles = static_cast<int>(L.grid.x * L.grid.y * L.grid.z);  // checked below 2^31 by the setup
+    kernel<<<dim3(static_cast<unsigned>(L.queue.ctas)), L.block, L.smem, stream>>>(
+        L.p, L.queue, static_cast<int>(L.grid.x), static_cast<int>(L.grid.y), tiles);
+    return cudaGetLastError();
+}
+
+template <int ZI, int XP, int UNR, int SOFT, int MODE>
+void add_balanced_split_variant(std::vector<VariantEntry>& v)
+{
+    v.push_back(VariantEntry{VariantKey{ZI, XP, UNR, kSrcShared, 0, kPrecFp32, SOFT, MODE, 3},
+                             &launch_balanced_split<ZI, XP, UNR, SOFT, MODE>, 0,
+                             reinterpret_cast<const void*>(&balanced_split_kernel<ZI, XP, UNR, SOFT, MODE>)});
+}
+
 template <int ZI, int XP, int UNR, int SOFT, int MODE>
 void add_split_variant(std::vector<VariantEntry>& v)
 {
@@ -824,5 +1121,6 @@ void register_fwd_3d_fp64(std::vector<VariantEntry>& v);
 void register_fwd_2d(std::vector<VariantEntry>& v);
 void register_fwd_split(std::vector<VariantEntry>& v);
 void register_fwd_queue_split(std::vector<VariantEntry>& v);
+void register_fwd_balanced_split(std::vector<VariantEntry>& v);
 
 }  // namespace coul

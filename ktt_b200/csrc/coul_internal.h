@@ -43,5 +43,6 @@ int validate_tune(const coul_tune* t, int mode, int soa, const VariantEntry** ou
 int validate_grid(const coul_grid* g);
 int launch_forward(coul_ctx* ctx, const VariantEntry* v, const FwdParams& prm, int mode, const coul_tune* t);
 int queue_split_setup(coul_ctx* ctx, const VariantEntry* v, FwdLaunch& L, const coul_tune* t);
+int balanced_split_setup(coul_ctx* ctx, const VariantEntry* v, FwdLaunch& L, const coul_tune* t);
 
 }  // namespace coul

@@ -5,8 +5,9 @@
 Atoms x, y ~ U[0, 128), z ~ U[0, 32), q ~ U[-1, 1]; the slice at z = 16 A.  For each compiled 2D
 tile shape: device time of the slice kernel (median of --repeat event-timed launches), pair rate,
 error against the FP64 oracle over the whole slice.  Shapes include the atom-split form (a cluster
-of 2 .. 16 CTAs per point tile, each streaming a share of the atoms, or its queue form, a persistent
-grid over (tile, atom chunk) items) and 2/8 or 3/8 of the rsqrts on the FMA pipe.  Then the whole call as a KTT user makes it (host atoms in, dz^2 slicing on the device,
+of 2 .. 16 CTAs per point tile, each streaming a share of the atoms; its queue form, a persistent
+grid over (tile, atom chunk) items; its balanced form, equal ranges of the (tile, atom) space per
+resident CTA) and 2/8 or 3/8 of the rsqrts on the FMA pipe.  Then the whole call as a KTT user makes it (host atoms in, dz^2 slicing on the device,
 host slice out; wall clock, median) for the fastest shape, and the FP64 oracle's own time on the
 host.  One JSON line per measurement.
 """
@@ -23,15 +24,20 @@ SHAPES = [(bx, by, xp, yi, split, soft, 0) for (bx, by) in ((32, 4), (32, 2), (6
 # the queue form of the atom split (split_form 1): chunk counts beyond a cluster's 16 as well
 SHAPES += [(bx, by, xp, yi, split, soft, 1) for (bx, by) in ((32, 4), (16, 8), (64, 2), (32, 8), (64, 4))
            for xp in (1, 2, 4) for yi in (2, 4, 8) for split in (8, 16, 24, 32, 48, 64) for soft in (0, 2, 3)]
+# the balanced form (split_form 2): the tile's thread layout x atom groups per CTA (at most 1024 threads)
+SHAPES += [(bx, by, xp, yi, groups, soft, 2, unroll) for (bx, by) in ((32, 1), (64, 1), (32, 2), (16, 2))
+           for xp in (1, 2, 4) for yi in (2, 4, 8) for groups in (4, 8, 16, 32) for soft in (0, 2, 3, 12)
+           for unroll in (1, 2) if 256 <= bx * by * groups <= 1024]
 
 
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--repeat", type=int, default=50)
     ap.add_argument("--only", default="", help="one configuration: block x, block y, x points, rows, atom split, "
-                                               "rsqrt share[, split form] (for profiling)")
+                                               "rsqrt share[, split form[, unroll]] (for profiling)")
     args = ap.parse_args()
-    shapes = [(tuple(int(v) for v in args.only.split(",")) + (0,))[:7]] if args.only else SHAPES
+    shapes = [(tuple(int(v) for v in args.only.split(",")) + (0, 1)[len(args.only.split(",")) - 6:])[:8]] \
+        if args.only else SHAPES
 
     import torch
 
@@ -51,9 +57,9 @@ def main() -> None:
     d_sliced = ctx.slice_atoms(atoms, case.z_slice)
     out = torch.empty((ny, nx), dtype=torch.float32, device="cuda")
     results = []
-    for bx, by, xp, yi, split, soft, form in shapes:
+    for bx, by, xp, yi, split, soft, form, *rest in shapes:
         tune = ktt_b200.Tune(block_x=bx, block_y=by, x_points=xp, z_iterations=yi, atom_split=split,
-                             rsqrt_soft=soft, split_form=form)
+                             rsqrt_soft=soft, split_form=form, unroll=rest[0] if rest else 1)
         if not ktt_b200.tune_supported_2d(tune):
             continue
         ms = []

@@ -67,8 +67,18 @@ def test_tune_validation_without_device():
         assert ktt_b200.tune_supported(T(atom_split=s, split_form=1, **split))
         assert ktt_b200.tune_supported_2d(T(z_iterations=4, x_points=2, rsqrt_soft=2, atom_split=s, split_form=1))
     assert not ktt_b200.tune_supported(T(atom_split=257, split_form=1, **split))
-    assert not ktt_b200.tune_supported(T(atom_split=4, split_form=2, **split))
     assert not ktt_b200.tune_supported(T(atom_split=4, split_form=1, precision=ktt_b200.PREC_FP64_MERGE, **split))
+    # the balanced form: 2..32 atom groups per CTA, tile threads x groups <= 1024
+    for g in (2, 4, 16, 32):
+        assert ktt_b200.tune_supported(T(block_x=32, block_y=1, atom_split=g, split_form=2, **split))
+        assert ktt_b200.tune_supported_2d(T(block_x=32, block_y=1, z_iterations=4, x_points=2, rsqrt_soft=2,
+                                            atom_split=g, split_form=2))
+    assert ktt_b200.tune_supported(T(block_x=32, block_y=4, atom_split=8, split_form=2, **split))
+    assert not ktt_b200.tune_supported(T(block_x=32, block_y=4, atom_split=16, split_form=2, **split))
+    assert not ktt_b200.tune_supported(T(block_x=32, block_y=1, atom_split=33, split_form=2, **split))
+    assert not ktt_b200.tune_supported(T(atom_split=4, split_form=3, **split))
+    assert not ktt_b200.tune_supported(T(block_x=32, block_y=1, atom_split=4, split_form=2,
+                                         precision=ktt_b200.PREC_COMPENSATED, **split))
 
 
 def test_variant_inventory():
@@ -79,9 +89,9 @@ def test_variant_inventory():
     split_keys = {(t.z_iterations, t.x_points, t.unroll, t.rsqrt_soft, t.split_form, d2)
                   for t, d2, soa in vs if t.atom_split}
     assert len(keys) + len(split_keys) == len(vs)  # no duplicates
-    # the atom-split forms (cluster and queue): FP32, float4 atoms through shared memory, 2D and 3D
+    # the atom-split forms (cluster, queue, balanced): FP32, float4 atoms through shared memory, 2D and 3D
     assert all(t.precision == 0 and t.atom_source == 0 and not soa for t, _, soa in vs if t.atom_split)
-    for form in (0, 1):
+    for form in (0, 1, 2):
         assert any(d2 for *_, f, d2 in split_keys if f == form) and any(not d2 for *_, f, d2 in split_keys if f == form)
     # the KTT CUDA space of CoulombSum3d.cpp: Z_ITERATIONS x unroll x USE_SOA, all present for x_points 1
     for zi in (1, 2, 4, 8, 16, 32):

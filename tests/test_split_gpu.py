@@ -1,7 +1,8 @@
 """The atom-split forms of the forward kernel against the FP64 oracle and against the
 one-CTA-per-tile form: the thread-block cluster form (cluster sizes 2..16, above 8 the B200's
-non-portable cluster sizes) and the queue form (a persistent grid over (tile, chunk) items, 2..256
-chunks); 3D maps and 2D slices, ragged atom counts (fewer atoms than chunks included), accumulate
+non-portable cluster sizes), the queue form (a persistent grid over (tile, chunk) items, 2..256
+chunks) and the balanced form (equal ranges of the (tile, atom) space per resident CTA, 2..32 atom
+groups per CTA); 3D maps and 2D slices, ragged atom counts (fewer atoms than chunks included), accumulate
 semantics, run-to-run determinism, and the two forms equal bit for bit for the same chunk count."""
 import numpy as np
 import pytest
@@ -129,3 +130,94 @@ def test_queue_split_2d_slice(ctx, shape, chunks):
     acc = base.clone()
     ctx.forward_2d(sliced, case.spacing, case.nx, case.ny, tune=tune, out=acc, accumulate=True)
     assert torch.equal(acc, base + got)
+
+
+@pytest.mark.parametrize("n_atoms", [0, 1, 5, 9, 1023, 1025, 4000, 8195])
+@pytest.mark.parametrize("block,groups", [((32, 1), 2), ((32, 1), 32), ((32, 2), 8), ((64, 1), 16)])
+def test_balanced_split_3d_matches_oracle(ctx, n_atoms, block, groups):
+    import torch
+    a = _atoms(n_atoms, seed=n_atoms + 77)
+    dims, h, origin = (37, 29, 19), 0.5, (-1.0, 0.5, 2.0)
+    tune = ktt_b200.Tune(block_x=block[0], block_y=block[1], z_iterations=8, x_points=2, rsqrt_soft=2,
+                         atom_split=groups, split_form=2)
+    atoms = torch.from_numpy(a).cuda() if n_atoms else torch.zeros((0, 4), device="cuda")
+    out = torch.full((dims[2], dims[1], dims[0]), float("nan"), device="cuda")
+    ctx.forward_3d(atoms, dims, h, origin, tune=tune, out=out)
+    got = out.cpu().numpy()
+    if n_atoms == 0:
+        assert np.all(got == 0.0)
+        return
+    ref = oracle.grid3d(a, h, dims, origin)
+    assert errors.report(got, ref)["rel_norm"] <= TOL
+    again = ctx.forward_3d(atoms, dims, h, origin, tune=tune)
+    assert torch.equal(out, again)  # fixed ranges per CTA, pieces added in CTA order
+
+
+@pytest.mark.parametrize("shape", [(4, 2, 0), (4, 2, 2), (4, 2, 3), (2, 2, 2), (8, 2, 2), (4, 4, 2), (2, 4, 2),
+                                   (8, 1, 2)])
+@pytest.mark.parametrize("block,groups", [((32, 1), 32), ((32, 1), 8), ((64, 1), 16), ((32, 2), 4)])
+def test_balanced_split_2d_slice(ctx, shape, block, groups):
+    import torch
+    zi, xp, soft = shape
+    case = workloads.slice_2d(n_atoms=4000, n=256)
+    ref = oracle.slice2d(case.ktt_atoms(), case.spacing, case.nx, case.ny)
+    sliced = ctx.slice_atoms(torch.from_numpy(case.atoms).cuda(), case.z_slice)
+    tune = ktt_b200.Tune(block_x=block[0], block_y=block[1], z_iterations=zi, x_points=xp, rsqrt_soft=soft,
+                         atom_split=groups, split_form=2)
+    got = ctx.forward_2d(sliced, case.spacing, case.nx, case.ny, tune=tune)
+    assert errors.report(got.cpu().numpy(), ref)["rel_norm"] <= TOL
+    assert torch.equal(got, ctx.forward_2d(sliced, case.spacing, case.nx, case.ny, tune=tune))
+    base = torch.linspace(-2, 2, case.nx * case.ny, device="cuda").reshape(case.ny, case.nx)
+    acc = base.clone()
+    ctx.forward_2d(sliced, case.spacing, case.nx, case.ny, tune=tune, out=acc, accumulate=True)
+    assert torch.equal(acc, base + got)
+
+
+def test_balanced_split_ragged_slice_and_slab(ctx):
+    import torch
+    a = _atoms(1234, seed=18)
+    nx, ny, h, zs = 101, 75, 0.5, 7.0
+    kat = a.copy()
+    kat[:, 2] = (np.float32(zs) - a[:, 2]) ** 2
+    ref = oracle.slice2d(kat, h, nx, ny)
+    sliced = ctx.slice_atoms(torch.from_numpy(a).cuda(), zs)
+    tune = ktt_b200.Tune(block_x=32, block_y=1, z_iterations=4, x_points=2, rsqrt_soft=2, atom_split=16,
+                         split_form=2)
+    v = ctx.forward_2d(sliced, h, nx, ny, tune=tune)
+    assert errors.report(v.cpu().numpy(), ref)["rel_norm"] <= TOL
+    # a z slab of a 3D map equals the same planes of the whole map
+    b = _atoms(900, seed=19)
+    dims = (40, 33, 48)
+    t3 = ktt_b200.Tune(block_x=32, block_y=1, z_iterations=8, x_points=1, rsqrt_soft=2, atom_split=8, split_form=2)
+    atoms = torch.from_numpy(b).cuda()
+    full = ctx.forward_3d(atoms, dims, h, tune=t3)
+    ref3 = oracle.grid3d(b, h, dims)
+    assert errors.report(full.cpu().numpy(), ref3)["rel_norm"] <= TOL
+    slab = ctx.forward_3d_slab(atoms, dims, h, 16, 40, tune=t3)
+    assert errors.report(slab.cpu().numpy(), ref3[16:40])["rel_norm"] <= TOL
+
+
+def test_balanced_split_counters_across_forms_and_grids(ctx):
+    """The balanced form zeroes its counters as it completes; launches of other grids, the queue
+    form's use of the same workspace and tiny maps (fewer units than CTAs) in between stay exact."""
+    import torch
+    a = _atoms(700, seed=23)
+    b = _atoms(3, seed=24)
+    atoms_a = torch.from_numpy(a).cuda()
+    atoms_b = torch.from_numpy(b).cuda()
+    bal = ktt_b200.Tune(block_x=32, block_y=1, z_iterations=8, x_points=2, rsqrt_soft=2, atom_split=16,
+                        split_form=2)
+    queue = ktt_b200.Tune(block_x=32, block_y=4, z_iterations=8, x_points=2, rsqrt_soft=2, atom_split=16,
+                          split_form=1)
+    cases = [((33, 17, 9), atoms_a, a, bal), ((33, 17, 9), atoms_a, a, bal), ((5, 4, 3), atoms_b, b, bal),
+             ((33, 17, 9), atoms_a, a, queue), ((33, 17, 9), atoms_a, a, bal), ((64, 40, 24), atoms_a, a, bal),
+             ((5, 4, 3), atoms_b, b, bal), ((64, 40, 24), atoms_a, a, bal)]
+    first = {}
+    for dims, atoms, host, tune in cases:
+        got = ctx.forward_3d(atoms, dims, 0.5, tune=tune)
+        ref = oracle.grid3d(host, 0.5, dims)
+        assert errors.report(got.cpu().numpy(), ref)["rel_norm"] <= TOL
+        key = (dims, tune.split_form)
+        if key in first:
+            assert torch.equal(got, first[key])
+        first.setdefault(key, got)
