@@ -140,6 +140,8 @@ typedef struct coul_ctx coul_ctx;
 
 /* ---- context ------------------------------------------------------------ */
 COUL_API int coul_ctx_create(int device, coul_ctx** ctx);
+/* Also releases the device resources of the context's batches that are still alive; their handles
+   stay valid for coul_batch_destroy only (coul_batch_run refuses them). */
 COUL_API int coul_ctx_destroy(coul_ctx* ctx);
 /* A context on the caller's own CUDA context (a CUcontext, passed as void*) instead of the device's
    primary context: every later call of this context makes cu_context current on the calling thread.
@@ -341,7 +343,11 @@ enum {
 /* Whether a persistent batched variant is compiled for this tile shape (the batch's counterpart of
    coul_tune_supported). */
 COUL_API int coul_batch_tune_supported(const coul_tune* tune);
-/* tune selects the tile shape (z_iterations, x_points, unroll, precision, rsqrt_soft, block). */
+/* tune selects the tile shape (z_iterations, x_points, unroll, precision, rsqrt_soft, block).  With
+   x_points 1 the tiles are linear in each molecule's x-y plane (thread i of x-y tile j takes the
+   plane's point j * threads + i, row-major), so only the plane's last tile is padded; otherwise the
+   block's threads are arranged per molecule as the power-of-two x extent that pads the plane least.
+   COUL_BATCH_SEPARATE launches the forward kernel of the same tune, which needs its own variant. */
 COUL_API int coul_batch_create(coul_ctx* ctx, const coul_molecule* molecules, int n_molecules, const coul_tune* tune,
                                coul_batch** batch);
 COUL_API int coul_batch_destroy(coul_batch* batch);

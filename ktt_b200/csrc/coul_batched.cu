@@ -48,6 +48,10 @@ static const std::vector<BatchVariant>& batch_variants()
         // 5/16 of the rsqrts on the FMA pipe (atoms alternating between 2 and 3 of 8 lane pairs)
         batch_variant<8, 2, 2, kPrecFp32, kSoftAlternate + 2>(),
         batch_variant<8, 2, 1, kPrecFp32, kSoftAlternate + 2>(),
+        // one x-y point per thread: linear x-y tiles, padded only at the end of each plane
+        batch_variant<16, 1, 2, kPrecFp32, 2>(),     batch_variant<16, 1, 1, kPrecFp32, kSoftAlternate + 2>(),
+        batch_variant<16, 1, 2, kPrecFp32, kSoftAlternate + 2>(), batch_variant<8, 1, 1, kPrecFp32, kSoftAlternate + 2>(),
+        batch_variant<16, 1, 1, kPrecFp64Merge, 2>(),
     };
     return v;
 }
@@ -74,10 +78,9 @@ struct coul_batch {
     int graph_accumulate = -1;
 };
 
-static void batch_release(coul_batch* b)
+// Frees a batch's device resources (its context current) and leaves the handle without them.
+static void batch_release_device(coul_batch* b)
 {
-    if (b == nullptr)
-        return;
     if (b->graph_exec)
         cudaGraphExecDestroy(b->graph_exec);
     if (b->graph)
@@ -88,8 +91,37 @@ static void batch_release(coul_batch* b)
         cudaFree(b->d_mols);
     if (b->d_counter)
         cudaFree(b->d_counter);
+    b->graph_exec = nullptr;
+    b->graph = nullptr;
+    b->capture_stream = nullptr;
+    b->d_mols = nullptr;
+    b->d_counter = nullptr;
+}
+
+static void batch_release(coul_batch* b)
+{
+    if (b == nullptr)
+        return;
+    if (b->ctx) {
+        auto& live = b->ctx->batches;
+        live.erase(std::remove(live.begin(), live.end(), b), live.end());
+    }
+    batch_release_device(b);
     delete b;
 }
+
+namespace coul {
+
+void orphan_batches(coul_ctx* ctx)
+{
+    for (coul_batch* b : ctx->batches) {
+        batch_release_device(b);
+        b->ctx = nullptr;
+    }
+    ctx->batches.clear();
+}
+
+}  // namespace coul
 
 static cudaError_t launch_batched(coul_batch* b, cudaStream_t stream, int accumulate)
 {
@@ -196,6 +228,7 @@ COUL_API int coul_batch_create(coul_ctx* ctx, const coul_molecule* molecules, in
         batch_release(b);
         return set_error(COUL_ERR_OUT_OF_MEMORY, std::string("batch set-up: ") + cudaGetErrorString(e));
     }
+    ctx->batches.push_back(b);
     *out = b;
     return COUL_OK;
 }

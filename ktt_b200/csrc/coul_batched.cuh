@@ -13,21 +13,24 @@ struct MolDesc {
     int64_t tile_begin;  // first work item of this molecule
     int nx, ny, nz;
     int tiles_x, tiles_y;
-    int tx;              // threads of a CTA along x for this molecule's tiles (the rest along y)
+    int tx;              // threads of a CTA along x for this molecule's tiles (the rest along y);
+                         // 0: linear tiles (one x-y point per thread, consecutive in the x-y plane)
     int vec_ok;
     float h, ox, oy, oz;
 };
 
-// Tile geometry of one molecule: its CTA threads are arranged as tx x (threads / tx), tx the power
-// of two dividing the thread count whose tile pads the grid's x-y plane least (ties: the block's
-// own x size).  The arrangement only moves points between threads; every point is computed the
-// same way.  Returns the molecule's work items.
+// Tile geometry of one molecule.  With one x point per thread (x_points 1) the tiles are linear:
+// thread i of x-y tile j takes the point j * threads + i of the grid's x-y plane in row-major order,
+// so only the plane's last tile is padded.  Otherwise the CTA threads are arranged as
+// tx x (threads / tx), tx the power of two dividing the thread count whose tile pads the grid's x-y
+// plane least (ties: the block's own x size).  The arrangement only moves points between threads;
+// every point is computed the same way.  Returns the molecule's work items.
 inline int64_t fill_mol_desc(MolDesc& d, const coul_molecule& m, const coul_tune& t)
 {
     const int threads = t.block_x * t.block_y;
     int best_tx = t.block_x;
     int64_t best_area = -1;
-    for (int tx = 1; tx <= threads; tx *= 2) {
+    for (int tx = 1; tx <= threads && t.x_points > 1; tx *= 2) {
         if (threads % tx)
             continue;
         const int64_t sx = static_cast<int64_t>(tx) * t.x_points;
@@ -48,11 +51,17 @@ inline int64_t fill_mol_desc(MolDesc& d, const coul_molecule& m, const coul_tune
     d.ox = m.grid.origin[0];
     d.oy = m.grid.origin[1];
     d.oz = m.grid.origin[2];
-    d.tx = best_tx;
-    const int64_t span_x = static_cast<int64_t>(best_tx) * t.x_points;
-    const int ty = threads / best_tx;
-    d.tiles_x = static_cast<int>((m.grid.nx + span_x - 1) / span_x);
-    d.tiles_y = (m.grid.ny + ty - 1) / ty;
+    if (t.x_points == 1) {
+        d.tx = 0;
+        d.tiles_x = static_cast<int>((static_cast<int64_t>(m.grid.nx) * m.grid.ny + threads - 1) / threads);
+        d.tiles_y = 1;
+    } else {
+        d.tx = best_tx;
+        const int64_t span_x = static_cast<int64_t>(best_tx) * t.x_points;
+        const int ty = threads / best_tx;
+        d.tiles_x = static_cast<int>((m.grid.nx + span_x - 1) / span_x);
+        d.tiles_y = (m.grid.ny + ty - 1) / ty;
+    }
     const int tiles_z = (m.grid.nz + t.z_iterations - 1) / t.z_iterations;
     const int xp = t.x_points;
     d.vec_ok = (xp > 1 && m.grid.nx % xp == 0 &&
@@ -121,9 +130,17 @@ __global__ void __launch_bounds__(kMaxThreads) batched_kernel(const BatchParams 
         p.out = m.out;
         p.accumulate = b.accumulate;
         p.status = b.status;
-        const int ty = static_cast<int>(blockDim.x * blockDim.y) / m.tx;
-        const int x0 = (tile_x * m.tx + tid % m.tx) * XP;
-        const int yrow = tile_y * ty + tid / m.tx;
+        int x0, yrow;
+        if (XP == 1 && m.tx == 0) {
+            // linear tile: plane points beyond the last row land at y >= ny (evaluated, not stored)
+            const int64_t q = static_cast<int64_t>(tile_x) * (blockDim.x * blockDim.y) + tid;
+            x0 = static_cast<int>(q % m.nx);
+            yrow = static_cast<int>(q / m.nx);
+        } else {
+            const int ty = static_cast<int>(blockDim.x * blockDim.y) / m.tx;
+            x0 = (tile_x * m.tx + tid % m.tx) * XP;
+            yrow = tile_y * ty + tid / m.tx;
+        }
         const int z0 = tile_z * ZI;
         // tiles that overhang the molecule's grid in z evaluate only their points inside it
         if (!tile_pass<ZI, XP, UNR, kSrcShared, 0, PREC, SOFT, kModeGrid3d, true>(p, x0, yrow, z0, m.vec_ok,

@@ -580,6 +580,7 @@ COUL_API int coul_ctx_destroy(coul_ctx* ctx)
     ctx_activate(ctx);
     if (ctx->stream)
         cudaStreamSynchronize(ctx->stream);
+    orphan_batches(ctx);
     if (ctx->d_atoms_cache)
         cudaFree(ctx->d_atoms_cache);
     if (ctx->d_out_cache)

@@ -19,6 +19,7 @@ static void add_soft(std::vector<VariantEntry>& v)
     add_variant<8, 2, 2, kSrcShared, 0, PREC, SOFT, kModeGrid3d>(v);
     add_variant<8, 4, 1, kSrcShared, 0, PREC, SOFT, kModeGrid3d>(v);
     add_variant<16, 1, 1, kSrcShared, 0, PREC, SOFT, kModeGrid3d>(v);
+    add_variant<16, 1, 2, kSrcShared, 0, PREC, SOFT, kModeGrid3d>(v);
     add_variant<16, 2, 1, kSrcShared, 0, PREC, SOFT, kModeGrid3d>(v);
     add_variant<16, 4, 1, kSrcShared, 0, PREC, SOFT, kModeGrid3d>(v);
     add_variant<32, 2, 1, kSrcShared, 0, PREC, SOFT, kModeGrid3d>(v);

@@ -10,6 +10,8 @@
 #include "coul_forward.cuh"
 #include "coulktt.h"
 
+struct coul_batch;
+
 struct coul_ctx {
     int device = 0;
     void* user_context = nullptr;  // the caller's CUcontext (coul_ctx_create_on), else the primary context
@@ -29,6 +31,7 @@ struct coul_ctx {
     std::vector<std::function<void()>> cleanups;  // frees buffers owned by other units (run at destroy)
     void* adjoint_workspace = nullptr;            // FP64 partials of coul_adjoint_3d (coul_adjoint.cu)
     void* queue_workspace = nullptr;              // partial blocks and counters of the atom split's queue form
+    std::vector<coul_batch*> batches;             // live batches (their device resources go with the context)
 };
 
 namespace coul {
@@ -44,5 +47,8 @@ int validate_grid(const coul_grid* g);
 int launch_forward(coul_ctx* ctx, const VariantEntry* v, const FwdParams& prm, int mode, const coul_tune* t);
 int queue_split_setup(coul_ctx* ctx, const VariantEntry* v, FwdLaunch& L, const coul_tune* t);
 int balanced_split_setup(coul_ctx* ctx, const VariantEntry* v, FwdLaunch& L, const coul_tune* t);
+// Releases the device resources of the context's live batches and detaches them (coul_batched.cu);
+// their handles stay valid for coul_batch_destroy.  Called by coul_ctx_destroy, context current.
+void orphan_batches(coul_ctx* ctx);
 
 }  // namespace coul

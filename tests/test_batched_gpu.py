@@ -19,6 +19,9 @@ def _small_batch(seed=21, n_mol=24, lo=50, hi=3000):
     ktt_b200.Tune(z_iterations=16, x_points=1, rsqrt_soft=2, block_x=64, block_y=2),
     ktt_b200.Tune(z_iterations=8, x_points=2, precision=ktt_b200.PREC_FP64_MERGE, rsqrt_soft=2),
     ktt_b200.Tune(z_iterations=8, x_points=2, unroll=2, rsqrt_soft=12),
+    # one x-y point per thread: linear x-y tiles in the batch, the block's own tiles one launch per molecule
+    ktt_b200.Tune(z_iterations=16, x_points=1, unroll=2, rsqrt_soft=12, block_x=8, block_y=4),
+    ktt_b200.Tune(z_iterations=8, x_points=1, rsqrt_soft=12, block_x=16, block_y=4),
 ])
 def test_persistent_graph_and_separate_agree_bitwise(ctx, tune):
     import torch
@@ -44,11 +47,13 @@ def test_persistent_graph_and_separate_agree_bitwise(ctx, tune):
     b.close()
 
 
-def test_batched_against_oracle(ctx):
+@pytest.mark.parametrize("tune", [None, ktt_b200.Tune(z_iterations=16, x_points=1, unroll=2, rsqrt_soft=2, block_x=8,
+                                                     block_y=4)])
+def test_batched_against_oracle(ctx, tune):
     import torch
     mols = _small_batch(seed=22, n_mol=10)
     inputs = [(torch.from_numpy(m.atoms).cuda(), m.dims, m.spacing, m.origin) for m in mols]
-    b = ktt_b200.Batch(ctx, inputs)
+    b = ktt_b200.Batch(ctx, inputs, tune) if tune is not None else ktt_b200.Batch(ctx, inputs)
     b.run(ktt_b200.BATCH_GRAPH)
     ctx.synchronize()
     for m, out in zip(mols, b.outputs):
@@ -67,3 +72,21 @@ def test_batch_rejects_unsupported_shape(ctx):
     with pytest.raises(ktt_b200.CoulombError) as e:
         ktt_b200.Batch(ctx, inputs, ktt_b200.Tune(z_iterations=32, x_points=4, rsqrt_soft=1))
     assert e.value.status == ktt_b200.COUL_ERR_UNSUPPORTED
+
+
+def test_batch_outlives_its_context():
+    """Destroying a context releases its live batches' device resources; the batch handles can still
+    be destroyed afterwards, and a run on them is refused."""
+    import torch
+    mols = _small_batch(n_mol=3)
+    c = ktt_b200.CoulombContext(0)
+    inputs = [(torch.from_numpy(m.atoms).cuda(), m.dims, m.spacing, m.origin) for m in mols]
+    kept = ktt_b200.Batch(c, inputs)
+    closed = ktt_b200.Batch(c, inputs)
+    closed.close()
+    kept.run(ktt_b200.BATCH_PERSISTENT)
+    c.synchronize()
+    c.close()
+    lib = ktt_b200.load_library()
+    assert lib.coul_batch_run(None, kept._handle, ktt_b200.BATCH_PERSISTENT, 0) == ktt_b200.COUL_ERR_INVALID_ARGUMENT
+    kept.close()
