@@ -293,6 +293,7 @@ __device__ __forceinline__ bool tile_accumulate(const FwdParams& p, const int x0
             const int cnt = stage_count(s);
             // atoms the stage evaluates: a ragged last stage rounds up to whole sub-tiles only
             const int ntr = cnt < kTileAtoms ? (cnt + kSubTile - 1) / kSubTile * kSubTile : kTileAtoms;
+            __builtin_assume(ntr > 0 && ntr <= kTileAtoms && ntr % kSubTile == 0);
             unsigned char* tile = tiles + buf * kTileAtoms * 16;
             if (ok && cnt < kTileAtoms) {
                 // Ragged last stage: the SoA remainder (< 4 atoms) by plain loads, then padding atoms
@@ -343,11 +344,9 @@ __device__ __forceinline__ bool tile_accumulate(const FwdParams& p, const int x0
             // the stage runs in whole sub-tiles of kSubTile atoms (ntr of them: all kTileAtoms, or the
             // ragged last stage rounded up); the whole stage is one phase of the FMA-pipe share's pattern
             if constexpr (PREC == kPrecFp64Pairs) {
-                for (int j0 = 0; j0 < ntr; j0 += kSubTile) {
 #pragma unroll UNR
-                    for (int j = 0; j < kSubTile; ++j)
-                        pair_block_3d_f64<XP, ZI>(gxd, gyd, gzd, atom_at(j0 + j), accd);
-                }
+                for (int j = 0; j < ntr; ++j)
+                    pair_block_3d_f64<XP, ZI>(gxd, gyd, gzd, atom_at(j), accd);
             } else {
                 // G: the stage's phase of the FMA-pipe share; LA: the z points the tile evaluates
                 auto stage = [&](auto phase, auto lanes) {
@@ -356,11 +355,9 @@ __device__ __forceinline__ bool tile_accumulate(const FwdParams& p, const int x0
                     constexpr int ZA = (LA + 1) / 2;
                     constexpr bool HA = (LA & 1) != 0;
                     if constexpr (PREC == kPrecFp32) {
-                        for (int j0 = 0; j0 < ntr; j0 += kSubTile) {
 #pragma unroll UNR
-                            for (int j = 0; j < kSubTile; ++j)
-                                eval_atom<MODE, XP, ZH, SOFT, G, HA, ZA>(gx, gy, gb, atom_at(j0 + j), acc);
-                        }
+                        for (int j = 0; j < ntr; ++j)
+                            eval_atom<MODE, XP, ZH, SOFT, G, HA, ZA>(gx, gy, gb, atom_at(j), acc);
                     } else {
                         for (int j0 = 0; j0 < ntr; j0 += kSubTile) {
                             clear_part();
