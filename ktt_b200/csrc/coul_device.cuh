@@ -72,6 +72,14 @@ __device__ __forceinline__ void fence_mbar_init()
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
+// Device-scope atomic add with acquire-release semantics; returns the old value.
+__device__ __forceinline__ unsigned atom_add_acq_rel_gpu(unsigned* p, unsigned v)
+{
+    unsigned old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+
 // Orders this thread's generic-proxy shared-memory accesses before later async-proxy (TMA) ones.
 __device__ __forceinline__ void fence_proxy_async_smem()
 {

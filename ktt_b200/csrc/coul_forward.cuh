@@ -791,15 +791,20 @@ __global__ void __launch_bounds__(kBalThreads, 1) balanced_split_kernel(const Fw
         s_issue_a = piece_end ? 0 : a + cnt;
         s_issued += 1u;
     };
+    // thread 0 initialises the ring and starts its first copies before the CTA's barrier, so the
+    // first atoms are in flight while the CTA's later warps are still being launched
     if (tid == 0) {
         s_issue_t = t_begin;
         s_issue_a = a_begin;
         s_issued = 0u;
-    }
-    ring_init(full, tid);
-    if (tid == 0)
+#pragma unroll
+        for (int st = 0; st < kStages; ++st)
+            mbar_init(&full[st], 1);
+        fence_mbar_init();
         while (s_issued < static_cast<uint32_t>(kStages) && s_issue_t <= t_end)
             issue();
+    }
+    __syncthreads();
 
     float gx[XP];
     float gy = 0.0f;
@@ -893,25 +898,23 @@ __global__ void __launch_bounds__(kBalThreads, 1) balanced_split_kernel(const Fw
     }
 
     // Count this CTA's split pieces (after all its partial blocks are written) and finish the tiles
-    // whose last piece it added.  The counting thread releases the CTA's writes before its count and
-    // acquires the other CTAs' after it; the barriers order the CTA's threads against it.
+    // whose last piece it added; the barriers order the CTA's threads against the counting threads.
     const bool first_split = a_begin > 0 || (t_begin == t_end && a_stop < N);
     const bool last_split = t_end != t_begin && a_stop < N;
     if (first_split || last_split) {
         if (tid == 0)
             s_last = 0;
         __syncthreads();
-        // lane 0 of warp i counts the CTA's first (i = 0) or last (i = 1) split piece
+        // lane 0 of warp i counts the CTA's first (i = 0) or last (i = 1) split piece, with one
+        // acquire-release atomic (release: the CTA's partial blocks, ordered before it by the barrier;
+        // acquire: the other CTAs' partial blocks of a tile whose last piece this is)
         const int i = tid / 32;
         if (tid % 32 == 0 && i < 2 && (i == 0 ? first_split : last_split)) {
-            __threadfence();
             const int64_t t = i == 0 ? t_begin : t_end;
             const int64_t first = split.cta_of(t * N);
             const int64_t last = split.cta_of((t + 1) * N - 1);
-            if (atomicAdd(&sq.tile_done[first], 1u) == static_cast<unsigned>(last - first)) {
-                __threadfence();
+            if (atom_add_acq_rel_gpu(&sq.tile_done[first], 1u) == static_cast<unsigned>(last - first))
                 atomicOr(&s_last, 1 << i);
-            }
         }
         __syncthreads();
         const int mask = s_last;
