@@ -81,8 +81,8 @@ enum {
    the fourth evaluates each pair in FP64. */
 enum {
     COUL_PREC_FP32 = 0,        /* one FP32 accumulator per point (KTT's kernel) */
-    COUL_PREC_COMPENSATED = 1, /* FP32 partial per atom sub-tile, merged by two-sum into (sum, error) */
-    COUL_PREC_FP64_MERGE = 2,  /* FP32 partial per atom sub-tile, merged into an FP64 accumulator */
+    COUL_PREC_COMPENSATED = 1, /* FP32 partial per 64-atom sub-tile, merged by two-sum into (sum, error) */
+    COUL_PREC_FP64_MERGE = 2,  /* FP32 partial per 64-atom sub-tile, merged into an FP64 accumulator */
     COUL_PREC_FP64_PAIRS = 3   /* every pair in FP64: exact differences, FP64 r^2, MUFU rsqrt estimate
                                   refined by one FP64 Newton step (about 2^-40), FP64 accumulation; the
                                   map's error is then its FP32 store.  3D maps, rsqrt_soft 0 only */

@@ -27,8 +27,8 @@ namespace coul {
 
 constexpr int kTileAtoms = 256;       // atoms per shared-memory stage
 constexpr int kStages = 2;            // depth of the TMA ring
-constexpr int kSubTile = 32;          // atoms per FP32 partial in the compensated / FP64-merge forms;
-                                      // a ragged last stage is evaluated in whole sub-tiles
+constexpr int kSubTile = 32;          // a ragged last stage is evaluated in whole sub-tiles of this many
+constexpr int kMergeAtoms = 64;       // atoms per FP32 partial in the compensated / FP64-merge forms
 constexpr int kMaxThreads = 256;      // launch bound of the forward kernels
 constexpr int kConstAtoms = 4096;     // atoms per __constant__ chunk (64 KiB)
 constexpr uint64_t kWaitBudgetNs = 1000000000ull;  // 1 s: a tile copy from L2 takes microseconds

@@ -158,7 +158,9 @@ __device__ __forceinline__ bool tile_accumulate(const FwdParams& p, const int x0
     static_assert(!ZTRIM || (MODE == kModeGrid3d && SRC == kSrcShared && PREC != kPrecFp64Pairs),
                   "z trimming: 3D maps, shared-memory atoms, FP32 pairs");
     static_assert(XP == 1 || XP == 2 || XP == 4 || XP == 8, "XP must be 1, 2, 4 or 8");
-    static_assert(kTileAtoms % kSubTile == 0, "sub-tiles must divide the stage");
+    // atoms per FP32 partial of the compensated / FP64-merge forms, and the ragged stage's granularity
+    constexpr int SUB = (PREC == kPrecCompensated || PREC == kPrecFp64Merge) ? kMergeAtoms : kSubTile;
+    static_assert(kTileAtoms % SUB == 0, "sub-tiles must divide the stage");
 
     float gx[XP];
 #pragma unroll
@@ -292,8 +294,8 @@ __device__ __forceinline__ bool tile_accumulate(const FwdParams& p, const int x0
             const bool ok = mbar_wait_bounded(&full[buf], parity);
             const int cnt = stage_count(s);
             // atoms the stage evaluates: a ragged last stage rounds up to whole sub-tiles only
-            const int ntr = cnt < kTileAtoms ? (cnt + kSubTile - 1) / kSubTile * kSubTile : kTileAtoms;
-            __builtin_assume(ntr > 0 && ntr <= kTileAtoms && ntr % kSubTile == 0);
+            const int ntr = cnt < kTileAtoms ? (cnt + SUB - 1) / SUB * SUB : kTileAtoms;
+            __builtin_assume(ntr > 0 && ntr <= kTileAtoms && ntr % SUB == 0);
             unsigned char* tile = tiles + buf * kTileAtoms * 16;
             if (ok && cnt < kTileAtoms) {
                 // Ragged last stage: the SoA remainder (< 4 atoms) by plain loads, then padding atoms
@@ -341,8 +343,8 @@ __device__ __forceinline__ bool tile_accumulate(const FwdParams& p, const int x0
                     return make_float4(f[j], f[kTileAtoms + j], f[2 * kTileAtoms + j], f[3 * kTileAtoms + j]);
                 }
             };
-            // the stage runs in whole sub-tiles of kSubTile atoms (ntr of them: all kTileAtoms, or the
-            // ragged last stage rounded up); the whole stage is one phase of the FMA-pipe share's pattern
+            // the stage runs in whole sub-tiles of SUB atoms (ntr atoms: all kTileAtoms, or the ragged
+            // last stage rounded up); the whole stage is one phase of the FMA-pipe share's pattern
             if constexpr (PREC == kPrecFp64Pairs) {
 #pragma unroll UNR
                 for (int j = 0; j < ntr; ++j)
@@ -359,10 +361,10 @@ __device__ __forceinline__ bool tile_accumulate(const FwdParams& p, const int x0
                         for (int j = 0; j < ntr; ++j)
                             eval_atom<MODE, XP, ZH, SOFT, G, HA, ZA>(gx, gy, gb, atom_at(j), acc);
                     } else {
-                        for (int j0 = 0; j0 < ntr; j0 += kSubTile) {
+                        for (int j0 = 0; j0 < ntr; j0 += SUB) {
                             clear_part();
 #pragma unroll UNR
-                            for (int j = 0; j < kSubTile; ++j)
+                            for (int j = 0; j < SUB; ++j)
                                 eval_atom<MODE, XP, ZH, SOFT, G, HA, ZA>(gx, gy, gb, atom_at(j0 + j), part);
                             merge();
                         }

@@ -1,5 +1,5 @@
 // Forward variants: 3D, float4 atoms through TMA-staged shared memory, FP32 partials per
-// 32-atom sub-tile merged by two-sum (compensated) or into FP64 (FP64 merge).
+// 64-atom sub-tile merged by two-sum (compensated) or into FP64 (FP64 merge).
 #include "coul_forward.cuh"
 
 namespace coul {
