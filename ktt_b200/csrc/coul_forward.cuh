@@ -808,12 +808,33 @@ __global__ void __launch_bounds__(kBalThreads, 1) balanced_split_kernel(const Fw
     }
     __syncthreads();
 
+    // The CTA's stages (the same count in every thread): the first piece's first stage holds at most
+    // kBalFirstAtoms atoms, every other at most kBalStageAtoms.  Only a stage whose buffer is refilled
+    // ends with a barrier.
+    auto stages_of = [](int atoms) { return (atoms + kBalStageAtoms - 1) / kBalStageAtoms; };
+    const int first_len = (t_begin == t_end ? a_stop : N) - a_begin;
+    const uint32_t n_stages = static_cast<uint32_t>(
+        1 + stages_of(first_len > kBalFirstAtoms ? first_len - kBalFirstAtoms : 0) +
+        (t_end > t_begin ? (t_end - t_begin - 1) * stages_of(N) + stages_of(a_stop) : 0));
+
     float gx[XP];
     float gy = 0.0f;
     float2 gb[ZH];
     float2 acc[XP][ZH];
     int tile_x = 0, tile_y = 0, x0 = 0, yrow = 0, z0 = 0;
     uint32_t k = 0;
+    bool failed = false;  // this thread gave up on a stage's copy
+    // A copy that never completed: the CTA learns of it at its next barrier; thread 0 then records it,
+    // drains what may still be in flight (bounded) and the CTA leaves.  Only the last kStages issued
+    // stages can be in flight: no stage is issued after a barrier that saw a failure.
+    auto give_up = [&]() {
+        if (tid == 0) {
+            report_status(p.status, kStatusTimeout);
+            const uint32_t issued = s_issued;
+            for (uint32_t r = issued > kStages ? issued - kStages : 0u; r < issued; ++r)
+                (void)mbar_wait_bounded(&full[r % kStages], (r / kStages) & 1u);
+        }
+    };
     for (int t = t_begin, a = a_begin; t <= t_end; ++k) {
         const int cnt = stage_count(t, a);
         const int piece_first = t == t_begin ? a_begin : 0;
@@ -830,44 +851,43 @@ __global__ void __launch_bounds__(kBalThreads, 1) balanced_split_kernel(const Fw
                     acc[i][j] = make_float2(0.0f, 0.0f);
         }
         const int buf = static_cast<int>(k % kStages);
-        const bool ok = mbar_wait_bounded(&full[buf], (k / kStages) & 1u);
-        // a ragged stage: zero-charge padding atoms up to the next whole step
-        const int cnt_step = (cnt + kBalAtomStep - 1) / kBalAtomStep * kBalAtomStep;
-        if (ok)
-            for (int j = cnt + tid; j < cnt_step; j += nthreads)
-                reinterpret_cast<float4*>(smem_raw)[buf * kBalStageAtoms + j] =
-                    make_float4(kPadCoord, kPadCoord, kPadCoord, 0.0f);
-        if (__syncthreads_or(ok ? 0 : 1)) {
-            // a copy never completed: record it, drain what may still be in flight (bounded), leave
-            if (tid == 0) {
-                report_status(p.status, kStatusTimeout);
-                for (uint32_t r = k; r < s_issued; ++r)
-                    (void)mbar_wait_bounded(&full[r % kStages], (r / kStages) & 1u);
-            }
-            return;
-        }
-        // group grp's share of the stage: `per` atoms (a whole number of steps) from grp * per
+        // once this thread has given up, it no longer waits (its values are void anyway)
+        if (!failed && !mbar_wait_bounded(&full[buf], (k / kStages) & 1u))
+            failed = true;
+        // group grp's share of the stage: `per` atoms (a whole number of steps) from grp * per, the
+        // last step of a ragged share atom by atom
         const int per = ((cnt + groups - 1) / groups + kBalAtomStep - 1) / kBalAtomStep * kBalAtomStep;
         const int j_begin = grp * per;
         const int j_count = cnt - j_begin < per ? cnt - j_begin : per;
         if (j_count > 0) {
-            const int j_end = j_begin + (j_count + kBalAtomStep - 1) / kBalAtomStep * kBalAtomStep;
+            const int j_full = j_begin + j_count / kBalAtomStep * kBalAtomStep;
+            const int j_stop = j_begin + j_count;
             const float4* tile = ring + buf * kBalStageAtoms;
             // the stage and the group select the phase of the FMA-pipe share (as in the other forms,
             // one form per lane pair for a contiguous run of atoms)
             with_phase<P>(static_cast<int>((k + static_cast<uint32_t>(grp)) % P), [&](auto phase) {
                 constexpr int G = decltype(phase)::value;
-                for (int j0 = j_begin; j0 < j_end; j0 += kBalAtomStep) {
+                for (int j0 = j_begin; j0 < j_full; j0 += kBalAtomStep) {
 #pragma unroll UNR
                     for (int j = 0; j < kBalAtomStep; ++j)
                         eval_atom<MODE, XP, ZH, SOFT, G, HALF>(gx, gy, gb, tile[j0 + j], acc);
                 }
+#pragma unroll 1
+                for (int j = j_full; j < j_stop; ++j)
+                    eval_atom<MODE, XP, ZH, SOFT, G, HALF>(gx, gy, gb, tile[j], acc);
             });
         }
-        fence_proxy_async_smem();
-        __syncthreads();
-        if (tid == 0 && s_issue_t <= t_end)
-            issue();
+        if (k + kStages < n_stages) {
+            // the buffer is refilled: everyone is done with it (generic-proxy reads ordered before
+            // the TMA's write)
+            fence_proxy_async_smem();
+            if (__syncthreads_or(failed ? 1 : 0)) {
+                give_up();
+                return;
+            }
+            if (tid == 0)
+                issue();
+        }
         a += cnt;
         const int piece_stop = t == t_end ? a_stop : N;
         if (a == piece_stop) {
@@ -877,7 +897,10 @@ __global__ void __launch_bounds__(kBalThreads, 1) balanced_split_kernel(const Fw
 #pragma unroll
                 for (int m = 0; m < ZI; ++m)
                     red[(grp * XP * ZI + i * ZI + m) * tile_threads + ttid] = lane(acc[i][m / 2], m & 1);
-            __syncthreads();
+            if (__syncthreads_or(failed ? 1 : 0)) {
+                give_up();
+                return;
+            }
             // A split tile's pieces: CTA c's first piece when c starts inside the tile, else its last
             // one; two partial-block slots per CTA.  Only a CTA's first and last pieces can be split;
             // they are counted when the CTA ends.
