@@ -20,7 +20,9 @@
 // RSQRT_SOFT (share of reciprocal square roots on the FMA pipe, of 8), ATOM_SPLIT (2 or more: the
 // atoms are split into that many chunks per point tile) and SPLIT_FORM (0: a thread-block cluster
 // of ATOM_SPLIT CTAs shares each tile, 2..16; 1: a persistent grid takes (tile, chunk) items from a
-// device queue, 2..256).  A configuration that maps to no compiled variant
+// device queue, 2..256; 2: one CTA per SM of WORK_GROUP_SIZE_X x WORK_GROUP_SIZE_Y x ATOM_SPLIT
+// threads (at most 1,024) takes an equal range of the (tile, atom) space, ATOM_SPLIT = 2..32 atom
+// groups sharing each tile's points).  A configuration that maps to no compiled variant
 // ends with ResultStatus::CompilationFailed, one beyond the device's launch limits with
 // DeviceLimitsExceeded -- the statuses KTT reports for a kernel that fails to compile or launch.
 // A definition with no built-in implementation is rejected when it is run.  GetKernelSource still
