@@ -290,7 +290,7 @@ int validate_grid(const coul_grid* g)
 
 // Device memory of the queue and balanced forms of the atom split, kept in the context and grown on
 // demand: partial blocks and counters (the layout is each form's own).
-struct QueueWorkspace {
+struct SplitWorkspace {
     void* mem = nullptr;
     size_t bytes = 0;
     // The balanced form's counters (at the start of the memory, one per CTA) are known to be zero for
@@ -303,10 +303,10 @@ struct QueueWorkspace {
 // Grow the context's split workspace to `need` bytes (drains the stream before freeing the old one).
 static int split_workspace(coul_ctx* ctx, size_t need, unsigned char** base)
 {
-    auto* ws = static_cast<QueueWorkspace*>(ctx->queue_workspace);
+    auto* ws = static_cast<SplitWorkspace*>(ctx->split_workspace_state);
     if (ws == nullptr) {
-        ws = new QueueWorkspace();
-        ctx->queue_workspace = ws;
+        ws = new SplitWorkspace();
+        ctx->split_workspace_state = ws;
         ctx->cleanups.push_back([ws] {
             if (ws->mem)
                 cudaFree(ws->mem);
@@ -370,7 +370,7 @@ int balanced_split_setup(coul_ctx* ctx, const VariantEntry* v, FwdLaunch& L, con
     const int rc = split_workspace(ctx, need, &base);
     if (rc != COUL_OK)
         return rc;
-    auto* ws = static_cast<QueueWorkspace*>(ctx->queue_workspace);
+    auto* ws = static_cast<SplitWorkspace*>(ctx->split_workspace_state);
     if (ws->balanced_clean_ctas != ctas) {
         if ((e = cudaMemsetAsync(base, 0, done_bytes, ctx->stream)) != cudaSuccess)
             return cuda_error(e, "balanced form counters reset");
@@ -398,7 +398,7 @@ int queue_split_setup(coul_ctx* ctx, const VariantEntry* v, FwdLaunch& L, const 
     const int rc = split_workspace(ctx, need, &base);
     if (rc != COUL_OK)
         return rc;
-    static_cast<QueueWorkspace*>(ctx->queue_workspace)->balanced_clean_ctas = 0;
+    static_cast<SplitWorkspace*>(ctx->split_workspace_state)->balanced_clean_ctas = 0;
     cudaError_t e;
     // the per-tile counters and the queue head start every launch at zero
     if ((e = cudaMemsetAsync(base + done_offset, 0, need - done_offset, ctx->stream)) != cudaSuccess)
@@ -687,8 +687,8 @@ COUL_API int coul_synchronize(coul_ctx* ctx)
         return cuda_error(e, "status read-back");
     if (status != kStatusOk) {
         cudaMemset(ctx->d_status, 0, sizeof(int));
-        if (ctx->queue_workspace)  // a kernel that gave up may have left counters behind
-            static_cast<QueueWorkspace*>(ctx->queue_workspace)->balanced_clean_ctas = 0;
+        if (ctx->split_workspace_state)  // a kernel that gave up may have left counters behind
+            static_cast<SplitWorkspace*>(ctx->split_workspace_state)->balanced_clean_ctas = 0;
         return set_error(COUL_ERR_TIMEOUT, "a kernel gave up on a bounded wait (status " + std::to_string(status) +
                                                "); its output is invalid");
     }

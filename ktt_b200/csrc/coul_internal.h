@@ -30,7 +30,7 @@ struct coul_ctx {
     int cc_minor = 0;
     std::vector<std::function<void()>> cleanups;  // frees buffers owned by other units (run at destroy)
     void* adjoint_workspace = nullptr;            // FP64 partials of coul_adjoint_3d (coul_adjoint.cu)
-    void* queue_workspace = nullptr;              // partial blocks and counters of the atom split's queue form
+    void* split_workspace_state = nullptr;        // partial blocks and counters of the queue and balanced forms
     std::vector<coul_batch*> batches;             // live batches (their device resources go with the context)
 };
 
