@@ -77,15 +77,18 @@ enum {
     COUL_ATOMS_CONSTANT = 1    /* chunks of 4096 atoms copied into __constant__ memory */
 };
 
-/* Precision form.  The first three evaluate each pair in FP32 and differ in how they accumulate;
-   the fourth evaluates each pair in FP64. */
+/* Precision form.  FP32, compensated and both FP64 merges evaluate each pair in FP32 and differ in
+   how they accumulate; FP64 pairs evaluates each pair in FP64. */
 enum {
     COUL_PREC_FP32 = 0,        /* one FP32 accumulator per point (KTT's kernel) */
     COUL_PREC_COMPENSATED = 1, /* FP32 partial per 64-atom sub-tile, merged by two-sum into (sum, error) */
     COUL_PREC_FP64_MERGE = 2,  /* FP32 partial per 64-atom sub-tile, merged into an FP64 accumulator */
-    COUL_PREC_FP64_PAIRS = 3   /* every pair in FP64: exact differences, FP64 r^2, MUFU rsqrt estimate
+    COUL_PREC_FP64_PAIRS = 3,  /* every pair in FP64: exact differences, FP64 r^2, MUFU rsqrt estimate
                                   refined by one FP64 Newton step (about 2^-40), FP64 accumulation; the
                                   map's error is then its FP32 store.  3D maps, rsqrt_soft 0 only */
+    COUL_PREC_FP64_MERGE_SHARED = 4 /* COUL_PREC_FP64_MERGE with the FP64 sums in shared memory instead of
+                                       registers (8 bytes per point per thread): the same values bit for
+                                       bit, more resident warps.  3D maps, TMA-staged atoms */
 };
 
 /*

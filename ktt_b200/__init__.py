@@ -35,6 +35,7 @@ PREC_FP32 = 0
 PREC_COMPENSATED = 1
 PREC_FP64_MERGE = 2
 PREC_FP64_PAIRS = 3
+PREC_FP64_MERGE_SHARED = 4  # PREC_FP64_MERGE with the FP64 sums in shared memory (same values, fewer registers)
 
 
 class CoulombError(RuntimeError):

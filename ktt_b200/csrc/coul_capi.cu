@@ -39,6 +39,7 @@ std::vector<VariantEntry>& registry()
         register_fwd_3d_soft(v);
         register_fwd_3d_soft_precise(v);
         register_fwd_3d_soft_fp64m(v);
+        register_fwd_3d_soft_fp64s(v);
         register_fwd_3d_fp64(v);
         register_fwd_2d(v);
         register_fwd_split(v);
@@ -242,7 +243,7 @@ int validate_tune(const coul_tune* t, int mode, int soa, const VariantEntry** ou
                                                      std::to_string(kMaxThreads) + " threads");
     if (t->atom_source != COUL_ATOMS_SHARED_TMA && t->atom_source != COUL_ATOMS_CONSTANT)
         return set_error(COUL_ERR_INVALID_ARGUMENT, "unknown atom_source");
-    if (t->precision < COUL_PREC_FP32 || t->precision > COUL_PREC_FP64_PAIRS)
+    if (t->precision < COUL_PREC_FP32 || t->precision > COUL_PREC_FP64_MERGE_SHARED)
         return set_error(COUL_ERR_INVALID_ARGUMENT, "unknown precision");
     if (t->rsqrt_soft < 0 || (t->rsqrt_soft > 8 && t->rsqrt_soft < kSoftAlternate) || t->rsqrt_soft > kSoftAlternate + 7)
         return set_error(COUL_ERR_INVALID_ARGUMENT, "rsqrt_soft must be in 0..8 or 10..17");
@@ -442,6 +443,8 @@ int launch_forward(coul_ctx* ctx, const VariantEntry* v, const FwdParams& prm, i
         return set_error(COUL_ERR_DEVICE_LIMITS, "grid too large for one launch");
     L.grid = dim3(static_cast<unsigned>(gx), static_cast<unsigned>(gy), static_cast<unsigned>(gz));
     L.smem = (t->atom_source == COUL_ATOMS_SHARED_TMA) ? (kStages * kTileAtoms * 16 + kStages * 8) : 0;
+    if (t->precision == COUL_PREC_FP64_MERGE_SHARED)
+        L.smem += shared_sums_bytes(t->block_x * t->block_y, t->z_iterations * t->x_points);
     if (v->key.split == 1) {
         L.split = t->atom_split;
         L.smem = split_smem_bytes(t->block_x * t->block_y, t->z_iterations * t->x_points);

@@ -21,7 +21,16 @@
 namespace coul {
 
 enum : int { kSrcShared = 0, kSrcConstant = 1 };
-enum : int { kPrecFp32 = 0, kPrecCompensated = 1, kPrecFp64Merge = 2, kPrecFp64Pairs = 3 };
+enum : int { kPrecFp32 = 0, kPrecCompensated = 1, kPrecFp64Merge = 2, kPrecFp64Pairs = 3, kPrecFp64MergeShared = 4 };
+
+// The FP64 sums of kPrecFp64MergeShared: after the TMA ring and its barriers in dynamic shared
+// memory, one double per point of every thread, point-major (thread t's point i at i * threads + t:
+// consecutive threads, consecutive words).
+__device__ __forceinline__ double* shared_sums(unsigned char* tiles)
+{
+    return reinterpret_cast<double*>(tiles + kStages * kTileAtoms * 16 + kStages * 8);
+}
+inline size_t shared_sums_bytes(int threads, int points) { return static_cast<size_t>(threads) * points * sizeof(double); }
 
 // Cluster sizes of the atom-split form: 2..8 are portable; 9..16 use the B200's non-portable
 // cluster sizes (opted into per kernel; refused with a device-limits error where the block does not fit).
@@ -159,7 +168,9 @@ __device__ __forceinline__ bool tile_accumulate(const FwdParams& p, const int x0
                   "z trimming: 3D maps, shared-memory atoms, FP32 pairs");
     static_assert(XP == 1 || XP == 2 || XP == 4 || XP == 8, "XP must be 1, 2, 4 or 8");
     // atoms per FP32 partial of the compensated / FP64-merge forms, and the ragged stage's granularity
-    constexpr int SUB = (PREC == kPrecCompensated || PREC == kPrecFp64Merge) ? kMergeAtoms : kSubTile;
+    constexpr int SUB =
+        (PREC == kPrecCompensated || PREC == kPrecFp64Merge || PREC == kPrecFp64MergeShared) ? kMergeAtoms : kSubTile;
+    static_assert(PREC != kPrecFp64MergeShared || SRC == kSrcShared, "shared-memory FP64 sums: TMA-staged atoms");
     static_assert(kTileAtoms % SUB == 0, "sub-tiles must divide the stage");
 
     float gx[XP];
@@ -206,6 +217,18 @@ __device__ __forceinline__ bool tile_accumulate(const FwdParams& p, const int x0
                 acc64[k][2 * i + 1] = 0.0;
             }
         }
+    // kPrecFp64MergeShared: this thread's FP64 sums in shared memory (thread-private slots, so no
+    // barrier); the same arithmetic as kPrecFp64Merge, with the registers of the sums freed
+    double* sums = nullptr;
+    int sum_tid = 0, sum_stride = 0;
+    if constexpr (PREC == kPrecFp64MergeShared) {
+        sums = shared_sums(tiles);
+        sum_tid = threadIdx.y * blockDim.x + threadIdx.x;
+        sum_stride = blockDim.x * blockDim.y;
+#pragma unroll
+        for (int q = 0; q < XP * ZI; ++q)
+            sums[q * sum_stride + sum_tid] = 0.0;
+    }
 
     // Fold a sub-tile partial into the accumulator of the chosen form.
     auto merge = [&]() {
@@ -222,6 +245,11 @@ __device__ __forceinline__ bool tile_accumulate(const FwdParams& p, const int x0
                 } else if constexpr (PREC == kPrecFp64Merge) {
                     acc64[k][2 * i] += static_cast<double>(part[k][i].x);
                     acc64[k][2 * i + 1] += static_cast<double>(part[k][i].y);
+                } else if constexpr (PREC == kPrecFp64MergeShared) {
+                    double* s0 = sums + (k * ZI + 2 * i) * sum_stride + sum_tid;
+                    *s0 += static_cast<double>(part[k][i].x);
+                    if (2 * i + 1 < ZI)
+                        s0[sum_stride] += static_cast<double>(part[k][i].y);
                 }
             }
     };
@@ -401,6 +429,8 @@ __device__ __forceinline__ bool tile_accumulate(const FwdParams& p, const int x0
                 val[k][m] = static_cast<float>(accd[k][m]);
             else if constexpr (PREC == kPrecCompensated)
                 val[k][m] = lane(acc[k][m / 2], m & 1) + lane(cmp[k][m / 2], m & 1);
+            else if constexpr (PREC == kPrecFp64MergeShared)
+                val[k][m] = static_cast<float>(sums[(k * ZI + m) * sum_stride + sum_tid]);
             else
                 val[k][m] = static_cast<float>(acc64[k][m]);
         }
@@ -408,6 +438,9 @@ __device__ __forceinline__ bool tile_accumulate(const FwdParams& p, const int x0
     (void)cmp;
     (void)acc64;
     (void)accd;
+    (void)sums;
+    (void)sum_tid;
+    (void)sum_stride;
     return true;
 }
 
@@ -447,9 +480,17 @@ __device__ __forceinline__ bool tile_pass(const FwdParams& p, const int x0, cons
     return true;
 }
 
+// Resident 256-thread blocks the register budget of fwd_kernel is sized for: with its FP64 sums in
+// shared memory a thread of up to 16 points fits in 51 registers (five such blocks per SM); otherwise
+// the compiler's choice.
+constexpr int fwd_min_blocks(const int prec, const int points)
+{
+    return prec == kPrecFp64MergeShared && points <= 16 ? 5 : 1;
+}
+
 // One tile per CTA: the block's position in the launch grid selects the tile.
 template <int ZI, int XP, int UNR, int SRC, int SOA, int PREC, int SOFT, int MODE>
-__global__ void __launch_bounds__(kMaxThreads) fwd_kernel(const FwdParams p, const int vec_ok)
+__global__ void __launch_bounds__(kMaxThreads, fwd_min_blocks(PREC, XP * ZI)) fwd_kernel(const FwdParams p, const int vec_ok)
 {
     const int x0 = (blockIdx.x * blockDim.x + threadIdx.x) * XP;
     int yrow, z0;
@@ -1023,6 +1064,12 @@ cudaError_t launch_fwd(const FwdLaunch& L, cudaStream_t stream)
         } while (off < n);
         return cudaSuccess;
     } else {
+        if (L.smem > 48u * 1024u) {
+            const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                       static_cast<int>(L.smem));
+            if (e != cudaSuccess)
+                return e;
+        }
         kernel<<<L.grid, L.block, L.smem, stream>>>(L.p, L.vec_store);
         return cudaGetLastError();
     }
@@ -1142,6 +1189,7 @@ void register_fwd_3d_precise(std::vector<VariantEntry>& v);
 void register_fwd_3d_soft(std::vector<VariantEntry>& v);
 void register_fwd_3d_soft_precise(std::vector<VariantEntry>& v);
 void register_fwd_3d_soft_fp64m(std::vector<VariantEntry>& v);
+void register_fwd_3d_soft_fp64s(std::vector<VariantEntry>& v);
 void register_fwd_3d_fp64(std::vector<VariantEntry>& v);
 void register_fwd_2d(std::vector<VariantEntry>& v);
 void register_fwd_split(std::vector<VariantEntry>& v);

@@ -293,3 +293,27 @@ def test_fp64_pair_variants_on_a_ragged_grid(ctx):
         assert rep["rel_point"] <= 2e-7, (tune.as_dict(), rep)
         count += 1
     assert count >= 16
+
+
+@pytest.mark.parametrize("tune", [
+    dict(block_x=32, block_y=1, z_iterations=8, x_points=2, unroll=2, rsqrt_soft=2),
+    dict(block_x=32, block_y=4, z_iterations=8, x_points=2, unroll=1, rsqrt_soft=12),
+    dict(block_x=64, block_y=2, z_iterations=16, x_points=1, unroll=1, rsqrt_soft=0),
+    dict(block_x=16, block_y=8, z_iterations=4, x_points=4, unroll=1, rsqrt_soft=3),
+])
+def test_fp64_merge_shared_sums_equal_register_sums(ctx, tune):
+    """The FP64 merge with its sums in shared memory is the same arithmetic as with the sums in
+    registers: the maps agree bit for bit, and both meet the FP64 oracle."""
+    import torch
+    rng = np.random.default_rng(41)
+    a = np.zeros((5000, 4), dtype=np.float32)
+    a[:, :3] = rng.uniform(0.0, 30.0, (5000, 3))
+    a[:, 3] = rng.uniform(-1.0, 1.0, 5000)
+    dims, h, origin = (61, 37, 45), 0.5, (0.3, -0.2, 1.0)
+    atoms = torch.from_numpy(a).cuda()
+    reg = ctx.forward_3d(atoms, dims, h, origin, tune=ktt_b200.Tune(precision=ktt_b200.PREC_FP64_MERGE, **tune))
+    shr = ctx.forward_3d(atoms, dims, h, origin,
+                         tune=ktt_b200.Tune(precision=ktt_b200.PREC_FP64_MERGE_SHARED, **tune))
+    assert torch.equal(reg, shr)
+    ref = oracle.grid3d(a, h, dims, origin)
+    assert errors.report(shr.cpu().numpy(), ref)["rel_norm"] <= 1e-5
