@@ -83,7 +83,8 @@ def _fast_fp32_tune():
 
 
 def _dtype(tune) -> str:
-    return {0: "f32", 1: "f32 pairs, compensated f32 sums", 2: "f32 pairs, f64 merge", 3: "f64 pairs"}[tune.precision]
+    return {0: "f32", 1: "f32 pairs, compensated f32 sums", 2: "f32 pairs, f64 merge", 3: "f64 pairs",
+            4: "f32 pairs, f64 merge (sums in shared memory)"}[tune.precision]
 
 
 def _soft_share(tune) -> float:

@@ -16,7 +16,8 @@
 //     VECTOR_SIZE (3D) / OUTER_UNROLL_FACTOR (2D) -> points per thread along x,
 //     INNER_UNROLL_FACTOR -> atom-loop unroll, USE_CONSTANT_MEMORY -> atom source,
 //     USE_SOA -> which argument layout the 3D kernel reads,
-// plus the B200 parameters PRECISION (0 FP32, 1 compensated, 2 FP64 merge, 3 FP64 pairs),
+// plus the B200 parameters PRECISION (0 FP32, 1 compensated, 2 FP64 merge, 3 FP64 pairs, 4 FP64 merge with
+// the sums in shared memory),
 // RSQRT_SOFT (share of reciprocal square roots on the FMA pipe, of 8), ATOM_SPLIT (2 or more: the
 // atoms are split into that many chunks per point tile) and SPLIT_FORM (0: a thread-block cluster
 // of ATOM_SPLIT CTAs shares each tile, 2..16; 1: a persistent grid takes (tile, chunk) items from a

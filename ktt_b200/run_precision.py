@@ -6,7 +6,7 @@ clustered: 65,536 atoms in 64 Gaussian clusters (sigma 2 A, centres uniform in t
 charges +1/-1 alternating within each cluster plus N(0, 0.01), total charge exactly zero; uniform:
 the benchmark's map (65,536 atoms uniform in the 128 A cube, q ~ U[-1, 1]); 256^3 grid at 0.5 A.
 Each form (FP32 accumulation, compensated two-sum, FP64 merge -- MUFU-only and with part of the
-rsqrts on the FMA pipe -- and FP64 pairs) is timed on the device (best of --repeat) and compared with
+rsqrts on the FMA pipe, and with the FP64 sums in shared memory -- and FP64 pairs) is timed on the device (best of --repeat) and compared with
 the FP64 oracle on a seeded subset of grid points.  Prints one JSON line per form: device time, pair
 rate, max abs error, max error / max |V| (rel_norm), rms error / rms V (rel_rms), the pointwise
 error max |dV| / max(|V|, floor) at the gate floor rms(V) (rel_point), at 0.1 rms(V) and at the strict
@@ -28,6 +28,7 @@ FORMS = (
     ("compensated_soft2", dict(precision=1, rsqrt_soft=2)),
     ("fp64_merge", dict(precision=2, rsqrt_soft=0)),
     ("fp64_merge_soft2", dict(precision=2, rsqrt_soft=2)),
+    ("fp64_merge_shared_soft2", dict(precision=4, rsqrt_soft=2)),
     ("fp64_pairs", dict(precision=3, rsqrt_soft=0)),
 )
 

@@ -221,7 +221,8 @@ def test_full_map_uniform_subset(ctx):
     idx = workloads.subset_indices(total, 0.001)
     ref, sabs = oracle.points3d(w.atoms, w.spacing, w.dims, idx, want_sumabs=True)
     bench_form = ktt_b200.tuned("b200_map3d")
-    assert bench_form is not None and bench_form.precision in (ktt_b200.PREC_COMPENSATED, ktt_b200.PREC_FP64_MERGE)
+    assert bench_form is not None and bench_form.precision in (ktt_b200.PREC_COMPENSATED, ktt_b200.PREC_FP64_MERGE,
+                                                               ktt_b200.PREC_FP64_MERGE_SHARED)
     forms = [(ktt_b200.Tune(), "norm"),
              (ktt_b200.Tune(precision=ktt_b200.PREC_FP64_MERGE, z_iterations=8), "point"),
              (bench_form, "point"),
@@ -241,8 +242,8 @@ def test_full_map_uniform_subset(ctx):
 def test_precision_forms_on_the_clustered_map(ctx):
     """The cancellation-heavy map (65,536 atoms in 64 Gaussian clusters of alternating +1/-1 charges,
     net charge 0, sum |q|/r about 1000 |V|; 256^3 grid) against FP64 on a seeded 0.1% subset.  The
-    compensated and FP64-merge forms -- all rsqrts on MUFU, 2/8 on the FMA pipe, and the alternating
-    5/16 share -- meet the gate (1e-5 normwise and pointwise at the floor rms(V*)); FP64 pairs meet
+    compensated and FP64-merge forms (FP64 sums in registers or in shared memory) -- all rsqrts on
+    MUFU, 2/8 on the FMA pipe, and the alternating 5/16 share -- meet the gate (1e-5 normwise and pointwise at the floor rms(V*)); FP64 pairs meet
     1e-5 pointwise at the strict floor (1e-3 rms(V*)); FP32 accumulation, with or without the FMA-pipe
     share, misses the pointwise gate, which is why the precise forms exist."""
     w = workloads.clustered_map()
@@ -251,7 +252,8 @@ def test_precision_forms_on_the_clustered_map(ctx):
     idx = workloads.subset_indices(total, 0.001, seed=23)
     ref, sabs = oracle.points3d(w.atoms, w.spacing, w.dims, idx, want_sumabs=True)
     tile = dict(block_x=64, block_y=1, z_iterations=8, x_points=2, unroll=2)
-    precise = [dict(precision=p, rsqrt_soft=s) for p in (ktt_b200.PREC_COMPENSATED, ktt_b200.PREC_FP64_MERGE)
+    precise = [dict(precision=p, rsqrt_soft=s) for p in (ktt_b200.PREC_COMPENSATED, ktt_b200.PREC_FP64_MERGE,
+                                                          ktt_b200.PREC_FP64_MERGE_SHARED)
                for s in (0, 2, 12)]
     reports = {}
     for fields in precise + [dict(precision=ktt_b200.PREC_FP32, rsqrt_soft=s) for s in (0, 2)]:
