@@ -743,7 +743,7 @@ constexpr int kBalAtomStep = 8;       // a group's atoms are evaluated in steps 
 // The balanced form's split of the T x N unit space over B CTAs: q = U / B units per CTA, the first
 // r = U % B CTAs one more.  start(b) = b q + min(b, r); cta_of(u) inverts it.
 struct BalanceSplit {
-    int64_t n, q, r;
+    int64_t q, r;
     __host__ __device__ int64_t start(int64_t b) const { return b * q + (b < r ? b : r); }
     __host__ __device__ int64_t cta_of(int64_t u) const
     {
@@ -806,7 +806,7 @@ __global__ void __launch_bounds__(kBalThreads, 1) balanced_split_kernel(const Fw
     // This CTA's units [u_begin, u_end): from atom a_begin of tile t_begin to atom a_stop - 1 of tile
     // t_end.  Its pieces: tile t_begin from a_begin, the tiles between whole, tile t_end up to a_stop.
     const int64_t b = blockIdx.x;
-    const BalanceSplit split{N, static_cast<int64_t>(tiles) * N / gridDim.x, static_cast<int64_t>(tiles) * N % gridDim.x};
+    const BalanceSplit split{static_cast<int64_t>(tiles) * N / gridDim.x, static_cast<int64_t>(tiles) * N % gridDim.x};
     const int64_t u_begin = split.start(b);
     const int64_t u_last = split.start(b + 1) - 1;
     const int t_begin = static_cast<int>(u_begin / N);
