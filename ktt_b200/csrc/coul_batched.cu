@@ -52,6 +52,9 @@ static const std::vector<BatchVariant>& batch_variants()
         batch_variant<16, 1, 2, kPrecFp32, 2>(),     batch_variant<16, 1, 1, kPrecFp32, kSoftAlternate + 2>(),
         batch_variant<16, 1, 2, kPrecFp32, kSoftAlternate + 2>(), batch_variant<8, 1, 1, kPrecFp32, kSoftAlternate + 2>(),
         batch_variant<16, 1, 1, kPrecFp64Merge, 2>(),
+        // FP64 merge with the sums in shared memory (the pointwise-accurate form with fewer registers)
+        batch_variant<8, 2, 1, kPrecFp64MergeShared, 2>(), batch_variant<8, 2, 2, kPrecFp64MergeShared, 2>(),
+        batch_variant<16, 1, 1, kPrecFp64MergeShared, 2>(),
     };
     return v;
 }
@@ -212,6 +215,14 @@ COUL_API int coul_batch_create(coul_ctx* ctx, const coul_molecule* molecules, in
     cudaError_t e;
     int blocks_per_sm = 0;
     b->smem = kStages * kTileAtoms * 16 + kStages * 8;
+    if (b->tune.precision == COUL_PREC_FP64_MERGE_SHARED)
+        b->smem += shared_sums_bytes(threads, b->tune.z_iterations * b->tune.x_points);
+    if (b->smem > 48u * 1024u &&
+        (e = cudaFuncSetAttribute(b->variant->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(b->smem))) != cudaSuccess) {
+        batch_release(b);
+        return cuda_error(e, "batched kernel shared memory");
+    }
     if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, b->variant->kernel, threads, b->smem)) !=
             cudaSuccess ||
         blocks_per_sm < 1) {

@@ -83,7 +83,7 @@ struct BatchParams {
 // One CTA per resident slot; each claims (molecule, tile) work items from b.counter until the
 // queue is empty and runs them through tile_pass, the TMA atom ring carrying over between items.
 template <int ZI, int XP, int UNR, int PREC, int SOFT>
-__global__ void __launch_bounds__(kMaxThreads) batched_kernel(const BatchParams b)
+__global__ void __launch_bounds__(kMaxThreads, fwd_min_blocks(PREC, XP * ZI)) batched_kernel(const BatchParams b)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + kStages * kTileAtoms * 16);

@@ -90,3 +90,31 @@ def test_batch_outlives_its_context():
     lib = ktt_b200.load_library()
     assert lib.coul_batch_run(None, kept._handle, ktt_b200.BATCH_PERSISTENT, 0) == ktt_b200.COUL_ERR_INVALID_ARGUMENT
     kept.close()
+
+
+def test_precise_batch_with_shared_sums(ctx):
+    """The batch in the FP64-merge form with its sums in shared memory: bit-identical to the same form
+    with register sums and to one forward launch per molecule, and within the pointwise gate of the
+    FP64 oracle."""
+    import torch
+    mols = _small_batch(seed=25, n_mol=8)
+    inputs = [(torch.from_numpy(m.atoms).cuda(), m.dims, m.spacing, m.origin) for m in mols]
+    maps = {}
+    for prec in (ktt_b200.PREC_FP64_MERGE, ktt_b200.PREC_FP64_MERGE_SHARED):
+        tune = ktt_b200.Tune(block_x=8, block_y=4, z_iterations=8, x_points=2, rsqrt_soft=2, precision=prec)
+        b = ktt_b200.Batch(ctx, inputs, tune)
+        for mode in (ktt_b200.BATCH_PERSISTENT, ktt_b200.BATCH_SEPARATE):
+            b.run(mode)
+            ctx.synchronize()
+            maps[(prec, mode)] = [o.cpu().numpy().copy() for o in b.outputs]
+        b.close()
+    ref_maps = maps[(ktt_b200.PREC_FP64_MERGE, ktt_b200.BATCH_PERSISTENT)]
+    for key, got in maps.items():
+        for a, r in zip(got, ref_maps):
+            assert np.array_equal(a.view(np.uint32), r.view(np.uint32)), key
+    for m, out in zip(mols, maps[(ktt_b200.PREC_FP64_MERGE_SHARED, ktt_b200.BATCH_PERSISTENT)]):
+        total = int(np.prod(m.dims))
+        idx = workloads.subset_indices(total, min(1.0, 3000 / total), seed=6)
+        ref, sabs = oracle.points3d(m.atoms, m.spacing, m.dims, idx, origin=m.origin, want_sumabs=True)
+        rep = errors.gate(out.reshape(-1)[idx], ref, sumabs=sabs)
+        assert rep["passes_norm"] and rep["passes_point"], rep
