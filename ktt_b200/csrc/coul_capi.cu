@@ -301,6 +301,32 @@ struct SplitWorkspace {
     int64_t balanced_clean_ctas = 0;
 };
 
+// Resident blocks per SM of a persistent form's kernel for this block size and dynamic shared memory.
+// The kernel's dynamic shared-memory attribute is only ever raised (never lowered, by any context
+// object sharing the CUDA context), so every size launched before stays launchable.  Queried once per
+// context object and kept: on the host these calls cost microseconds, which a call's event pair would
+// otherwise count while the GPU waits for the launch.
+static int resident_blocks(coul_ctx* ctx, const void* kernel, int threads, size_t smem, int* blocks)
+{
+    for (const auto& o : ctx->occupancy_cache)
+        if (o.kernel == kernel && o.threads == threads && o.smem == smem) {
+            *blocks = o.blocks_per_sm;
+            return COUL_OK;
+        }
+    cudaError_t e;
+    cudaFuncAttributes fa{};
+    if ((e = cudaFuncGetAttributes(&fa, kernel)) != cudaSuccess)
+        return cuda_error(e, "kernel attributes");
+    if (smem > static_cast<size_t>(fa.maxDynamicSharedSizeBytes) &&
+        (e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem))) !=
+            cudaSuccess)
+        return cuda_error(e, "persistent form shared memory");
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, kernel, threads, smem)) != cudaSuccess)
+        return cuda_error(e, "occupancy query");
+    ctx->occupancy_cache.push_back(coul_ctx::Occupancy{kernel, threads, smem, *blocks});
+    return COUL_OK;
+}
+
 // Grow the context's split workspace to `need` bytes (drains the stream before freeing the old one).
 static int split_workspace(coul_ctx* ctx, size_t need, unsigned char** base)
 {
@@ -348,13 +374,9 @@ int balanced_split_setup(coul_ctx* ctx, const VariantEntry* v, FwdLaunch& L, con
     L.smem = static_cast<size_t>(kStages) * kBalStageAtoms * 16 + kStages * 8 +
              static_cast<size_t>(groups * values) * sizeof(float);
     cudaError_t e;
-    if ((e = cudaFuncSetAttribute(v->occupancy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  static_cast<int>(L.smem))) != cudaSuccess)
-        return cuda_error(e, "balanced form shared memory");
     int blocks_per_sm = 0;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, v->occupancy_kernel, threads, L.smem)) !=
-        cudaSuccess)
-        return cuda_error(e, "occupancy query");
+    if (const int rc_occ = resident_blocks(ctx, v->occupancy_kernel, threads, L.smem, &blocks_per_sm))
+        return rc_occ;
     if (blocks_per_sm < 1)
         return set_error(COUL_ERR_DEVICE_LIMITS, "the balanced form's block does not fit on an SM");
     // every CTA resident, at least one unit each
@@ -405,9 +427,8 @@ int queue_split_setup(coul_ctx* ctx, const VariantEntry* v, FwdLaunch& L, const 
     if ((e = cudaMemsetAsync(base + done_offset, 0, need - done_offset, ctx->stream)) != cudaSuccess)
         return cuda_error(e, "queue counters reset");
     int blocks_per_sm = 0;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, v->occupancy_kernel, threads, L.smem)) !=
-        cudaSuccess)
-        return cuda_error(e, "occupancy query");
+    if (const int rc_occ = resident_blocks(ctx, v->occupancy_kernel, threads, L.smem, &blocks_per_sm))
+        return rc_occ;
     if (blocks_per_sm < 1)
         return set_error(COUL_ERR_DEVICE_LIMITS, "the queue form's block does not fit on an SM");
     L.queue.partial = reinterpret_cast<float*>(base);

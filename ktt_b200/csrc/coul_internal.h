@@ -32,6 +32,13 @@ struct coul_ctx {
     void* adjoint_workspace = nullptr;            // FP64 partials of coul_adjoint_3d (coul_adjoint.cu)
     void* split_workspace_state = nullptr;        // partial blocks and counters of the queue and balanced forms
     std::vector<coul_batch*> batches;             // live batches (their device resources go with the context)
+    struct Occupancy {
+        const void* kernel;
+        int threads;
+        size_t smem;
+        int blocks_per_sm;
+    };
+    std::vector<Occupancy> occupancy_cache;       // persistent forms' resident blocks (coul_capi.cu)
 };
 
 namespace coul {
