@@ -317,6 +317,10 @@ static int resident_blocks(coul_ctx* ctx, const void* kernel, int threads, size_
     cudaFuncAttributes fa{};
     if ((e = cudaFuncGetAttributes(&fa, kernel)) != cudaSuccess)
         return cuda_error(e, "kernel attributes");
+    if (threads > fa.maxThreadsPerBlock)
+        return set_error(COUL_ERR_DEVICE_LIMITS, "a block of " + std::to_string(threads) +
+                                                     " threads exceeds this variant's launch bound of " +
+                                                     std::to_string(fa.maxThreadsPerBlock));
     if (smem > static_cast<size_t>(fa.maxDynamicSharedSizeBytes) &&
         (e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem))) !=
             cudaSuccess)
