@@ -221,3 +221,28 @@ def test_balanced_split_counters_across_forms_and_grids(ctx):
         if key in first:
             assert torch.equal(got, first[key])
         first.setdefault(key, got)
+
+
+def test_balanced_split_alternating_sizes_and_contexts(ctx):
+    """The persistent forms keep their occupancy per context and only ever raise a kernel's shared
+    memory limit: configurations of one kernel with large and small shared memory, alternated within a
+    context and across two contexts on the same device, all stay launchable and exact."""
+    import torch
+    a = _atoms(2100, seed=29)
+    dims, h = (45, 31, 26), 0.5
+    atoms = torch.from_numpy(a).cuda()
+    ref = oracle.grid3d(a, h, dims)
+    big = ktt_b200.Tune(block_x=64, block_y=1, z_iterations=8, x_points=2, rsqrt_soft=2, atom_split=16, split_form=2)
+    small = ktt_b200.Tune(block_x=32, block_y=1, z_iterations=8, x_points=2, rsqrt_soft=2, atom_split=2, split_form=2)
+    other = ktt_b200.CoulombContext(0)
+    try:
+        first = {}
+        for c, tune in ((ctx, big), (ctx, small), (other, small), (ctx, big), (other, big), (ctx, small)):
+            got = c.forward_3d(atoms, dims, h, tune=tune)
+            assert errors.report(got.cpu().numpy(), ref)["rel_norm"] <= TOL
+            key = tune.atom_split
+            if key in first:
+                assert torch.equal(got, first[key])
+            first.setdefault(key, got)
+    finally:
+        other.close()
