@@ -12,35 +12,23 @@ struct MolDesc {
     float* out;
     int64_t tile_begin;  // first work item of this molecule
     int nx, ny, nz;
-    int tiles_x, tiles_y;
-    int tx;              // threads of a CTA along x for this molecule's tiles (the rest along y);
-                         // 0: linear tiles (one x-y point per thread, consecutive in the x-y plane)
+    int tiles_x, tiles_y;  // x-y tiles (tiles_y is 1: the x-y tiles are linear)
+    int pitch;             // row length of the x-y numbering: nx rounded up to a multiple of x_points
     int vec_ok;
     float h, ox, oy, oz;
 };
 
-// Tile geometry of one molecule.  With one x point per thread (x_points 1) the tiles are linear:
-// thread i of x-y tile j takes the point j * threads + i of the grid's x-y plane in row-major order,
-// so only the plane's last tile is padded.  Otherwise the CTA threads are arranged as
-// tx x (threads / tx), tx the power of two dividing the thread count whose tile pads the grid's x-y
-// plane least (ties: the block's own x size).  The arrangement only moves points between threads;
-// every point is computed the same way.  Returns the molecule's work items.
+// Tile geometry of one molecule.  The x-y tiles are linear: the plane is numbered row by row with
+// rows of `pitch` points (nx rounded up to a multiple of x_points, so a thread's x_points points never
+// cross a row), and thread i of x-y tile j takes the x_points points from (j * threads + i) * x_points.
+// Only the plane's last tile, and for an nx that x_points does not divide the padding column(s), hold
+// points outside the grid (evaluated, not stored).  Each point keeps its position x mod x_points in
+// its thread, so it is computed exactly as in a one-CTA-per-tile launch.  Returns the molecule's work
+// items.
 inline int64_t fill_mol_desc(MolDesc& d, const coul_molecule& m, const coul_tune& t)
 {
     const int threads = t.block_x * t.block_y;
-    int best_tx = t.block_x;
-    int64_t best_area = -1;
-    for (int tx = 1; tx <= threads && t.x_points > 1; tx *= 2) {
-        if (threads % tx)
-            continue;
-        const int64_t sx = static_cast<int64_t>(tx) * t.x_points;
-        const int64_t sy = threads / tx;
-        const int64_t area = (m.grid.nx + sx - 1) / sx * sx * ((m.grid.ny + sy - 1) / sy * sy);
-        if (best_area < 0 || area < best_area || (area == best_area && tx == t.block_x)) {
-            best_area = area;
-            best_tx = tx;
-        }
-    }
+    const int xp = t.x_points;
     d.atoms = reinterpret_cast<const float4*>(m.d_atoms);
     d.n_atoms = m.n_atoms;
     d.out = m.d_out;
@@ -51,24 +39,16 @@ inline int64_t fill_mol_desc(MolDesc& d, const coul_molecule& m, const coul_tune
     d.ox = m.grid.origin[0];
     d.oy = m.grid.origin[1];
     d.oz = m.grid.origin[2];
-    if (t.x_points == 1) {
-        d.tx = 0;
-        d.tiles_x = static_cast<int>((static_cast<int64_t>(m.grid.nx) * m.grid.ny + threads - 1) / threads);
-        d.tiles_y = 1;
-    } else {
-        d.tx = best_tx;
-        const int64_t span_x = static_cast<int64_t>(best_tx) * t.x_points;
-        const int ty = threads / best_tx;
-        d.tiles_x = static_cast<int>((m.grid.nx + span_x - 1) / span_x);
-        d.tiles_y = (m.grid.ny + ty - 1) / ty;
-    }
+    d.pitch = (m.grid.nx + xp - 1) / xp * xp;
+    const int64_t span = static_cast<int64_t>(threads) * xp;
+    d.tiles_x = static_cast<int>((static_cast<int64_t>(d.pitch) * m.grid.ny + span - 1) / span);
+    d.tiles_y = 1;
     const int tiles_z = (m.grid.nz + t.z_iterations - 1) / t.z_iterations;
-    const int xp = t.x_points;
     d.vec_ok = (xp > 1 && m.grid.nx % xp == 0 &&
                 (reinterpret_cast<uintptr_t>(m.d_out) % (sizeof(float) * (xp >= 4 ? 4 : xp))) == 0)
                    ? 1
                    : 0;
-    return static_cast<int64_t>(d.tiles_x) * d.tiles_y * tiles_z;
+    return static_cast<int64_t>(d.tiles_x) * tiles_z;
 }
 
 struct BatchParams {
@@ -113,9 +93,7 @@ __global__ void __launch_bounds__(kMaxThreads, fwd_min_blocks(PREC, XP * ZI)) ba
         const MolDesc m = b.mols[lo];
         const long long local = item - m.tile_begin;
         const int tile_x = static_cast<int>(local % m.tiles_x);
-        const long long rest = local / m.tiles_x;
-        const int tile_y = static_cast<int>(rest % m.tiles_y);
-        const int tile_z = static_cast<int>(rest / m.tiles_y);
+        const int tile_z = static_cast<int>(local / m.tiles_x);
 
         FwdParams p{};
         p.atoms = m.atoms;
@@ -130,17 +108,11 @@ __global__ void __launch_bounds__(kMaxThreads, fwd_min_blocks(PREC, XP * ZI)) ba
         p.out = m.out;
         p.accumulate = b.accumulate;
         p.status = b.status;
-        int x0, yrow;
-        if (XP == 1 && m.tx == 0) {
-            // linear tile: plane points beyond the last row land at y >= ny (evaluated, not stored)
-            const int64_t q = static_cast<int64_t>(tile_x) * (blockDim.x * blockDim.y) + tid;
-            x0 = static_cast<int>(q % m.nx);
-            yrow = static_cast<int>(q / m.nx);
-        } else {
-            const int ty = static_cast<int>(blockDim.x * blockDim.y) / m.tx;
-            x0 = (tile_x * m.tx + tid % m.tx) * XP;
-            yrow = tile_y * ty + tid / m.tx;
-        }
+        // linear x-y tile: points past the plane's last row land at y >= ny, padding columns at
+        // x >= nx (evaluated, not stored)
+        const int64_t p0 = (static_cast<int64_t>(tile_x) * (blockDim.x * blockDim.y) + tid) * XP;
+        const int x0 = static_cast<int>(p0 % m.pitch);
+        const int yrow = static_cast<int>(p0 / m.pitch);
         const int z0 = tile_z * ZI;
         // tiles that overhang the molecule's grid in z evaluate only their points inside it
         if (!tile_pass<ZI, XP, UNR, kSrcShared, 0, PREC, SOFT, kModeGrid3d, true>(p, x0, yrow, z0, m.vec_ok,
