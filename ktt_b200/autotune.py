@@ -202,10 +202,11 @@ def tune_map3d(grid: int = 256, atoms: int = 65536, searcher: str = "mcmc", budg
 
 def tune_batch(molecules: int = 512, seed: int = 4, searcher: str = "mcmc", budget: int = 40,
                dry_run: bool = False, profile: bool = False, results_path: str = "", model: str = "",
-               search_seed: int | None = None, reference=None, reference_name: str = "") -> dict:
+               search_seed: int | None = None, reference=None, reference_name: str = "",
+               precisions=(0,)) -> dict:
     """Searches the batched-map tile space (the coulombBatch definition) on the uneven molecule batch
-    (`molecules` molecules of 200-20000 atoms, log-uniform, from `seed`); reference as in tune_map3d,
-    applied to every molecule."""
+    (`molecules` molecules of 200-20000 atoms, log-uniform, from `seed`) over the accumulation forms
+    `precisions`; reference as in tune_map3d, applied to every molecule."""
     import ktt_b200
     from ktt_b200 import pyktt as ktt
     from ktt_b200 import workloads
@@ -214,7 +215,7 @@ def tune_batch(molecules: int = 512, seed: int = 4, searcher: str = "mcmc", budg
     tuner.SetGlobalSizeType(ktt.GlobalSizeType.CUDA)
     definition = tuner.AddKernelDefinition("coulombBatch", "", ktt.DimensionVector(1, 1, 2), ktt.DimensionVector())
     kernel = tuner.CreateSimpleKernel("CoulombBatch", definition)
-    _add_space(ktt, tuner, kernel, definition, BATCH_SPACE, ktt_b200.batch_tune_supported, (0,))
+    _add_space(ktt, tuner, kernel, definition, BATCH_SPACE, ktt_b200.batch_tune_supported, precisions)
     if dry_run:
         return {"configurations": tuner.GetConfigurationsCount(kernel)}
 
@@ -252,6 +253,7 @@ def tune_batch(molecules: int = 512, seed: int = 4, searcher: str = "mcmc", budg
         "batched": _tune_from([best["config"][k] for k in list(BATCH_SPACE) + ["PRECISION"]],
                               list(BATCH_SPACE) + ["PRECISION"]).as_dict(),
         "batched_gpairs_per_s": round(best["gpairs_per_s"], 1),
+        "precisions": list(precisions),
         "workload": f"{len(mols)} molecules, seed {seed}, margin 8 A per side",
         "source": f"ktt_b200.autotune batch: {searcher} searcher, {len(results)} of "
                   f"{tuner.GetConfigurationsCount(kernel)} configurations of the coulombBatch definition",
@@ -274,7 +276,7 @@ def main() -> None:
     ap.add_argument("--molecules", type=int, default=512)
     ap.add_argument("--seed", type=int, default=4)
     ap.add_argument("--dry-run", action="store_true", help="report the configuration space only")
-    ap.add_argument("--precisions", default="0", help="accumulation forms to search (map3d), e.g. 1,2")
+    ap.add_argument("--precisions", default="0", help="accumulation forms to search, e.g. 2,4")
     ap.add_argument("--save", action="store_true", help="write ktt_b200/tuned/b200_<target>.json")
     ap.add_argument("--out", default="", help="write the result to this file instead")
     args = ap.parse_args()
@@ -288,7 +290,8 @@ def main() -> None:
                             precisions=tuple(int(p) for p in args.precisions.split(",")))
     else:
         result = tune_batch(args.molecules, args.seed, args.searcher, args.budget, args.dry_run, args.profile,
-                            args.results, args.model, args.search_seed)
+                            args.results, args.model, args.search_seed,
+                            precisions=tuple(int(p) for p in args.precisions.split(",")))
     print(json.dumps({k: v for k, v in result.items() if k != "trials"}))
     path = args.out or (os.path.join(TUNED, "b200_map3d.json" if args.target == "map3d" else "b200_batch.json")
                         if args.save else "")
@@ -296,9 +299,11 @@ def main() -> None:
         if args.target == "batch" and os.path.exists(path):
             with open(path) as f:
                 previous = json.load(f)
-            # keep the KTT-form baseline tile the batch measurement compares against
-            if "ktt_form" in previous:
-                result["ktt_form"] = previous["ktt_form"]
+            # keep the KTT-form baseline tile the batch measurement compares against, and the fastest
+            # FP32 tile of an earlier search
+            for key in ("ktt_form", "fast_fp32"):
+                if key in previous:
+                    result[key] = previous[key]
         with open(path, "w") as f:
             json.dump(result, f, indent=1)
             f.write("\n")

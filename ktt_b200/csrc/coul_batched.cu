@@ -54,7 +54,7 @@ static const std::vector<BatchVariant>& batch_variants()
         batch_variant<16, 1, 1, kPrecFp64Merge, 2>(),
         // FP64 merge with the sums in shared memory (the pointwise-accurate form with fewer registers)
         batch_variant<8, 2, 1, kPrecFp64MergeShared, 2>(), batch_variant<8, 2, 2, kPrecFp64MergeShared, 2>(),
-        batch_variant<16, 1, 1, kPrecFp64MergeShared, 2>(),
+        batch_variant<16, 1, 1, kPrecFp64MergeShared, 2>(), batch_variant<4, 4, 1, kPrecFp64MergeShared, 2>(),
     };
     return v;
 }

@@ -1,6 +1,6 @@
 """Measure the batched persistent path on the uneven-molecule batch.
 
-    python -m ktt_b200.run_batch [--molecules 512] [--repeat 3] [--margin 8] [--set field=value ...]
+    python -m ktt_b200.run_batch [--molecules 512] [--repeat 3] [--margin 8] [--fast-fp32] [--set field=value ...]
     python -m ktt_b200.run_batch --autotune-ktt-form [--save ktt_b200/tuned/b200_batch.json]
 
 512 molecules with atom counts log-uniform in [200, 20000] (seeded), atoms uniform in a cube of side
@@ -12,7 +12,8 @@ launches), and one synchronous launch per molecule of KTT's plain reference kern
 (directCoulombSumReference: one point per thread, Examples/CoulombSum3d/CoulombSum3dReference.cu).
 
 The batched kernel's tile comes from `python -m ktt_b200.autotune batch` (KTT's searchers over the
-tuner's coulombBatch definition), stored under "batched"; --autotune-ktt-form searches the KTT-form
+tuner's coulombBatch definition), stored under "batched" (the pointwise-accurate FP64-merge form) and,
+for FP32 accumulation, under "fast_fp32" (--fast-fp32 measures that one); --autotune-ktt-form searches the KTT-form
 baseline's (z_iterations, x_points, CTA shape) exhaustively on the batch and stores it under
 "ktt_form", so both arms run at their best tile shape.
 """
@@ -70,6 +71,7 @@ def main() -> None:
     ap.add_argument("--margin", type=float, default=8.0, help="A of margin on every side of the bounding box")
     ap.add_argument("--set", action="append", default=[], metavar="FIELD=VALUE")
     ap.add_argument("--autotune-ktt-form", action="store_true")
+    ap.add_argument("--fast-fp32", action="store_true", help="the FP32-accumulation tile of the tuned file")
     ap.add_argument("--save", default="", help="write the tuned configurations, with the new ktt_form, to this file")
     ap.add_argument("--tuned", default=DEFAULT_TUNED, help="tuned configurations to start from")
     args = ap.parse_args()
@@ -98,8 +100,11 @@ def main() -> None:
             with open(args.save, "w") as f:
                 json.dump(tuned, f, indent=1)
                 f.write("\n")
-    tune = ktt_b200.Tune(**tuned.get("batched", {})) if tuned else \
-        ktt_b200.Tune(block_x=8, block_y=16, z_iterations=8, x_points=2, unroll=2, rsqrt_soft=2)
+    if args.fast_fp32 and "fast_fp32" in tuned:
+        tune = ktt_b200.Tune(**tuned["fast_fp32"]["batched"])
+    else:
+        tune = ktt_b200.Tune(**tuned.get("batched", {})) if tuned else \
+            ktt_b200.Tune(block_x=8, block_y=16, z_iterations=8, x_points=2, unroll=2, rsqrt_soft=2)
     ktt_tune = ktt_b200.Tune(**tuned["ktt_form"]) if "ktt_form" in tuned else \
         ktt_b200.Tune(block_x=32, block_y=4, z_iterations=8, x_points=2, atom_source=ktt_b200.ATOMS_CONSTANT)
     for s in args.set:
