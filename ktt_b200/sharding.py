@@ -1,4 +1,5 @@
-"""Multi-GPU layout: one process per GPU, one map split into z slabs.
+"""Multi-GPU layout: one process per GPU, one map split into z slabs, or a batch of molecules dealt
+out to the ranks.
 
 Grid points are independent, so a map shards by z slabs with no collective on the data path: every
 rank holds all atoms, evaluates its slab with coul_forward_3d_slab (the full grid's coordinates, so
@@ -6,6 +7,9 @@ the slabs put together equal the single-GPU map bit for bit), and writes it to i
 optional all-gather assembles the whole map on every rank (NCCL over NVLink on GPUs, gloo on CPU).
 The reference has no multi-device path for this computation (KTT tunes one kernel on one device,
 Source/Api/Tuner.h:83 takes one platform/device index).
+
+A batch of molecules shards by molecule (molecule_plan: longest first, each to the least-loaded
+rank), each rank running its share through one persistent launch, again with no collective.
 
 The timing helpers (barrier, max over ranks) are the ones the benchmark uses.
 """
@@ -88,3 +92,40 @@ def forward_3d_sharded(ctx, atoms, dims, spacing, origin=None, tune=None, group=
     dist.all_gather(parts, padded, group=group)
     full = torch.cat([p[: b - a] for p, (a, b) in zip(parts, plan)], dim=0)
     return slab, (z0, z1), full
+
+
+def molecule_plan(pairs: list[float], world: int) -> list[list[int]]:
+    """Molecules of a batch dealt to ranks, longest processing time first: each molecule in
+    decreasing order of pair count goes to the rank with the fewest pairs so far (ties: the lower
+    rank), so every rank's share stays within one molecule of the average.  Deterministic; returns
+    each rank's molecule indices in the order they were dealt."""
+    if world < 1:
+        raise ValueError("world >= 1 required")
+    order = sorted(range(len(pairs)), key=lambda i: (-pairs[i], i))
+    load = [0.0] * world
+    plan: list[list[int]] = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        plan[r].append(i)
+        load[r] += pairs[i]
+    return plan
+
+
+def batch_sharded(ctx, molecules, tune=None, group=None):
+    """This rank's molecules of a batch (molecule_plan over the ranks' count), evaluated by one
+    persistent launch on this rank's GPU; no collective on the data path.  `molecules` as for
+    ktt_b200.Batch.  Returns (indices, outputs): the molecule indices this rank evaluated and their
+    maps, in the same order."""
+    import ktt_b200
+    rank, world = rank_world(group)
+    pairs = [float(m[0].shape[0]) * int(m[1][0]) * int(m[1][1]) * int(m[1][2]) for m in molecules]
+    mine = molecule_plan(pairs, world)[rank]
+    if not mine:
+        return [], []
+    batch = ktt_b200.Batch(ctx, [molecules[i] for i in mine], tune)
+    try:
+        batch.run(ktt_b200.BATCH_PERSISTENT)
+        ctx.synchronize()
+        return mine, list(batch.outputs)
+    finally:
+        batch.close()

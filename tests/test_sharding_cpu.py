@@ -84,3 +84,19 @@ def test_sharded_map_gloo(tmp_path, world):
         assert (int(row[0]), int(row[1])) == plan[r]
         assert row[2] == 1.0, f"rank {r}: gathered map differs from the oracle's"
         assert row[3] == 10.0 * world
+
+
+@pytest.mark.parametrize("world", [1, 2, 3, 8])
+def test_molecule_plan_deals_every_molecule_once_balanced(world):
+    rng = np.random.default_rng(7)
+    pairs = list(rng.lognormal(20.0, 1.5, 137))
+    plan = sharding.molecule_plan(pairs, world)
+    assert len(plan) == world
+    dealt = sorted(i for part in plan for i in part)
+    assert dealt == list(range(len(pairs)))
+    loads = [sum(pairs[i] for i in part) for part in plan]
+    # longest processing time first: no rank exceeds the average by more than the largest molecule
+    assert max(loads) <= sum(pairs) / world + max(pairs)
+    assert sharding.molecule_plan(pairs, world) == plan  # deterministic
+    with pytest.raises(ValueError):
+        sharding.molecule_plan(pairs, 0)

@@ -1,5 +1,6 @@
 """z-slab sharding on one GPU: the slabs of a map, each evaluated by coul_forward_3d_slab as the
-ranks of a sharded run would, put together equal the single-launch map bit for bit."""
+ranks of a sharded run would, put together equal the single-launch map bit for bit; and the
+molecule-sharded batch on one rank equals one batch of all molecules."""
 import numpy as np
 import pytest
 
@@ -67,3 +68,20 @@ def test_bad_slab_rejected(ctx, z0, z1):
     with pytest.raises(ktt_b200.CoulombError):
         ctx.forward_3d_slab(torch.from_numpy(a).cuda(), dims, h, z0, z1, origin,
                             out=torch.empty((max(z1 - z0, 1), dims[1], dims[0]), device="cuda"))
+
+
+def test_batch_sharded_single_rank_equals_batch(ctx):
+    """One rank (no process group): batch_sharded evaluates every molecule, in the plan's order, with
+    the same maps bit for bit as one Batch of all of them."""
+    import torch
+    from ktt_b200 import workloads
+    mols = workloads.molecule_batch(seed=31, n_mol=6, lo=50, hi=2000)
+    inputs = [(torch.from_numpy(m.atoms).cuda(), m.dims, m.spacing, m.origin) for m in mols]
+    idx, outs = sharding.batch_sharded(ctx, inputs)
+    assert sorted(idx) == list(range(len(mols)))
+    b = ktt_b200.Batch(ctx, inputs)
+    b.run(ktt_b200.BATCH_PERSISTENT)
+    ctx.synchronize()
+    for i, o in zip(idx, outs):
+        assert torch.equal(o, b.outputs[i])
+    b.close()
