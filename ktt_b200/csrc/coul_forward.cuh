@@ -732,8 +732,8 @@ __global__ void __launch_bounds__(kMaxThreads) queue_split_kernel(const FwdParam
 // pieces in CTA order, stores it and zeroes the counter for the next launch: deterministic for a
 // given grid, and no CTA waits on another.
 // A CTA of up to kBalThreads threads fills an SM by itself (64 registers a thread): its warps meet at
-// every stage, so they progress together -- where two CTAs share an SM, the warp schedulers let one
-// run ahead and the other finishes alone at half the occupancy.
+// the barriers of refilled stages and piece ends, so they progress together -- where two CTAs share an
+// SM, the warp schedulers let one run ahead and the other finishes alone at half the occupancy.
 constexpr int kBalStageAtoms = 4096;  // atoms per stage of the balanced form's ring (at most)
 constexpr int kBalFirstAtoms = 1024;  // atoms in a CTA's first stage: the SM starts work sooner
 constexpr int kBalThreads = 1024;     // launch bound of the balanced form (tile threads x groups)
