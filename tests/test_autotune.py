@@ -108,6 +108,21 @@ def test_batch_search_short():
 
 
 @pytest.mark.gpu
+def test_precise_forms_searched_and_validated():
+    """PRECISION as a searched parameter: the map search over both FP64-merge forms and the batch
+    search over the shared-sum form validate every configuration they try against the reference."""
+    spy = _Spy()
+    result = autotune.tune_map3d(grid=64, atoms=2048, searcher="random", budget=6, reference=spy,
+                                 precisions=(ktt_b200.PREC_FP64_MERGE, ktt_b200.PREC_FP64_MERGE_SHARED))
+    assert all(t["status"] == "Ok" for t in result["trials"]), result["trials"]
+    assert result["tune"]["precision"] in (ktt_b200.PREC_FP64_MERGE, ktt_b200.PREC_FP64_MERGE_SHARED)
+    batch = autotune.tune_batch(molecules=10, seed=8, searcher="random", budget=5, reference=_Spy(),
+                                precisions=(ktt_b200.PREC_FP64_MERGE_SHARED,))
+    assert all(t["status"] == "Ok" for t in batch["trials"]), batch["trials"]
+    assert batch["batched"]["precision"] == ktt_b200.PREC_FP64_MERGE_SHARED and batch["precisions"] == [4]
+
+
+@pytest.mark.gpu
 def test_fp64_reference_kernel_matches_the_oracle():
     import torch
 
